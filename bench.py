@@ -1,0 +1,425 @@
+"""Benchmark of the B200 relational hot path: hash groupby aggregation,
+200M rows (Zipf(1.1) int64 keys over 10M distinct values; float64 N(0,1) with
+10% nulls; int32 U[0, 1e6)); SUM and MEAN of the float64 column, COUNT(*) and
+COUNT of the float64 column, MIN/MAX and NUNIQUE of the int32 column.
+
+One step = one groupby_aggregation call through the public API (C ABI) on
+device-resident inputs (4.2 GB, far larger than the 126 MB L2, so no flush is
+needed).  Prints ONE JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs (torchrun) are independent replicas: the path is a single-GPU
+task body and shards by rows with no data-path collective (weak scaling);
+the process group only carries the barrier and the max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "legate-dataframe_b200"))
+
+METRIC = "join/groupby rows/s + % HBM roofline (1 B200); batched p50/p99 vs unbatched"
+N_ROWS = 200_000_000
+N_KEYS = 10_000_000
+AGGS = [
+    ("v", "sum", "sum_v"),
+    ("v", "mean", "mean_v"),
+    (None, "count_all", "count"),
+    ("v", "count", "count_v"),
+    ("i", "min", "min_i"),
+    ("i", "max", "max_i"),
+    ("i", "count_distinct", "nunique_i"),
+]
+IN_BYTES_PER_ROW = 8 + 8 + 1 + 4  # key + f64 + its null mask + i32 (legate layout)
+
+
+def measured_peak_gbs():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# synthetic input (seeded, generated on the device)
+# ---------------------------------------------------------------------------
+def make_input_device(n_rows: int, device):
+    import torch
+
+    g = torch.Generator(device=device)
+    ranks = torch.arange(1, N_KEYS + 1, device=device, dtype=torch.float64)
+    w = ranks.pow(-1.1)
+    cdf = torch.cumsum(w, 0)
+    cdf /= cdf[-1].clone()
+    g.manual_seed(3)
+    perm = torch.randperm(N_KEYS, device=device, generator=g)
+    key_values = perm.to(torch.int64) * 2_654_435_761 + 12_345  # 10M distinct int64 values
+    keys = torch.empty(n_rows, dtype=torch.int64, device=device)
+    g.manual_seed(1)
+    chunk = 50_000_000
+    for s in range(0, n_rows, chunk):
+        e = min(n_rows, s + chunk)
+        u = torch.rand(e - s, dtype=torch.float64, device=device, generator=g)
+        r = torch.searchsorted(cdf, u).clamp_(max=N_KEYS - 1)
+        keys[s:e] = key_values[r]
+        del u, r
+    del cdf, w, ranks, perm
+    g.manual_seed(4)
+    v = torch.randn(n_rows, dtype=torch.float64, device=device, generator=g)
+    valid = (torch.rand(n_rows, device=device, generator=g) >= 0.10).to(torch.uint8)
+    g.manual_seed(5)
+    i = torch.randint(0, 1_000_000, (n_rows,), dtype=torch.int32, device=device, generator=g)
+    torch.cuda.synchronize(device)
+    return keys, v, valid, i
+
+
+def device_table(keys, v, valid, i):
+    import pyarrow as pa
+
+    from legate_dataframe import LogicalColumn, LogicalTable
+
+    cols = [
+        LogicalColumn.from_torch(keys, pa.int64()),
+        LogicalColumn.from_torch(v, pa.float64(), valid),
+        LogicalColumn.from_torch(i, pa.int32()),
+    ]
+    return LogicalTable(cols, ["k", "v", "i"])
+
+
+def host_sample(keys, v, valid, i, n):
+    import numpy as np
+    import pyarrow as pa
+
+    k = keys[:n].cpu().numpy()
+    vv = v[:n].cpu().numpy()
+    m = valid[:n].cpu().numpy().astype(bool)
+    ii = i[:n].cpu().numpy()
+    return pa.table({"k": k, "v": pa.array(vv, mask=~m), "i": ii})
+
+
+def output_bytes(tbl) -> int:
+    total = 0
+    for c in tbl.get_columns():
+        from legate_dataframe import _native as N
+
+        total += c.size * N.TYPE_WIDTH[c.ldf_type] + (c.size if c.valid is not None else 0)
+    return total
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if r[5 + j].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines: the reference's CPU path (Arrow Acero aggregate, the calls of
+# GroupByAggregationTask::cpu_variant) on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_groupby_rate(sample, use_threads: bool, min_seconds: float = 10.0):
+    from oracle import arrow_ref
+
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        arrow_ref.groupby(sample, ["k"], AGGS, use_threads=use_threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or reps >= 20:
+            break
+    return sample.num_rows * reps / el, el, reps
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation of the path (Arrow
+    Acero aggregate) with every host thread, on bounded samples."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np
+    import pyarrow as pa
+
+    n = 8_000_000
+    rng = np.random.default_rng(3)
+    ranks = np.arange(1, N_KEYS + 1, dtype=np.float64)
+    cdf = np.cumsum(ranks ** -1.1)
+    cdf /= cdf[-1]
+    key_values = rng.permutation(N_KEYS).astype(np.int64) * 2_654_435_761 + 12_345
+    k = key_values[np.minimum(np.searchsorted(cdf, np.random.default_rng(1).random(n)), N_KEYS - 1)]
+    r4 = np.random.default_rng(4)
+    v = r4.normal(size=n)
+    m = r4.random(n) < 0.10
+    i = np.random.default_rng(5).integers(0, 1_000_000, n).astype(np.int32)
+    sample = pa.table({"k": k, "v": pa.array(v, mask=m), "i": i})
+    from oracle import arrow_ref
+
+    for _ in range(args.warmup):
+        arrow_ref.groupby(sample, ["k"], AGGS, use_threads=True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        arrow_ref.groupby(sample, ["k"], AGGS, use_threads=True)
+    el = time.perf_counter() - t0
+    rate = n * args.steps / el
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+int64",
+        "data": "synthetic (seeded, config-1 distributions)",
+        "config": {"workload": "groupby config 1 (Zipf 1.1 int64 keys over 10M, f64 N(0,1) 10% nulls, i32)",
+                   "rows_per_step": n, "full_rows": N_ROWS},
+        "cpu_baseline": {"value": rate, "unit": "rows/s", "cores": cores, "kind": "port",
+                         "sample": f"{n} rows/step of the config-1 distribution; Arrow {pa.__version__} Acero "
+                                   "aggregate (hash_sum/mean/count_all/count/min/max/count_distinct), "
+                                   "use_threads=True: the Arrow calls of the reference's cpu_variant"},
+        "e2e": {"value": rate, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rows", type=int, default=N_ROWS)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, default=4_000_000)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+
+    from legate_dataframe import _native as N
+    from legate_dataframe.lib.groupby_aggregation import groupby_aggregation
+
+    N.lib()
+    n = args.rows
+    keys, v, valid, i = make_input_device(n, device)
+    table = device_table(keys, v, valid, i)
+
+    def step():
+        return groupby_aggregation(table, ["k"], AGGS)
+
+    for _ in range(max(args.warmup, 3)):
+        out = step()
+    groups = out.num_rows()
+    out_b = output_bytes(out)
+    del out
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- timed region (device-resident inputs) -----------------------------
+    launches0 = N.launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            out = step()
+            del out
+        ev1.record()
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = (N.launch_count() - launches0) // args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * n / (ms_step / 1e3)
+
+    # ---- per-kernel device times (CUDA events on the launching stream) ------
+    N.profile_enable(True)
+    N.profile_report(reset=True)
+    for _ in range(2):
+        out = step()
+        del out
+    torch.cuda.synchronize()
+    prof = N.profile_report(reset=True)
+    N.profile_enable(False)
+    agg_cnt, agg_ms = prof.get("aggregate", (1, float("nan")))
+    agg_ms /= max(agg_cnt, 1)
+    total_prof = sum(t for _, t in prof.values())
+    peak, peak_kind = measured_peak_gbs()
+    algo_kernel = n * IN_BYTES_PER_ROW
+    achieved = algo_kernel / (agg_ms / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "groupby_config1_aggregate_traffic.json"
+    if tp.exists():
+        try:
+            tj = json.loads(tp.read_text())
+            traffic = float(tj["dram_bytes_per_row"]) * n
+        except (KeyError, ValueError):
+            traffic = None
+    op_bytes = n * IN_BYTES_PER_ROW + out_b
+
+    # ---- end to end: host (pinned) -> device -> op -> host -----------------
+    e2e = None
+    if rank == 0 or world > 1:
+        hk = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        hv = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        hm = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        hi = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        hk.copy_(keys)
+        hv.copy_(v)
+        hm.copy_(valid)
+        hi.copy_(i)
+        dk, dv, dm, di = torch.empty_like(keys), torch.empty_like(v), torch.empty_like(valid), torch.empty_like(i)
+        torch.cuda.synchronize()
+        d2h = 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record()
+        for _ in range(args.e2e_steps):
+            dk.copy_(hk, non_blocking=True)
+            dv.copy_(hv, non_blocking=True)
+            dm.copy_(hm, non_blocking=True)
+            di.copy_(hi, non_blocking=True)
+            res = groupby_aggregation(device_table(dk, dv, dm, di), ["k"], AGGS)
+            host = res.to_arrow()
+            d2h = output_bytes(res)
+            del res, host
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * n / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
+               "h2d_bytes_per_step": n * IN_BYTES_PER_ROW, "d2h_bytes_per_step": d2h}
+        del hk, hv, hm, hi, dk, dv, dm, di
+
+    # ---- CPU baseline (rank 0, N=1 only) ------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import pyarrow as pa
+
+        sample = host_sample(keys, v, valid, i, min(args.cpu_sample, n))
+        rate, el, reps = cpu_groupby_rate(sample, use_threads=False)
+        cpu = {"value": rate, "unit": "rows/s", "cores": 1, "kind": "port",
+               "sample": f"first {sample.num_rows} rows of the same input x{reps} ({el:.1f} s); Arrow "
+                         f"{pa.__version__} Acero aggregate hash_sum/mean/count_all/count/min/max/count_distinct, "
+                         "use_threads=False: the Arrow calls of the reference's cpu_variant (one legate CPU task)"}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "rows/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": max(args.warmup, 3),
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64+int64 (fixed-point exact f64 sums)",
+        "data": "synthetic (seeded on device: Zipf(1.1) keys over 10M int64, f64 N(0,1) 10% nulls, i32 U[0,1e6))",
+        "config": {"workload": "groupby config 1: 200M rows; SUM/MEAN(f64), COUNT(*), COUNT(f64), MIN/MAX(i32), "
+                               "NUNIQUE(i32)", "rows": n, "groups": groups,
+                   "l2": "inputs 4.2 GB >> 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "aggregate", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes": algo_kernel, "kernel_ms": agg_ms,
+                     "op_frac": (op_bytes / (ms_step / 1e3) / 1e9) / peak, "op_algorithmic_bytes": op_bytes},
+        "kernel_ms": {k: round(t / max(c, 1), 4) for k, (c, t) in prof.items()},
+        "kernel_share": {k: round(t / total_prof, 4) for k, (c, t) in prof.items()} if total_prof else {},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,186 @@
+/*
+ * ldf_b200.h -- C ABI of the B200-native relational hot path (join, groupby
+ * aggregation, sort, local hash partition) of legate-dataframe.
+ *
+ * Every entry point replaces the libcudf calls made inside one legate GPU task
+ * body of the reference.  The task body keeps reading its arguments exactly as
+ * it does today (same order, same TaskContext); instead of building cudf views
+ * it fills `ldf_column` descriptors straight from the legate physical stores
+ * (data, bool-per-row null mask, Rect<1> string ranges + chars) and calls one
+ * function below on `ctx.stream()`.
+ *
+ * Conventions
+ *  - Plain C: pointers, sizes, int status.  No cudf/legate/torch types.
+ *  - `stream` is a cudaStream_t passed as void*.  All device work is ordered on
+ *    it; the only host synchronisation is the read-back of an output row count.
+ *  - Inputs are borrowed and read-only.  Outputs are allocated through the
+ *    caller's `ldf_allocator` (legate: `legate::create_buffer`-backed, never
+ *    cudaMalloc inside a task) and handed back for zero-copy binding.  A NULL
+ *    allocator selects stream-ordered cudaMallocAsync/cudaFreeAsync.
+ *  - Status: 0 on success; otherwise an LDF_ERR_* code and a message readable
+ *    with ldf_b200_last_error() (thread-local).  Host wrappers rethrow them as
+ *    std::invalid_argument / std::runtime_error like the reference does.
+ */
+#ifndef LDF_B200_H
+#define LDF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  LDF_OK                   = 0,
+  LDF_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  LDF_ERR_CUDA             = 2, /* LDF_CUDA_TRY failure (utils.hpp:241-245) */
+  LDF_ERR_OUT_OF_MEMORY    = 3, /* allocator returned NULL */
+  LDF_ERR_UNSUPPORTED      = 4, /* type/aggregation not supported */
+  LDF_ERR_TIMEOUT          = 5, /* a bounded device-side wait expired */
+  LDF_ERR_INTERNAL         = 6
+};
+
+/* ---- column types (Arrow logical types used by the path) ---------------- */
+enum {
+  LDF_BOOL8   = 1, /* arrow bool, stored one byte per row (legate layout) */
+  LDF_INT8    = 2,
+  LDF_INT16   = 3,
+  LDF_INT32   = 4,
+  LDF_INT64   = 5,
+  LDF_UINT8   = 6,
+  LDF_UINT16  = 7,
+  LDF_UINT32  = 8,
+  LDF_UINT64  = 9,
+  LDF_FLOAT32 = 10,
+  LDF_FLOAT64 = 11,
+  LDF_STRING  = 12, /* legate string: Rect<1> ranges + int8 chars */
+  LDF_TIMESTAMP_US = 13 /* int64 microseconds */
+};
+
+/* legate::Rect<1> of a string row: inclusive global [lo, hi] char range. */
+typedef struct {
+  int64_t lo;
+  int64_t hi;
+} ldf_range;
+
+/* One column in the legate physical layout (core/column.hpp:454-671).
+ *  data       fixed width: `size` values; LDF_STRING: `size` ldf_range
+ *  valid      legate null mask, one byte per row, nonzero = valid; NULL when
+ *             the column is not nullable
+ *  chars      LDF_STRING only: character bytes; global char position p is
+ *             chars[p - chars_base]
+ */
+typedef struct {
+  int32_t type;
+  int32_t nullable; /* output columns: set by the library; inputs: valid != NULL */
+  int64_t size;
+  void* data;
+  uint8_t* valid;
+  char* chars;
+  int64_t chars_base;
+  int64_t num_chars;
+} ldf_column;
+
+/* Device memory for outputs and scratch (legate TaskMemoryResource,
+ * core/allocator.cu:27-81). `allocate` returns NULL on failure. */
+typedef struct {
+  void* ctx;
+  void* (*allocate)(void* ctx, size_t nbytes, void* stream);
+  void (*deallocate)(void* ctx, void* ptr, size_t nbytes, void* stream);
+} ldf_allocator;
+
+/* ---- join --------------------------------------------------------------- */
+enum { LDF_JOIN_INNER = 0, LDF_JOIN_LEFT = 1, LDF_JOIN_FULL = 2, LDF_JOIN_SEMI = 3, LDF_JOIN_ANTI = 4 };
+
+/* Hash join: build on `rhs`, probe with `lhs`; the output holds the lhs_out
+ * columns followed by the rhs_out columns.  LEFT makes every rhs output column
+ * nullable, FULL every output column (join.cpp:348-383).  `out` has
+ * n_lhs_out + n_rhs_out entries and is filled by the call.
+ * Replaces cudf_join + cudf::gather in JoinTask::gpu_variant (join.cu:32-155);
+ * semantics of JoinTask::cpu_variant (join.cpp:168-228). */
+int ldf_b200_join(const ldf_column* lhs, int32_t lhs_ncols,
+                  const ldf_column* rhs, int32_t rhs_ncols,
+                  const int32_t* lhs_keys, const int32_t* rhs_keys, int32_t nkeys,
+                  int32_t join_type, int32_t nulls_equal,
+                  const int32_t* lhs_out, int32_t n_lhs_out,
+                  const int32_t* rhs_out, int32_t n_rhs_out,
+                  ldf_column* out, const ldf_allocator* alloc, void* stream);
+
+/* ---- groupby aggregation ------------------------------------------------ */
+enum {
+  LDF_AGG_SUM            = 0,
+  LDF_AGG_MIN            = 1,
+  LDF_AGG_MAX            = 2,
+  LDF_AGG_COUNT          = 3,
+  LDF_AGG_COUNT_ALL      = 4,
+  LDF_AGG_MEAN           = 5,
+  LDF_AGG_COUNT_DISTINCT = 6,
+  LDF_AGG_PRODUCT        = 7,
+  LDF_AGG_VARIANCE       = 8,
+  LDF_AGG_STDDEV         = 9
+};
+/* arrow::compute::CountOptions::CountMode */
+enum { LDF_COUNT_ONLY_VALID = 0, LDF_COUNT_ONLY_NULL = 1, LDF_COUNT_ALL = 2 };
+
+typedef struct {
+  int32_t in_col;     /* input column (ignored for COUNT_ALL) */
+  int32_t kind;       /* LDF_AGG_* */
+  int32_t count_mode; /* LDF_COUNT_* for COUNT / COUNT_DISTINCT */
+  int32_t out_type;   /* output LDF_* type (the Arrow hash_<kind> result type) */
+} ldf_aggregation;
+
+/* Hash groupby: output = key columns then one column per aggregation, in
+ * request order; null keys form a group (null_policy::INCLUDE).  Output row
+ * order is unspecified.  Replaces the cudf::groupby call in
+ * GroupByAggregationTask::gpu_variant (groupby_aggregation.cu:90-167);
+ * semantics of the Acero hash_* aggregations (groupby_aggregation.cpp:41-94). */
+int ldf_b200_groupby_aggregation(const ldf_column* table, int32_t ncols,
+                                 const int32_t* keys, int32_t nkeys,
+                                 const ldf_aggregation* aggs, int32_t naggs,
+                                 ldf_column* out, const ldf_allocator* alloc, void* stream);
+
+/* ---- sort --------------------------------------------------------------- */
+/* Stable lexicographic sort of the whole table on `keys`.  `nulls_at_end`
+ * applies to every key regardless of direction (sort.cu:309-323).
+ * `limit` = INT64_MIN for none, >0 head, <0 tail (sort.cu:275-291).
+ * The sort is always stable, so `stable` only documents the request.
+ * Replaces cudf::(stable_)sort_by_key in SortTask::gpu_variant (sort.cu:325-330). */
+int ldf_b200_sort(const ldf_column* table, int32_t ncols,
+                  const int32_t* keys, const uint8_t* ascending, int32_t nkeys,
+                  int32_t nulls_at_end, int32_t stable, int64_t limit,
+                  ldf_column* out, const ldf_allocator* alloc, void* stream);
+
+/* ---- local hash partition ---------------------------------------------- */
+/* Reorder the table so that rows of bucket b (= hash(keys) % nparts) are
+ * contiguous, buckets in order, input order kept inside a bucket.
+ * `offsets` (host, nparts + 1 entries) receives the bucket start offsets and
+ * the total.  Replaces cudf::hash_partition + cudf::split in
+ * task::repartition_by_hash (core/repartition_by_hash.cu:296-310). */
+int ldf_b200_hash_partition(const ldf_column* table, int32_t ncols,
+                            const int32_t* keys, int32_t nkeys, int32_t nparts,
+                            ldf_column* out, int64_t* offsets,
+                            const ldf_allocator* alloc, void* stream);
+
+/* ---- utilities ---------------------------------------------------------- */
+/* Message of the last failed call on this thread ("" if none). */
+const char* ldf_b200_last_error(void);
+/* Library version string. */
+const char* ldf_b200_version(void);
+/* Release the buffers of an output column produced by this library. */
+int ldf_b200_free_column(ldf_column* col, const ldf_allocator* alloc, void* stream);
+
+/* ---- instrumentation (no counterpart in the reference; used by the bench) */
+/* Number of kernels this library has launched in the process. */
+unsigned long long ldf_b200_launch_count(void);
+/* Bracket every later launch with CUDA events on its stream (on != 0). */
+void ldf_b200_profile_enable(int on);
+/* Per-kernel "name launches total_ms" lines; returns the full text length. */
+int ldf_b200_profile_report(char* buf, size_t len, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LDF_B200_H */

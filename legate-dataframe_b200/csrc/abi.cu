@@ -1,0 +1,120 @@
+// extern "C" entry points (include/ldf_b200.h): argument checks, exception ->
+// status translation, one OpContext per call.
+#include "radix.cuh"
+
+namespace ldf {
+void join(const ldf_column* lhs, int lhs_ncols, const ldf_column* rhs, int rhs_ncols,
+          const int32_t* lhs_keys, const int32_t* rhs_keys, int nkeys, int join_type,
+          bool nulls_equal, const int32_t* lhs_out, int n_lhs_out, const int32_t* rhs_out,
+          int n_rhs_out, ldf_column* out, const OpContext& ctx);
+void groupby_aggregation(const ldf_column* table, int ncols, const int32_t* keys, int nkeys,
+                         const ldf_aggregation* aggs, int naggs, ldf_column* out, const OpContext& ctx);
+void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const uint8_t* ascending, int nkeys,
+                bool nulls_at_end, int64_t limit, ldf_column* out, const OpContext& ctx);
+void hash_partition(const ldf_column* table, int ncols, const int32_t* keys, int nkeys, int nparts,
+                    ldf_column* out, int64_t* offsets, const OpContext& ctx);
+}  // namespace ldf
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& f)
+{
+  g_last_error.clear();
+  try {
+    f();
+    return LDF_OK;
+  } catch (const ldf::LdfError& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return LDF_ERR_INTERNAL;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return LDF_ERR_INTERNAL;
+  }
+}
+
+void check_table(const ldf_column* t, int32_t ncols, const char* what)
+{
+  LDF_REQUIRE(ncols >= 0, std::string(what) + ": negative column count");
+  LDF_REQUIRE(ncols == 0 || t != nullptr, std::string(what) + ": null column array");
+  for (int i = 0; i < ncols; ++i) {
+    ldf::type_width(t[i].type);
+    LDF_REQUIRE(t[i].size == t[0].size, std::string(what) + ": columns differ in length");
+    LDF_REQUIRE(t[i].size == 0 || t[i].data != nullptr, std::string(what) + ": column without data");
+    if (t[i].type == LDF_STRING)
+      LDF_REQUIRE(t[i].size == 0 || t[i].chars != nullptr || t[i].num_chars == 0,
+                  std::string(what) + ": string column without chars");
+  }
+}
+}  // namespace
+
+extern "C" {
+
+const char* ldf_b200_last_error(void) { return g_last_error.c_str(); }
+const char* ldf_b200_version(void) { return "ldf_b200 0.1.0 (sm_100a)"; }
+
+int ldf_b200_join(const ldf_column* lhs, int32_t lhs_ncols, const ldf_column* rhs, int32_t rhs_ncols,
+                  const int32_t* lhs_keys, const int32_t* rhs_keys, int32_t nkeys, int32_t join_type,
+                  int32_t nulls_equal, const int32_t* lhs_out, int32_t n_lhs_out, const int32_t* rhs_out,
+                  int32_t n_rhs_out, ldf_column* out, const ldf_allocator* alloc, void* stream)
+{
+  return guarded([&] {
+    check_table(lhs, lhs_ncols, "lhs");
+    check_table(rhs, rhs_ncols, "rhs");
+    LDF_REQUIRE(out != nullptr || n_lhs_out + n_rhs_out == 0, "null output array");
+    ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
+    ldf::join(lhs, lhs_ncols, rhs, rhs_ncols, lhs_keys, rhs_keys, nkeys, join_type, nulls_equal != 0,
+              lhs_out, n_lhs_out, rhs_out, n_rhs_out, out, ctx);
+  });
+}
+
+int ldf_b200_groupby_aggregation(const ldf_column* table, int32_t ncols, const int32_t* keys, int32_t nkeys,
+                                 const ldf_aggregation* aggs, int32_t naggs, ldf_column* out,
+                                 const ldf_allocator* alloc, void* stream)
+{
+  return guarded([&] {
+    check_table(table, ncols, "table");
+    LDF_REQUIRE(naggs >= 0 && (naggs == 0 || aggs != nullptr), "bad aggregation list");
+    ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
+    ldf::groupby_aggregation(table, ncols, keys, nkeys, aggs, naggs, out, ctx);
+  });
+}
+
+int ldf_b200_sort(const ldf_column* table, int32_t ncols, const int32_t* keys, const uint8_t* ascending,
+                  int32_t nkeys, int32_t nulls_at_end, int32_t stable, int64_t limit, ldf_column* out,
+                  const ldf_allocator* alloc, void* stream)
+{
+  (void)stable;  // the radix sort is always stable
+  return guarded([&] {
+    check_table(table, ncols, "table");
+    ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
+    ldf::sort_table(table, ncols, keys, ascending, nkeys, nulls_at_end != 0, limit, out, ctx);
+  });
+}
+
+int ldf_b200_hash_partition(const ldf_column* table, int32_t ncols, const int32_t* keys, int32_t nkeys,
+                            int32_t nparts, ldf_column* out, int64_t* offsets, const ldf_allocator* alloc,
+                            void* stream)
+{
+  return guarded([&] {
+    check_table(table, ncols, "table");
+    LDF_REQUIRE(offsets != nullptr, "null offsets array");
+    ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
+    ldf::hash_partition(table, ncols, keys, nkeys, nparts, out, offsets, ctx);
+  });
+}
+
+int ldf_b200_free_column(ldf_column* col, const ldf_allocator* alloc, void* stream)
+{
+  return guarded([&] {
+    if (col == nullptr) return;
+    ldf::Allocator a(alloc, static_cast<cudaStream_t>(stream));
+    ldf::free_out_column(a, *col);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,360 @@
+// Common device/host infrastructure of the B200 relational kernels:
+// error handling, the allocator contract, device column views, key hashing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstring>
+#include <utility>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ldf_b200.h"
+
+namespace ldf {
+
+// ---------------------------------------------------------------------------
+// Errors.  Host code throws LdfError; the C-ABI layer turns it into a status
+// code plus a thread-local message.
+// ---------------------------------------------------------------------------
+struct LdfError : std::runtime_error {
+  int code;
+  LdfError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw LdfError(code, msg); }
+
+#define LDF_CUDA(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e__ = (call);                                                             \
+    if (e__ != cudaSuccess) {                                                             \
+      ::ldf::fail(LDF_ERR_CUDA, std::string("CUDA error ") + cudaGetErrorString(e__) +    \
+                                  " at " + __FILE__ + ":" + std::to_string(__LINE__));    \
+    }                                                                                     \
+  } while (0)
+
+#define LDF_CHECK_LAUNCH() LDF_CUDA(cudaGetLastError())
+
+#define LDF_REQUIRE(cond, msg)                                                 \
+  do {                                                                         \
+    if (!(cond)) ::ldf::fail(LDF_ERR_INVALID_ARGUMENT, (msg));                 \
+  } while (0)
+
+// Number of SMs of the current device (148 on B200); grids are sized in
+// multiples of it.
+int num_sms();
+
+// ---------------------------------------------------------------------------
+// Kernel launches.  Every kernel of the library goes through `launch`, which
+// counts launches and, when profiling is on, brackets the launch with CUDA
+// events on its own stream (per-kernel device time, read by the bench).
+// ---------------------------------------------------------------------------
+namespace prof {
+void begin(const char* name, cudaStream_t s);
+void end(const char* name, cudaStream_t s);
+}  // namespace prof
+
+template <typename... KArgs, typename... Args>
+inline void launch(const char* name, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                   cudaStream_t s, Args&&... args)
+{
+  prof::begin(name, s);
+  kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+  LDF_CHECK_LAUNCH();
+  prof::end(name, s);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation.  All device memory (outputs and scratch) comes from the caller's
+// allocator; with none, stream-ordered cudaMallocAsync.  Scratch buffers are
+// RAII and released on the same stream, so no device-wide synchronisation.
+// ---------------------------------------------------------------------------
+class Allocator {
+ public:
+  Allocator(const ldf_allocator* a, cudaStream_t s) : a_(a), s_(s) {}
+  void* allocate(size_t nbytes) const;
+  void deallocate(void* p, size_t nbytes) const;
+  cudaStream_t stream() const { return s_; }
+
+ private:
+  const ldf_allocator* a_;
+  cudaStream_t s_;
+};
+
+template <typename T>
+class Buffer {
+ public:
+  Buffer() = default;
+  Buffer(const Allocator& a, size_t n) : a_(&a), n_(n)
+  {
+    p_ = static_cast<T*>(a.allocate(bytes()));
+  }
+  Buffer(const Buffer&)            = delete;
+  Buffer& operator=(const Buffer&) = delete;
+  Buffer(Buffer&& o) noexcept { *this = std::move(o); }
+  Buffer& operator=(Buffer&& o) noexcept
+  {
+    reset();
+    a_ = o.a_;
+    p_ = o.p_;
+    n_ = o.n_;
+    o.p_ = nullptr;
+    o.n_ = 0;
+    return *this;
+  }
+  ~Buffer() { reset(); }
+  void reset()
+  {
+    if (p_ && a_) a_->deallocate(p_, bytes());
+    p_ = nullptr;
+    n_ = 0;
+  }
+  // Give up ownership (used for outputs that are handed back to the caller).
+  T* release()
+  {
+    T* p = p_;
+    p_   = nullptr;
+    n_   = 0;
+    return p;
+  }
+  T* get() const { return p_; }
+  size_t size() const { return n_; }
+  size_t bytes() const { return n_ == 0 ? 16 : n_ * sizeof(T); }
+
+ private:
+  const Allocator* a_ = nullptr;
+  T* p_               = nullptr;
+  size_t n_           = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Types.
+// ---------------------------------------------------------------------------
+inline int type_width(int t)
+{
+  switch (t) {
+    case LDF_BOOL8:
+    case LDF_INT8:
+    case LDF_UINT8: return 1;
+    case LDF_INT16:
+    case LDF_UINT16: return 2;
+    case LDF_INT32:
+    case LDF_UINT32:
+    case LDF_FLOAT32: return 4;
+    case LDF_INT64:
+    case LDF_UINT64:
+    case LDF_FLOAT64:
+    case LDF_TIMESTAMP_US: return 8;
+    case LDF_STRING: return 16;  // one ldf_range per row
+    default: fail(LDF_ERR_UNSUPPORTED, "unsupported column type id " + std::to_string(t));
+  }
+}
+inline bool is_string(int t) { return t == LDF_STRING; }
+inline bool is_float(int t) { return t == LDF_FLOAT32 || t == LDF_FLOAT64; }
+inline bool is_signed_int(int t)
+{
+  return t == LDF_INT8 || t == LDF_INT16 || t == LDF_INT32 || t == LDF_INT64 ||
+         t == LDF_TIMESTAMP_US;
+}
+
+// Device view of one input column (the legate layout, read directly: the
+// bool-per-row null mask and the global Rect<1> string ranges are consumed
+// as they are, no bitmask / offsets conversion pass).
+struct DCol {
+  const void* data;
+  const uint8_t* valid;
+  const char* chars;
+  int64_t chars_base;
+  int32_t type;
+  int32_t width;
+};
+
+inline DCol make_dcol(const ldf_column& c)
+{
+  DCol d;
+  d.data       = c.data;
+  d.valid      = c.valid;
+  d.chars      = c.chars;
+  d.chars_base = c.chars_base;
+  d.type       = c.type;
+  d.width      = type_width(c.type);
+  return d;
+}
+
+// Device view of one output column.
+struct OCol {
+  void* data;
+  uint8_t* valid;
+  int32_t type;
+  int32_t width;
+};
+
+// ---------------------------------------------------------------------------
+// Device helpers.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool dvalid(const DCol& c, int64_t r)
+{
+  return c.valid == nullptr || c.valid[r] != 0;
+}
+
+// Raw bits of a fixed-width value, zero-extended; floats are normalised so
+// that -0.0 == 0.0 and every NaN is one value (equality/hash semantics).
+__device__ __forceinline__ uint64_t dbits(const DCol& c, int64_t r)
+{
+  switch (c.width) {
+    case 1: return static_cast<const uint8_t*>(c.data)[r];
+    case 2: return static_cast<const uint16_t*>(c.data)[r];
+    case 4: {
+      uint32_t v = static_cast<const uint32_t*>(c.data)[r];
+      if (c.type == LDF_FLOAT32) {
+        if ((v & 0x7fffffffu) == 0) v = 0;
+        else if ((v & 0x7f800000u) == 0x7f800000u && (v & 0x007fffffu)) v = 0x7fc00000u;
+      }
+      return v;
+    }
+    default: {
+      uint64_t v = static_cast<const uint64_t*>(c.data)[r];
+      if (c.type == LDF_FLOAT64) {
+        if ((v & 0x7fffffffffffffffull) == 0) v = 0;
+        else if ((v & 0x7ff0000000000000ull) == 0x7ff0000000000000ull &&
+                 (v & 0x000fffffffffffffull))
+          v = 0x7ff8000000000000ull;
+      }
+      return v;
+    }
+  }
+}
+
+__device__ __forceinline__ bool is_signed_int_dev(int t)
+{
+  return t == LDF_INT8 || t == LDF_INT16 || t == LDF_INT32 || t == LDF_INT64 ||
+         t == LDF_TIMESTAMP_US;
+}
+
+// Sign-extended value of a signed integer column.
+__device__ __forceinline__ int64_t signed_value(const DCol& c, int64_t r)
+{
+  switch (c.width) {
+    case 1: return static_cast<const int8_t*>(c.data)[r];
+    case 2: return static_cast<const int16_t*>(c.data)[r];
+    case 4: return static_cast<const int32_t*>(c.data)[r];
+    default: return static_cast<const int64_t*>(c.data)[r];
+  }
+}
+
+// MurmurHash3's 64-bit finaliser (public domain), used as the key mixer.
+__device__ __host__ __forceinline__ uint64_t mix64(uint64_t x)
+{
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdull;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ull;
+  x ^= x >> 33;
+  return x;
+}
+
+__device__ __host__ __forceinline__ uint64_t hash_combine64(uint64_t seed, uint64_t h)
+{
+  return mix64(seed ^ (h + 0x9e3779b97f4a7c15ull + (seed << 6) + (seed >> 2)));
+}
+
+// Byte length of a string row (ranges are inclusive, so hi = lo - 1 is "").
+__device__ __forceinline__ int64_t dstr_len(const DCol& c, int64_t r)
+{
+  const ldf_range* rg = static_cast<const ldf_range*>(c.data);
+  return rg[r].hi - rg[r].lo + 1;
+}
+__device__ __forceinline__ const uint8_t* dstr_ptr(const DCol& c, int64_t r)
+{
+  const ldf_range* rg = static_cast<const ldf_range*>(c.data);
+  return reinterpret_cast<const uint8_t*>(c.chars) + (rg[r].lo - c.chars_base);
+}
+
+// Hash of a byte string: 8-byte little-endian words folded through mix64.
+// The same function is restated in the numpy oracle (hash partition parity).
+__device__ __forceinline__ uint64_t hash_bytes(const uint8_t* p, int64_t n)
+{
+  uint64_t h = 0x27d4eb2f165667c5ull ^ (static_cast<uint64_t>(n) * 0x9e3779b97f4a7c15ull);
+  int64_t i  = 0;
+  for (; i + 8 <= n; i += 8) {
+    uint64_t w = 0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) w |= static_cast<uint64_t>(p[i + b]) << (8 * b);
+    h = mix64(h ^ w) + 0x165667b19e3779f9ull;
+  }
+  if (i < n) {
+    uint64_t w = 0;
+    for (int b = 0; i + b < n; ++b) w |= static_cast<uint64_t>(p[i + b]) << (8 * b);
+    h = mix64(h ^ w) + 0x165667b19e3779f9ull;
+  }
+  return mix64(h);
+}
+
+__device__ __forceinline__ bool bytes_equal(const uint8_t* a, const uint8_t* b, int64_t n)
+{
+  for (int64_t i = 0; i < n; ++i)
+    if (a[i] != b[i]) return false;
+  return true;
+}
+
+// Hash of one column value of a row, null-aware.  A null hashes to a fixed
+// constant.
+__device__ __forceinline__ uint64_t hash_value(const DCol& c, int64_t r)
+{
+  if (!dvalid(c, r)) return 0x5bd1e9955bd1e995ull;
+  if (c.type == LDF_STRING) return hash_bytes(dstr_ptr(c, r), dstr_len(c, r));
+  return mix64(dbits(c, r) + 0x9e3779b97f4a7c15ull * static_cast<uint64_t>(c.width));
+}
+
+// Value equality between row ra of column a and row rb of column b (same
+// type), nulls equal to nulls.
+__device__ __forceinline__ bool values_equal(const DCol& a, int64_t ra, const DCol& b, int64_t rb)
+{
+  bool va = dvalid(a, ra), vb = dvalid(b, rb);
+  if (va != vb) return false;
+  if (!va) return true;
+  if (a.type == LDF_STRING) {
+    int64_t la = dstr_len(a, ra), lb = dstr_len(b, rb);
+    if (la != lb) return false;
+    return bytes_equal(dstr_ptr(a, ra), dstr_ptr(b, rb), la);
+  }
+  return dbits(a, ra) == dbits(b, rb);
+}
+
+// Lemire's multiply-shift range reduction: hash -> [0, n).
+__device__ __forceinline__ uint64_t fastrange(uint64_t h, uint64_t n)
+{
+  return __umul64hi(h, n);
+}
+
+// Copy one fixed-width value.
+__device__ __forceinline__ void copy_fixed(void* dst, int64_t di, const void* src, int64_t si, int w)
+{
+  switch (w) {
+    case 1: static_cast<uint8_t*>(dst)[di] = static_cast<const uint8_t*>(src)[si]; break;
+    case 2: static_cast<uint16_t*>(dst)[di] = static_cast<const uint16_t*>(src)[si]; break;
+    case 4: static_cast<uint32_t*>(dst)[di] = static_cast<const uint32_t*>(src)[si]; break;
+    case 8: static_cast<uint64_t*>(dst)[di] = static_cast<const uint64_t*>(src)[si]; break;
+    default: static_cast<ldf_range*>(dst)[di] = static_cast<const ldf_range*>(src)[si]; break;
+  }
+}
+__device__ __forceinline__ void zero_fixed(void* dst, int64_t di, int w)
+{
+  switch (w) {
+    case 1: static_cast<uint8_t*>(dst)[di] = 0; break;
+    case 2: static_cast<uint16_t*>(dst)[di] = 0; break;
+    case 4: static_cast<uint32_t*>(dst)[di] = 0; break;
+    case 8: static_cast<uint64_t*>(dst)[di] = 0; break;
+    default: static_cast<ldf_range*>(dst)[di] = ldf_range{0, -1}; break;
+  }
+}
+
+// Bounded spin budget for device-side waits (look-back).  A wait that runs
+// out sets the call's error word and returns; it never traps or hangs.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace ldf

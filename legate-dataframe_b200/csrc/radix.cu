@@ -1,0 +1,363 @@
+// Onesweep LSD radix sort (Adinets & Merrill, "Onesweep", 2022) of row ids by
+// 8-bit digits, stable.  One upfront kernel builds the digit histograms of all
+// passes from the unpermuted columns (histograms do not depend on order); each
+// pass is then ONE kernel: tile load -> warp-level stable ranking with
+// __match_any_sync -> per-digit decoupled look-back across tiles -> tile staged
+// in shared memory in digit order -> coalesced runs written out.  Passes whose
+// digit is constant over all rows are skipped from the histograms.
+#include "radix.cuh"
+
+namespace ldf {
+namespace {
+
+constexpr int RT    = 256;
+constexpr int RI    = 8;
+constexpr int RTILE = RT * RI;
+constexpr int RW    = RT / 32;
+
+__device__ __forceinline__ uint64_t sort_word(const SortKeyDesc& k, int64_t row)
+{
+  const DCol& c = k.col;
+  if (!dvalid(c, row)) return 0;
+  uint64_t o;
+  switch (c.type) {
+    case LDF_INT8: o = static_cast<uint8_t>(static_cast<const int8_t*>(c.data)[row]) ^ 0x80u; break;
+    case LDF_INT16: o = static_cast<uint16_t>(static_cast<const int16_t*>(c.data)[row]) ^ 0x8000u; break;
+    case LDF_INT32: o = static_cast<uint32_t>(static_cast<const int32_t*>(c.data)[row]) ^ 0x80000000u; break;
+    case LDF_INT64:
+    case LDF_TIMESTAMP_US: o = static_cast<uint64_t>(static_cast<const int64_t*>(c.data)[row]) ^ (1ull << 63); break;
+    case LDF_FLOAT32: {
+      uint32_t b = static_cast<const uint32_t*>(c.data)[row];
+      if ((b & 0x7f800000u) == 0x7f800000u && (b & 0x007fffffu)) return 0;  // NaN: CLASS pass
+      if ((b & 0x7fffffffu) == 0) b = 0;                                    // -0.0 == 0.0
+      o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+      o &= 0xffffffffull;
+      break;
+    }
+    case LDF_FLOAT64: {
+      uint64_t b = static_cast<const uint64_t*>(c.data)[row];
+      if ((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull && (b & 0x000fffffffffffffull)) return 0;
+      if ((b & 0x7fffffffffffffffull) == 0) b = 0;
+      o = (b & (1ull << 63)) ? ~b : (b | (1ull << 63));
+      break;
+    }
+    default: o = dbits(c, row); break;  // unsigned, bool, string ranks (uint32)
+  }
+  if (k.descending) {
+    const uint64_t mask = k.key_bytes >= 8 ? ~0ull : ((1ull << (8 * k.key_bytes)) - 1);
+    o                   = ~o & mask;
+  }
+  return o;
+}
+
+// 0 = value, 1 = NaN, 2 = null when nulls_at_end; reversed otherwise
+// (Arrow places NaN next to the values and nulls outermost, either direction).
+__device__ __forceinline__ uint32_t class_digit(const SortKeyDesc& k, int64_t row)
+{
+  const DCol& c = k.col;
+  uint32_t cls  = 0;
+  if (!dvalid(c, row)) cls = 2;
+  else if (c.type == LDF_FLOAT64) {
+    uint64_t b = static_cast<const uint64_t*>(c.data)[row];
+    if ((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull && (b & 0x000fffffffffffffull)) cls = 1;
+  } else if (c.type == LDF_FLOAT32) {
+    uint32_t b = static_cast<const uint32_t*>(c.data)[row];
+    if ((b & 0x7f800000u) == 0x7f800000u && (b & 0x007fffffu)) cls = 1;
+  }
+  return k.nulls_at_end ? cls : 2 - cls;
+}
+
+__device__ __forceinline__ uint64_t bucket_word(const RadixPass& p, int64_t row)
+{
+  uint64_t h = 0x243f6a8885a308d3ull;
+  for (int j = 0; j < p.hash_keys.n; ++j) h = hash_combine64(h, hash_value(p.hash_keys.c[j], row));
+  return h % p.nparts;
+}
+
+__device__ __forceinline__ uint64_t pass_word(const RadixPass& p, int64_t row)
+{
+  if (p.src == DigitSrc::BUCKET) return bucket_word(p, row);
+  return sort_word(p.key, row);
+}
+
+__device__ __forceinline__ uint32_t pass_digit_of_row(const RadixPass& p, int64_t row)
+{
+  if (p.src == DigitSrc::CLASS) return class_digit(p.key, row);
+  return static_cast<uint32_t>(pass_word(p, row) >> p.shift) & 0xffu;
+}
+
+constexpr int kHistPassesPerLaunch = 16;
+struct HistArgs {
+  int npasses;
+  RadixPass p[kHistPassesPerLaunch];
+  int64_t n;
+  uint32_t* hist;  // [npasses][256]
+};
+
+__global__ void __launch_bounds__(RT) histogram_kernel(HistArgs a)
+{
+  __shared__ uint32_t sh[kHistPassesPerLaunch * 256];
+  for (int i = threadIdx.x; i < a.npasses * 256; i += RT) sh[i] = 0;
+  __syncthreads();
+  for (int64_t r = blockIdx.x * (int64_t)RT + threadIdx.x; r < a.n; r += (int64_t)gridDim.x * RT) {
+    for (int q = 0; q < a.npasses; ++q) atomicAdd(&sh[q * 256 + pass_digit_of_row(a.p[q], r)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < a.npasses * 256; i += RT)
+    if (sh[i]) atomicAdd(&a.hist[i], sh[i]);
+}
+
+struct PassArgs {
+  RadixPass p;
+  int64_t n;
+  const uint64_t* keys_in;
+  uint64_t* keys_out;
+  const int32_t* vals_in;  // null: identity
+  int32_t* vals_out;
+  const uint64_t* digit_base;  // [256]
+  uint64_t* status;            // [tiles * 256]
+  unsigned long long* counter;
+  int* err;
+};
+
+// GATHER: the word is loaded from the columns at the row (first pass of a
+// word); otherwise it is the carried key.  WRITE_KEYS: later passes of the same
+// word follow, so carry the word along.
+template <bool GATHER, bool WRITE_KEYS>
+__global__ void __launch_bounds__(RT) onesweep_kernel(PassArgs a)
+{
+  __shared__ uint32_t s_whist[RW][256];
+  __shared__ uint32_t s_tile_start[256];
+  __shared__ uint64_t s_gbase[256];
+  __shared__ uint64_t s_keys[WRITE_KEYS ? RTILE : 1];
+  __shared__ int32_t s_vals[RTILE];
+  __shared__ uint8_t s_dig[RTILE];
+  __shared__ uint32_t s_scan[RW + 1];
+  __shared__ int64_t s_tile;
+
+  const int64_t tile = next_tile_id(a.counter, &s_tile);
+  for (int i = threadIdx.x; i < RW * 256; i += RT) (&s_whist[0][0])[i] = 0;
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const int64_t tbase    = tile * RTILE;
+  uint64_t key[RI];
+  int32_t val[RI];
+  uint32_t dig[RI];
+  uint32_t lrank[RI];
+#pragma unroll
+  for (int i = 0; i < RI; ++i) {
+    const int64_t idx = tbase + warp * (32 * RI) + i * 32 + lane;
+    key[i]            = 0;
+    val[i]            = 0;
+    dig[i]            = 256;
+    if (idx < a.n) {
+      const int64_t row = a.vals_in ? a.vals_in[idx] : idx;
+      val[i]            = static_cast<int32_t>(row);
+      if (a.p.src == DigitSrc::CLASS) {
+        dig[i] = class_digit(a.p.key, row);
+      } else {
+        key[i] = GATHER ? pass_word(a.p, row) : a.keys_in[idx];
+        dig[i] = static_cast<uint32_t>(key[i] >> a.p.shift) & 0xffu;
+      }
+    }
+  }
+  // stable warp-level ranking, items in (i, lane) order
+#pragma unroll
+  for (int i = 0; i < RI; ++i) {
+    const uint32_t d     = dig[i];
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank  = __popc(peers & lt_mask);
+    uint32_t base        = 0;
+    if (d < 256) base = s_whist[warp][d];
+    __syncwarp();
+    if (d < 256 && rank == 0) s_whist[warp][d] = base + __popc(peers);
+    __syncwarp();
+    lrank[i] = base + rank;
+  }
+  __syncthreads();
+  // per-digit warp prefixes and tile counts (thread t owns digit t)
+  const int t = threadIdx.x;
+  uint32_t run = 0;
+#pragma unroll
+  for (int w = 0; w < RW; ++w) {
+    uint32_t c    = s_whist[w][t];
+    s_whist[w][t] = run;
+    run += c;
+  }
+  uint32_t tile_total;
+  const uint32_t start = block_exclusive_scan<uint32_t, RT>(run, s_scan, &tile_total);
+  s_tile_start[t]      = start;
+  // per-digit decoupled look-back
+  {
+    uint64_t* st = a.status;
+    uint64_t excl;
+    if (tile == 0) {
+      st_release_u64(&st[t], kFlagPrefix | run);
+      excl = 0;
+    } else {
+      st_release_u64(&st[tile * 256 + t], kFlagAgg | run);
+      excl          = 0;
+      int64_t j     = tile - 1;
+      uint32_t spins = 0;
+      while (j >= 0) {
+        uint64_t s = ld_volatile_u64(&st[j * 256 + t]);
+        uint64_t f = s & ~kValueMask;
+        if (f == 0) {
+          if (++spins > kSpinLimit) {
+            atomicExch(a.err, LDF_ERR_TIMEOUT);
+            break;
+          }
+          __nanosleep(32);
+          continue;
+        }
+        excl += s & kValueMask;
+        if (f == kFlagPrefix) break;
+        --j;
+      }
+      st_release_u64(&st[tile * 256 + t], kFlagPrefix | (excl + run));
+    }
+    s_gbase[t] = a.digit_base[t] + excl;
+  }
+  __syncthreads();
+  // stage the tile in digit order
+#pragma unroll
+  for (int i = 0; i < RI; ++i) {
+    const uint32_t d = dig[i];
+    if (d < 256) {
+      const uint32_t lp = s_tile_start[d] + s_whist[warp][d] + lrank[i];
+      if (WRITE_KEYS) s_keys[lp] = key[i];
+      s_vals[lp] = val[i];
+      s_dig[lp]  = static_cast<uint8_t>(d);
+    }
+  }
+  __syncthreads();
+  const int64_t cnt = a.n - tbase < RTILE ? a.n - tbase : RTILE;
+  for (int j = threadIdx.x; j < cnt; j += RT) {
+    const uint32_t d  = s_dig[j];
+    const int64_t pos = static_cast<int64_t>(s_gbase[d]) + (j - static_cast<int64_t>(s_tile_start[d]));
+    if (WRITE_KEYS) a.keys_out[pos] = s_keys[j];
+    a.vals_out[pos] = s_vals[j];
+  }
+}
+
+__global__ void iota_kernel(int32_t* p, int64_t n)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = static_cast<int32_t>(i);
+}
+
+unsigned hblocks(int64_t n)
+{
+  int64_t b   = ceil_div(n, RT);
+  int64_t cap = static_cast<int64_t>(num_sms()) * 4;
+  return static_cast<unsigned>(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+// Two passes belong to the same carried word when they read the same column
+// transform (or bucket) and differ only in shift.
+bool same_word(const RadixPass& a, const RadixPass& b)
+{
+  if (a.src != b.src || a.src == DigitSrc::CLASS) return false;
+  if (a.src == DigitSrc::BUCKET) return true;
+  return a.key.col.data == b.key.col.data && a.key.descending == b.key.descending;
+}
+
+}  // namespace
+
+void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
+                      uint32_t* d_hist)
+{
+  cudaStream_t s = ctx.stream();
+  LDF_CUDA(cudaMemsetAsync(d_hist, 0, passes.size() * 256 * sizeof(uint32_t), s));
+  for (size_t b = 0; b < passes.size(); b += kHistPassesPerLaunch) {
+    HistArgs h{};
+    h.npasses = static_cast<int>(std::min<size_t>(kHistPassesPerLaunch, passes.size() - b));
+    for (int q = 0; q < h.npasses; ++q) h.p[q] = passes[b + q];
+    h.n    = n;
+    h.hist = d_hist + b * 256;
+    if (n > 0) launch("histogram", histogram_kernel, hblocks(n), RT, 0, s, h);
+    LDF_CHECK_LAUNCH();
+  }
+}
+
+void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
+                     int32_t* perm, std::vector<uint32_t>* hist_out)
+{
+  const Allocator& al = ctx.alloc();
+  cudaStream_t s      = ctx.stream();
+  const size_t P      = passes.size();
+  std::vector<uint32_t> hist(P * 256, 0);
+  if (P > 0 && n > 0) {
+    Buffer<uint32_t> d_hist(al, P * 256);
+    radix_histograms(ctx, passes, n, d_hist.get());
+    LDF_CUDA(cudaMemcpyAsync(hist.data(), d_hist.get(), P * 256 * sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, s));
+    ctx.finish();
+  }
+  if (hist_out) *hist_out = hist;
+  // schedule: skip constant-digit passes; the first executed pass of a word
+  // gathers it, later passes of the same word read it carried
+  std::vector<int> run;
+  for (size_t q = 0; q < P; ++q) {
+    bool constant = false;
+    for (int d = 0; d < 256; ++d)
+      if (hist[q * 256 + d] == static_cast<uint32_t>(n)) constant = true;
+    if (!constant && n > 0) run.push_back(static_cast<int>(q));
+  }
+  if (run.empty()) {
+    if (n > 0) launch("iota", iota_kernel, hblocks(n), RT, 0, s, perm, n);
+    LDF_CHECK_LAUNCH();
+    return;
+  }
+  std::vector<uint64_t> bases(run.size() * 256);
+  for (size_t k = 0; k < run.size(); ++k) {
+    uint64_t acc = 0;
+    for (int d = 0; d < 256; ++d) {
+      bases[k * 256 + d] = acc;
+      acc += hist[run[k] * 256 + d];
+    }
+  }
+  Buffer<uint64_t> d_bases(al, bases.size());
+  LDF_CUDA(cudaMemcpyAsync(d_bases.get(), bases.data(), bases.size() * 8, cudaMemcpyHostToDevice, s));
+
+  const int64_t tiles = ceil_div(n, RTILE);
+  Buffer<uint64_t> status(al, tiles * 256 + 2);
+  Buffer<uint64_t> keys[2] = {Buffer<uint64_t>(al, n), Buffer<uint64_t>(al, n)};
+  Buffer<int32_t> vals_tmp(al, n);
+  // ping-pong so that the last pass writes into `perm`
+  int32_t* vbuf[2];
+  const bool odd = run.size() % 2 == 1;
+  vbuf[0]        = odd ? perm : vals_tmp.get();
+  vbuf[1]        = odd ? vals_tmp.get() : perm;
+  const int32_t* vin = nullptr;
+  const uint64_t* kin = nullptr;
+  for (size_t k = 0; k < run.size(); ++k) {
+    const RadixPass& p = passes[run[k]];
+    const bool gather  = k == 0 || !same_word(passes[run[k - 1]], p);
+    const bool write_keys = p.src != DigitSrc::CLASS && k + 1 < run.size() && same_word(p, passes[run[k + 1]]);
+    LDF_CUDA(cudaMemsetAsync(status.get(), 0, (tiles * 256 + 2) * 8, s));
+    PassArgs a{};
+    a.p          = p;
+    a.n          = n;
+    a.keys_in    = kin;
+    a.keys_out   = keys[k % 2].get();
+    a.vals_in    = vin;
+    a.vals_out   = vbuf[k % 2];
+    a.digit_base = d_bases.get() + k * 256;
+    a.status     = status.get();
+    a.counter    = reinterpret_cast<unsigned long long*>(status.get() + tiles * 256);
+    a.err        = ctx.err();
+    const unsigned g = static_cast<unsigned>(tiles);
+    if (gather && write_keys) launch("onesweep", onesweep_kernel<true, true>, g, RT, 0, s, a);
+    else if (gather) launch("onesweep", onesweep_kernel<true, false>, g, RT, 0, s, a);
+    else if (write_keys) launch("onesweep", onesweep_kernel<false, true>, g, RT, 0, s, a);
+    else launch("onesweep", onesweep_kernel<false, false>, g, RT, 0, s, a);
+    LDF_CHECK_LAUNCH();
+    vin = vbuf[k % 2];
+    kin = keys[k % 2].get();
+  }
+}
+
+}  // namespace ldf

@@ -1,0 +1,51 @@
+// Onesweep-style LSD radix sort of (key, row) pairs with 8-bit digits, used by
+// `sort` (multi-key, stable) and by `hash_partition` (stable bucket order).
+#pragma once
+
+#include "table_ops.cuh"
+
+namespace ldf {
+
+// How a pass obtains the digit of a row.
+enum class DigitSrc : int {
+  CARRIED = 0,  // byte `shift/8` of the carried key word
+  COLUMN  = 1,  // load the key column at the row, transform, then byte
+  CLASS   = 2,  // 0/1/2 class of the row: value / NaN / null, ordered by nulls_at_end
+  BUCKET  = 3   // hash of the key columns % nparts (then byte)
+};
+
+// Value transform of one sort key column into an order-preserving unsigned
+// word (ascending), inverted for descending; null and NaN rows give 0 (their
+// order comes from the CLASS pass).
+struct SortKeyDesc {
+  DCol col;
+  int descending;
+  int nulls_at_end;
+  int key_bytes;  // bytes of the transformed word (1..8)
+};
+
+struct RadixPass {
+  DigitSrc src;
+  int shift;  // bit offset of the digit in the key word
+  SortKeyDesc key;
+  KeyCols hash_keys;  // BUCKET
+  uint32_t nparts;    // BUCKET
+};
+
+// Stable sort of rows by a list of passes (least significant first).
+// Returns the permutation (row ids) in `perm` (n entries, caller allocated).
+// `hist_only` variants are used by the planner.
+struct RadixPlan {
+  std::vector<RadixPass> passes;  // in execution order (LS first)
+};
+
+// Upfront digit histograms of every candidate pass: hist[p * 256 + d].
+void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
+                      uint32_t* d_hist);
+
+// Run the passes; `perm` receives the row order.  Passes whose histogram has a
+// single bucket holding every row are skipped.
+void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
+                     int32_t* perm, std::vector<uint32_t>* hist_out = nullptr);
+
+}  // namespace ldf

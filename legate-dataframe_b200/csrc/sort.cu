@@ -1,0 +1,361 @@
+// sort (stable, multi-key) and the local hash_partition.
+//
+// sort: reference SortTask::gpu_variant (cpp/src/sort.cu:295-379): keys in
+// order, per-key ascending/descending, `nulls_at_end` for every key regardless
+// of direction (the null-precedence flip of sort.cu:309-323, which makes the
+// GPU agree with Arrow SortIndices, sort.cpp:324-342), head/tail `limit`
+// (apply_limit, sort.cu:275-291).  The radix sort is stable, so `stable=false`
+// returns the stable order too.
+//
+// String keys are replaced by their dense rank among the distinct strings
+// (bytewise order, shorter prefix first): distinct strings come from a hash
+// table, are ranked by repeated stable radix passes over 8-byte big-endian
+// chunks (rank of the previous chunks as the major key), and every row then
+// sorts on the uint32 rank.
+//
+// hash_partition: reference task::repartition_by_hash local step
+// (cpp/src/core/repartition_by_hash.cu:296-310): bucket = hash(keys) % nparts,
+// rows grouped by bucket, start offsets returned; here one stable radix pass
+// on the bucket id (two for more than 256 buckets) then one gather.
+#include "radix.cuh"
+
+namespace ldf {
+namespace {
+
+constexpr uint64_t kEmpty = ~0ull;
+
+// ---- string ranking --------------------------------------------------------
+__global__ void str_find_insert_kernel(DCol col, int64_t n, unsigned long long* slots, uint64_t cap,
+                                       int32_t* row_slot, int* overflow)
+{
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if (!dvalid(col, r)) {
+      row_slot[r] = -1;
+      continue;
+    }
+    const uint64_t h     = hash_bytes(dstr_ptr(col, r), dstr_len(col, r));
+    const uint64_t entry = (static_cast<uint64_t>(r) << 32) | static_cast<uint32_t>(h);
+    uint64_t idx         = fastrange(h, cap);
+    int64_t found        = -1;
+    for (int probe = 0; probe < 4096; ++probe) {
+      uint64_t v = slots[idx];
+      if (v == kEmpty) {
+        v = atomicCAS(&slots[idx], kEmpty, entry);
+        if (v == kEmpty) {
+          found = static_cast<int64_t>(idx);
+          break;
+        }
+      }
+      if (static_cast<uint32_t>(v) == static_cast<uint32_t>(h) &&
+          values_equal(col, r, col, static_cast<int64_t>(v >> 32))) {
+        found = static_cast<int64_t>(idx);
+        break;
+      }
+      idx = idx + 1 == cap ? 0 : idx + 1;
+    }
+    if (found < 0) atomicExch(overflow, 1);
+    row_slot[r] = static_cast<int32_t>(found);
+  }
+}
+
+// slot -> dense distinct id; distinct id -> representative row
+__global__ void str_compact_kernel(const unsigned long long* slots, uint64_t cap, int32_t* slot_id,
+                                   int32_t* repr, unsigned long long* count)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < static_cast<int64_t>(cap);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t v = slots[i];
+    if (v == kEmpty) continue;
+    unsigned long long d = atomicAdd(count, 1ull);  // order is irrelevant: ids get sorted
+    slot_id[i]           = static_cast<int32_t>(d);
+    repr[d]              = static_cast<int32_t>(v >> 32);
+  }
+}
+
+// chunk c (8 bytes, big-endian, zero padded) of each distinct string
+__global__ void str_chunk_kernel(DCol col, const int32_t* repr, int64_t D, int chunk, uint64_t* out,
+                                 uint32_t* lens)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < D; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r   = repr[i];
+    const int64_t len = dstr_len(col, r);
+    const uint8_t* p  = dstr_ptr(col, r);
+    uint64_t w        = 0;
+    for (int b = 0; b < 8; ++b) {
+      int64_t o = static_cast<int64_t>(chunk) * 8 + b;
+      w         = (w << 8) | (o < len ? p[o] : 0);
+    }
+    out[i] = w;
+    if (lens) lens[i] = static_cast<uint32_t>(len);
+  }
+}
+
+// new rank = number of (prev rank, word) changes along the sorted order
+__global__ void rank_flags_kernel(const int32_t* perm, int64_t D, const uint32_t* prev, const uint64_t* word,
+                                  uint32_t* flags)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < D; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i == 0) {
+      flags[0] = 0;
+      continue;
+    }
+    const int32_t a = perm[i - 1], b = perm[i];
+    flags[i] = (prev[a] != prev[b] || word[a] != word[b]) ? 1u : 0u;
+  }
+}
+__global__ void rank_scatter_kernel(const int32_t* perm, int64_t D, const int64_t* scanned, const uint32_t* flags,
+                                    uint32_t* rank)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < D; i += (int64_t)gridDim.x * blockDim.x)
+    rank[perm[i]] = static_cast<uint32_t>(scanned[i] + flags[i]);
+}
+__global__ void row_rank_kernel(const int32_t* row_slot, const int32_t* slot_id, const uint32_t* rank, int64_t n,
+                                uint32_t* out)
+{
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    int32_t s = row_slot[r];
+    out[r]    = s >= 0 ? rank[slot_id[s]] : 0u;
+  }
+}
+__global__ void max_len_kernel(DCol col, const int32_t* repr, int64_t D, unsigned long long* out)
+{
+  unsigned long long m = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < D; i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, static_cast<unsigned long long>(dstr_len(col, repr[i])));
+  for (int d = 16; d > 0; d >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, d));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+unsigned blocks_for(int64_t n)
+{
+  int64_t b   = ceil_div(n, 256);
+  int64_t cap = static_cast<int64_t>(num_sms()) * 8;
+  return static_cast<unsigned>(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+DCol u32_col(const uint32_t* p)
+{
+  DCol d{};
+  d.data  = p;
+  d.type  = LDF_UINT32;
+  d.width = 4;
+  return d;
+}
+DCol u64_col(const uint64_t* p)
+{
+  DCol d{};
+  d.data  = p;
+  d.type  = LDF_UINT64;
+  d.width = 8;
+  return d;
+}
+
+void add_word_passes(std::vector<RadixPass>& v, const SortKeyDesc& k)
+{
+  for (int b = 0; b < k.key_bytes; ++b) {
+    RadixPass p{};
+    p.src   = DigitSrc::COLUMN;
+    p.shift = 8 * b;
+    p.key   = k;
+    v.push_back(p);
+  }
+}
+
+}  // namespace
+
+// Dense bytewise rank of every row's string (nulls get 0; they are ordered
+// by the CLASS pass).  `out` has n entries.
+void string_ranks(const OpContext& ctx, const DCol& col, int64_t n, uint32_t* out)
+{
+  const Allocator& al = ctx.alloc();
+  cudaStream_t s      = ctx.stream();
+  if (n == 0) return;
+  uint64_t cap = static_cast<uint64_t>(2 * n + 64);
+  Buffer<unsigned long long> slots(al, cap);
+  Buffer<int32_t> row_slot(al, n);
+  Buffer<int64_t> misc(al, 4);
+  LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, cap * 8, s));
+  LDF_CUDA(cudaMemsetAsync(misc.get(), 0, 32, s));
+  int* overflow              = reinterpret_cast<int*>(misc.get());
+  unsigned long long* dcount = reinterpret_cast<unsigned long long*>(misc.get() + 1);
+  unsigned long long* maxlen = reinterpret_cast<unsigned long long*>(misc.get() + 2);
+  launch("str_find_insert", str_find_insert_kernel, blocks_for(n), 256, 0, s, col, n, slots.get(), cap, row_slot.get(), overflow);
+  LDF_CHECK_LAUNCH();
+  Buffer<int32_t> slot_id(al, cap);
+  Buffer<int32_t> repr(al, n);
+  launch("str_compact", str_compact_kernel, blocks_for(cap), 256, 0, s, slots.get(), cap, slot_id.get(), repr.get(), dcount);
+  LDF_CHECK_LAUNCH();
+  int64_t h[3];
+  LDF_CUDA(cudaMemcpyAsync(h, misc.get(), 24, cudaMemcpyDeviceToHost, s));
+  ctx.finish();
+  if (h[0] != 0) fail(LDF_ERR_INTERNAL, "string dictionary overflow");
+  const int64_t D = h[1];
+  Buffer<uint32_t> rank(al, std::max<int64_t>(D, 1));
+  if (D > 0) {
+    launch("max_len", max_len_kernel, blocks_for(D), 256, 0, s, col, repr.get(), D, maxlen);
+    LDF_CHECK_LAUNCH();
+    const int64_t L = ctx.read_i64(misc.get() + 2);
+    LDF_CUDA(cudaMemsetAsync(rank.get(), 0, D * 4, s));
+    Buffer<uint64_t> word(al, D);
+    Buffer<uint32_t> lens(al, D);
+    Buffer<int32_t> perm(al, D);
+    Buffer<uint32_t> flags(al, D);
+    Buffer<int64_t> scanned(al, D);
+    Buffer<int64_t> total(al, 1);
+    const int nchunks = static_cast<int>((L + 7) / 8);
+    // chunks, then the length as the final tie-break (shorter prefix first)
+    for (int c = 0; c <= nchunks; ++c) {
+      if (c < nchunks) {
+        launch("str_chunk", str_chunk_kernel, blocks_for(D), 256, 0, s, col, repr.get(), D, c, word.get(), nullptr);
+      } else {
+        launch("str_chunk", str_chunk_kernel, blocks_for(D), 256, 0, s, col, repr.get(), D, 0, word.get(), lens.get());
+        // word := length (zero-extended)
+        LDF_CUDA(cudaMemsetAsync(word.get(), 0, D * 8, s));
+        LDF_CUDA(cudaMemcpy2DAsync(word.get(), 8, lens.get(), 4, 4, D, cudaMemcpyDeviceToDevice, s));
+      }
+      LDF_CHECK_LAUNCH();
+      std::vector<RadixPass> passes;
+      SortKeyDesc wk{u64_col(word.get()), 0, 1, 8};
+      SortKeyDesc rk{u32_col(rank.get()), 0, 1, 4};
+      add_word_passes(passes, wk);
+      add_word_passes(passes, rk);
+      radix_sort_rows(ctx, passes, D, perm.get());
+      launch("rank_flags", rank_flags_kernel, blocks_for(D), 256, 0, s, perm.get(), D, rank.get(), word.get(), flags.get());
+      LDF_CHECK_LAUNCH();
+      exclusive_scan_u32(flags.get(), scanned.get(), D, total.get(), ctx);
+      launch("rank_scatter", rank_scatter_kernel, blocks_for(D), 256, 0, s, perm.get(), D, scanned.get(), flags.get(), rank.get());
+      LDF_CHECK_LAUNCH();
+      const int64_t ndistinct_ranks = ctx.read_i64(total.get()) + 1;
+      if (ndistinct_ranks == D) break;
+    }
+  }
+  launch("row_rank", row_rank_kernel, blocks_for(n), 256, 0, s, row_slot.get(), slot_id.get(), rank.get(), n, out);
+  LDF_CHECK_LAUNCH();
+}
+
+void gather_table(const OpContext& ctx, const ldf_column* table, int ncols, const int32_t* map, int64_t rows,
+                  ldf_column* out)
+{
+  for (int j = 0; j < ncols; ++j) {
+    const ldf_column& c = table[j];
+    out[j]              = alloc_out_column(ctx.alloc(), c.type, rows, c.valid != nullptr);
+    if (c.type == LDF_STRING) gather_strings(ctx, make_dcol(c), map, rows, out[j]);
+    else gather_fixed(ctx, make_dcol(c), map, rows, out[j]);
+  }
+}
+
+void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const uint8_t* ascending, int nkeys,
+                bool nulls_at_end, int64_t limit, ldf_column* out, const OpContext& ctx)
+{
+  if (nkeys < 1) fail(LDF_ERR_INVALID_ARGUMENT, "must sort along at least one column");
+  for (int j = 0; j < nkeys; ++j) {
+    LDF_REQUIRE(keys[j] >= 0 && keys[j] < ncols, "sort key column out of range");
+    for (int q = 0; q < j; ++q) LDF_REQUIRE(keys[q] != keys[j], "duplicate sort keys");
+  }
+  const Allocator& al = ctx.alloc();
+  const int64_t n     = ncols > 0 ? table[0].size : 0;
+  LDF_REQUIRE(n < (int64_t(1) << 31), "tables of 2^31 rows or more per task are not supported");
+  std::vector<Buffer<uint32_t>> ranks;
+  std::vector<RadixPass> passes;
+  // least significant key first
+  for (int j = nkeys - 1; j >= 0; --j) {
+    const ldf_column& c = table[keys[j]];
+    SortKeyDesc k{};
+    k.col          = make_dcol(c);
+    k.descending   = ascending[j] ? 0 : 1;
+    k.nulls_at_end = nulls_at_end ? 1 : 0;
+    if (c.type == LDF_STRING) {
+      ranks.emplace_back(al, std::max<int64_t>(n, 1));
+      string_ranks(ctx, k.col, n, ranks.back().get());
+      DCol rc  = u32_col(ranks.back().get());
+      rc.valid = c.valid;
+      k.col    = rc;
+    }
+    k.key_bytes = k.col.width;
+    add_word_passes(passes, k);
+    if (c.valid != nullptr || is_float(c.type)) {
+      RadixPass p{};
+      p.src = DigitSrc::CLASS;
+      p.key = k;
+      passes.push_back(p);
+    }
+  }
+  Buffer<int32_t> perm(al, std::max<int64_t>(n, 1));
+  radix_sort_rows(ctx, passes, n, perm.get());
+  int64_t first = 0, rows = n;
+  if (limit != INT64_MIN && (limit < 0 ? -limit : limit) < n) {
+    if (limit < 0) {
+      first = n + limit;
+      rows  = -limit;
+    } else {
+      rows = limit;
+    }
+  }
+  gather_table(ctx, table, ncols, perm.get() + first, rows, out);
+  ctx.finish();
+}
+
+namespace {
+__global__ void bucket_count_kernel(KeyCols k, int64_t n, uint32_t nparts, unsigned long long* counts)
+{
+  extern __shared__ unsigned int sc[];
+  const bool use_smem = nparts <= 8192;
+  if (use_smem)
+    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) sc[i] = 0;
+  __syncthreads();
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t h = 0x243f6a8885a308d3ull;
+    for (int j = 0; j < k.n; ++j) h = hash_combine64(h, hash_value(k.c[j], r));
+    uint32_t b = static_cast<uint32_t>(h % nparts);
+    if (use_smem) atomicAdd(&sc[b], 1u);
+    else atomicAdd(&counts[b], 1ull);
+  }
+  __syncthreads();
+  if (use_smem)
+    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x)
+      if (sc[i]) atomicAdd(&counts[i], static_cast<unsigned long long>(sc[i]));
+}
+}  // namespace
+
+void hash_partition(const ldf_column* table, int ncols, const int32_t* keys, int nkeys, int nparts,
+                    ldf_column* out, int64_t* offsets, const OpContext& ctx)
+{
+  LDF_REQUIRE(nparts >= 1, "nparts must be positive");
+  KeyCols k       = make_keys(table, ncols, keys, nkeys);
+  const int64_t n = ncols > 0 ? table[0].size : 0;
+  LDF_REQUIRE(n < (int64_t(1) << 31), "tables of 2^31 rows or more per task are not supported");
+  const Allocator& al = ctx.alloc();
+  cudaStream_t s      = ctx.stream();
+  std::vector<RadixPass> passes;
+  for (uint64_t span = 1, shift = 0; span < static_cast<uint64_t>(nparts); span <<= 8, shift += 8) {
+    RadixPass p{};
+    p.src       = DigitSrc::BUCKET;
+    p.shift     = static_cast<int>(shift);
+    p.hash_keys = k;
+    p.nparts    = static_cast<uint32_t>(nparts);
+    passes.push_back(p);
+  }
+  Buffer<int32_t> perm(al, std::max<int64_t>(n, 1));
+  radix_sort_rows(ctx, passes, n, perm.get());
+  // bucket sizes
+  Buffer<unsigned long long> counts(al, nparts);
+  LDF_CUDA(cudaMemsetAsync(counts.get(), 0, static_cast<size_t>(nparts) * 8, s));
+  if (n > 0) {
+    size_t smem = nparts <= 8192 ? static_cast<size_t>(nparts) * 4 : 0;
+    launch("bucket_count", bucket_count_kernel, blocks_for(n), 256, smem, s, k, n, static_cast<uint32_t>(nparts), counts.get());
+    LDF_CHECK_LAUNCH();
+  }
+  std::vector<unsigned long long> h(nparts);
+  LDF_CUDA(cudaMemcpyAsync(h.data(), counts.get(), static_cast<size_t>(nparts) * 8, cudaMemcpyDeviceToHost, s));
+  gather_table(ctx, table, ncols, perm.get(), n, out);
+  ctx.finish();
+  int64_t acc = 0;
+  for (int b = 0; b < nparts; ++b) {
+    offsets[b] = acc;
+    acc += static_cast<int64_t>(h[b]);
+  }
+  offsets[nparts] = acc;
+}
+
+}  // namespace ldf

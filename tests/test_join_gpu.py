@@ -1,0 +1,123 @@
+"""Parity of the sm_100a hash join (through the C ABI) with the oracle and
+the golden vectors: every join type, nulls_equal both ways, int/float/string
+and multi-column keys, duplicates, empty tables, and the single-pass (unique
+build keys) and two-pass (repeated build keys) probe paths."""
+
+import zlib
+
+import numpy as np
+import pyarrow as pa
+import pytest
+
+from ldf_testing import assert_tables_equal, load_golden
+from oracle import relational as R
+
+pytestmark = pytest.mark.gpu
+
+HOW = {"inner": 0, "left": 1, "full": 2, "semi": 3, "anti": 4}
+JOIN_CASES = [c for c in load_golden() if c["op"] == "join"]
+
+
+def run_join(lhs, rhs, lk, rk, how, nulls_equal=True, lo=None, ro=None):
+    from legate_dataframe import LogicalTable
+    from legate_dataframe.lib.join import JoinType, join
+
+    res = join(LogicalTable.from_arrow(lhs), LogicalTable.from_arrow(rhs), lhs_keys=lk, rhs_keys=rk,
+               join_type=JoinType(HOW[how]), lhs_out_columns=lo, rhs_out_columns=ro, nulls_equal=nulls_equal)
+    return res.to_arrow()
+
+
+@pytest.mark.parametrize("case", JOIN_CASES, ids=[c["name"] for c in JOIN_CASES])
+def test_join_golden(case):
+    t = case["tables"]
+    res = run_join(t["lhs"], t["rhs"], case["lhs_keys"], case["rhs_keys"], case["how"], case["nulls_equal"],
+                   case["lhs_out"], case["rhs_out"])
+    assert_tables_equal(res, t["expected"], check_types=False)
+
+
+def _keys(rng, n, kind, key_range, null_p):
+    mask = rng.random(n) < null_p if null_p else None
+    if kind == "string":
+        v = [f"key-{x:05d}" * (1 + x % 3) for x in rng.integers(0, key_range, n)]
+        if mask is not None:
+            v = [None if m else s for s, m in zip(v, mask)]
+        return pa.array(v, pa.string())
+    if kind.startswith("float"):
+        return pa.array(rng.integers(0, key_range, n).astype(kind), mask=mask)
+    return pa.array(rng.integers(0, key_range, n).astype(kind), mask=mask)
+
+
+@pytest.mark.parametrize("how", list(HOW))
+@pytest.mark.parametrize("nulls_equal", [True, False])
+@pytest.mark.parametrize("kind", ["int32", "int64", "float64", "string", "uint8"])
+def test_join_random_parity(how, nulls_equal, kind):
+    rng = np.random.default_rng(zlib.crc32(f"{how}{nulls_equal}{kind}".encode()))
+    nl, nr = 3000, 2000
+    kr = 200 if kind != "uint8" else 50
+    lhs = pa.table({"lk": _keys(rng, nl, kind, kr, 0.05), "lp": pa.array(rng.normal(size=nl), mask=rng.random(nl) < .1),
+                    "ls": pa.array([f"l{i}" for i in range(nl)])})
+    rhs = pa.table({"rk": _keys(rng, nr, kind, kr, 0.05), "rp": rng.integers(-9, 9, nr).astype(np.int16),
+                    "rb": pa.array(rng.random(nr) < 0.5)})
+    res = run_join(lhs, rhs, ["lk"], ["rk"], how, nulls_equal)
+    exp = R.join(lhs, rhs, ["lk"], ["rk"], how, nulls_equal)
+    assert_tables_equal(res, exp)
+
+
+@pytest.mark.parametrize("how", list(HOW))
+def test_join_multikey(how):
+    rng = np.random.default_rng(7)
+    n = 4000
+    lhs = pa.table({"a": _keys(rng, n, "int32", 20, 0.05), "b": _keys(rng, n, "string", 15, 0.05),
+                    "v": np.arange(n)})
+    rhs = pa.table({"c": _keys(rng, n // 2, "int32", 20, 0.05), "d": _keys(rng, n // 2, "string", 15, 0.05),
+                    "w": np.arange(n // 2) * 3})
+    for ne in (True, False):
+        res = run_join(lhs, rhs, ["a", "b"], ["c", "d"], how, ne)
+        exp = R.join(lhs, rhs, ["a", "b"], ["c", "d"], how, ne)
+        assert_tables_equal(res, exp)
+
+
+@pytest.mark.parametrize("how", ["inner", "left", "full"])
+def test_join_unique_build_single_pass(how):
+    # unique build keys take the one-pass probe with look-back offsets
+    rng = np.random.default_rng(3)
+    nb, npb = 300_000, 1_000_000
+    bk = rng.permutation(nb).astype(np.int32)
+    pk = np.where(rng.random(npb) < 0.8, rng.integers(0, nb, npb), rng.integers(nb, 2 * nb, npb)).astype(np.int32)
+    rhs = pa.table({"k": bk, "p0": rng.integers(-2**40, 2**40, nb), "p1": rng.integers(-2**40, 2**40, nb)})
+    lhs = pa.table({"k": pa.array(pk, mask=rng.random(npb) < 0.05), "x": rng.random(npb)})
+    res = run_join(lhs, rhs, ["k"], ["k"], how, True, ["k", "x"], ["p0", "p1"])
+    exp = R.join(lhs, rhs, ["k"], ["k"], how, True, ["k", "x"], ["p0", "p1"])
+    assert_tables_equal(res, exp)
+
+
+def test_join_config0_shape():
+    # the reference benchmark shape: 1M x 1M int64 keys U[0, 2^20), seeds 1 and 2
+    l_rng, r_rng = np.random.default_rng(1), np.random.default_rng(2)
+    n = 1_000_000
+    lhs = pa.table({"key": l_rng.integers(0, 1 << 20, n), "payload": l_rng.integers(-2**40, 2**40, n)})
+    rhs = pa.table({"key": r_rng.integers(0, 1 << 20, n), "payload_r": r_rng.integers(-2**40, 2**40, n)})
+    res = run_join(lhs, rhs, ["key"], ["key"], "inner")
+    exp = R.join(lhs, rhs, ["key"], ["key"], "inner")
+    assert res.num_rows == exp.num_rows
+    assert_tables_equal(res, exp)
+
+
+@pytest.mark.parametrize("how", list(HOW))
+def test_join_empty(how):
+    e = pa.table({"k": pa.array([], pa.int64()), "v": pa.array([], pa.float64())})
+    f = pa.table({"k": pa.array([1, 2, 2], pa.int64()), "w": pa.array([1.0, 2.0, 3.0])})
+    for lhs, rhs in ((e, f), (f.rename_columns(["k", "v"]), e.rename_columns(["k", "w"])), (e, e.rename_columns(["k", "w"]))):
+        res = run_join(lhs, rhs, ["k"], ["k"], how)
+        exp = R.join(lhs, rhs, ["k"], ["k"], how)
+        assert_tables_equal(res, exp)
+
+
+def test_join_all_null_keys():
+    lhs = pa.table({"k": pa.array([None] * 5, pa.int32()), "v": np.arange(5)})
+    rhs = pa.table({"k": pa.array([None, 1, None], pa.int32()), "w": np.arange(3)})
+    for how in HOW:
+        for ne in (True, False):
+            res = run_join(lhs, rhs, ["k"], ["k"], how, ne)
+            exp = R.join(lhs, rhs, ["k"], ["k"], how, ne)
+            assert_tables_equal(res, exp)

@@ -1,0 +1,130 @@
+"""Pin the CPU oracle: against the reference's golden vectors / known answers
+and against the reference's own CPU path (Arrow Acero / SortIndices) on
+seeded inputs.  CPU only."""
+
+import numpy as np
+import pyarrow as pa
+import pyarrow.compute as pc
+import pytest
+
+from ldf_testing import agg_spec, assert_tables_equal, load_golden
+from oracle import arrow_ref as A
+from oracle import relational as R
+
+CASES = list(load_golden())
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["op"] + ":" + c["name"] for c in CASES])
+def test_oracle_matches_golden(case):
+    t = case["tables"]
+    if case["op"] == "join":
+        res = R.join(t["lhs"], t["rhs"], case["lhs_keys"], case["rhs_keys"], case["how"], case["nulls_equal"],
+                     case["lhs_out"], case["rhs_out"])
+        assert_tables_equal(res, t["expected"], check_types=False)
+    elif case["op"] == "groupby":
+        res = R.groupby(t["table"], case["keys"], agg_spec(case["aggs"]))
+        assert_tables_equal(res, t["expected"], sort_by=case["keys"], rtol=1e-12)
+    else:
+        res = R.sort(t["table"], case["keys"], case["ascending"], case["nulls_at_end"], case["limit"])
+        assert_tables_equal(res, t["expected"], sort_by=None)
+
+
+def _random_table(rng, n, key_type, null_p, nkeys=1, prefix="k", key_range=50):
+    cols = {}
+    for j in range(nkeys):
+        mask = rng.random(n) < null_p if null_p else None
+        if key_type == "string":
+            vals = [f"s{v}" for v in rng.integers(0, key_range, n)]
+            cols[f"{prefix}{j}"] = pa.array([None if (mask is not None and m) else v for v, m in
+                                            zip(vals, mask if mask is not None else [False] * n)], pa.string())
+        else:
+            vals = rng.integers(0, key_range, n).astype(key_type)
+            cols[f"{prefix}{j}"] = pa.array(vals, mask=mask)
+    cols[prefix + "_pay"] = pa.array(rng.normal(size=n), mask=rng.random(n) < 0.1)
+    cols[prefix + "_ipay"] = pa.array(rng.integers(-1000, 1000, n).astype(np.int32))
+    return pa.table(cols)
+
+
+@pytest.mark.parametrize("how", ["inner", "left", "full", "semi", "anti"])
+@pytest.mark.parametrize("nulls_equal", [True, False])
+@pytest.mark.parametrize("key_type", ["int32", "int64", "string"])
+@pytest.mark.parametrize("nkeys", [1, 2])
+def test_oracle_join_vs_arrow(how, nulls_equal, key_type, nkeys):
+    rng = np.random.default_rng(11 + nkeys)
+    lhs = _random_table(rng, 300, key_type, 0.1, nkeys, "l", 40)
+    rhs = _random_table(rng, 200, key_type, 0.1, nkeys, "r", 40)
+    lk = [f"l{j}" for j in range(nkeys)]
+    rk = [f"r{j}" for j in range(nkeys)]
+    exp = A.join(lhs, rhs, lk, rk, how, nulls_equal)
+    res = R.join(lhs, rhs, lk, rk, how, nulls_equal)
+    assert_tables_equal(res, exp, check_types=False)
+
+
+@pytest.mark.parametrize("key_type", ["int64", "string", "float32"])
+def test_oracle_groupby_vs_arrow(key_type):
+    rng = np.random.default_rng(5)
+    n = 2000
+    t = _random_table(rng, n, key_type if key_type != "float32" else "int64", 0.05, 2, "k", 12)
+    if key_type == "float32":
+        t = t.set_column(0, "k0", pc.cast(t.column("k0"), pa.float32()))
+    aggs = [("k_pay", "sum", "s"), ("k_pay", "mean", "m"), ("k_pay", "count", "c"), (None, "count_all", "ca"),
+            ("k_ipay", "min", "mn"), ("k_ipay", "max", "mx"), ("k_ipay", "count_distinct", "nd"),
+            ("k_pay", ("count", pc.CountOptions(mode="all")), "call"),
+            ("k_pay", ("count", pc.CountOptions(mode="only_null")), "cnull"),
+            ("k_ipay", ("count_distinct", pc.CountOptions(mode="all")), "ndall"), ("k_ipay", "sum", "isum")]
+    exp = A.groupby(t, ["k0", "k1"], aggs)
+    res = R.groupby(t, ["k0", "k1"], aggs)
+    assert_tables_equal(res, exp, sort_by=["k0", "k1"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("nulls_at_end", [True, False])
+@pytest.mark.parametrize("asc", [[True, True, True], [False, True, False], [True, False, True]])
+def test_oracle_sort_vs_arrow(nulls_at_end, asc):
+    rng = np.random.default_rng(3)
+    n = 3000
+    t = pa.table({
+        "a": pa.array(rng.integers(0, 20, n), mask=rng.random(n) < 0.1),
+        "b": pa.array(rng.integers(0, 5, n).astype(np.float64), mask=rng.random(n) < 0.1),
+        "c": pa.array([None if m else f"x{v}" for v, m in zip(rng.integers(0, 30, n), rng.random(n) < 0.1)]),
+        "idx": np.arange(n),
+    })
+    keys = ["c", "a", "b"]
+    exp = A.sort(t, keys, asc, nulls_at_end)
+    res = R.sort(t, keys, asc, nulls_at_end)
+    assert_tables_equal(res, exp, sort_by=None)
+
+
+def test_oracle_partition_properties():
+    rng = np.random.default_rng(9)
+    n = 5000
+    t = pa.table({"k": pa.array(rng.integers(0, 300, n), mask=rng.random(n) < 0.05),
+                  "s": [f"v{v}" for v in rng.integers(0, 100, n)], "i": np.arange(n)})
+    out, offsets, bucket = R.hash_partition(t, ["k", "s"], 16)
+    assert offsets[0] == 0 and offsets[-1] == n
+    # permutation of the input, stable within buckets, equal keys in one bucket
+    idx = np.asarray(out.column("i"))
+    assert sorted(idx.tolist()) == list(range(n))
+    for b in range(16):
+        seg = idx[offsets[b]:offsets[b + 1]]
+        assert np.all(np.diff(seg) > 0)
+        assert np.all(bucket[seg] == b)
+    keys = list(zip(t.column("k").to_pylist(), t.column("s").to_pylist()))
+    seen = {}
+    for i, kk in enumerate(keys):
+        assert seen.setdefault(kk, bucket[i]) == bucket[i]
+
+
+def test_oracle_hash_known_answers():
+    # MurmurHash3 fmix64 of small integers (independent big-int restatement)
+    def fmix(x):
+        m = (1 << 64) - 1
+        x ^= x >> 33
+        x = (x * 0xFF51AFD7ED558CCD) & m
+        x ^= x >> 33
+        x = (x * 0xC4CEB9FE1A85EC53) & m
+        x ^= x >> 33
+        return x
+
+    xs = np.array([0, 1, 2, 12345, (1 << 64) - 1], dtype=np.uint64)
+    got = R._mix64(xs)
+    assert [int(g) for g in got] == [fmix(int(x)) for x in xs]
