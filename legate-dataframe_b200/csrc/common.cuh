@@ -196,7 +196,7 @@ struct OCol {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool dvalid(const DCol& c, int64_t r)
 {
-  return c.valid == nullptr || c.valid[r] != 0;
+  return c.valid == nullptr || __ldg(c.valid + r) != 0;
 }
 
 // Raw bits of a fixed-width value, zero-extended; floats are normalised so
@@ -204,10 +204,10 @@ __device__ __forceinline__ bool dvalid(const DCol& c, int64_t r)
 __device__ __forceinline__ uint64_t dbits(const DCol& c, int64_t r)
 {
   switch (c.width) {
-    case 1: return static_cast<const uint8_t*>(c.data)[r];
-    case 2: return static_cast<const uint16_t*>(c.data)[r];
+    case 1: return __ldg(static_cast<const uint8_t*>(c.data) + r);
+    case 2: return __ldg(static_cast<const uint16_t*>(c.data) + r);
     case 4: {
-      uint32_t v = static_cast<const uint32_t*>(c.data)[r];
+      uint32_t v = __ldg(static_cast<const uint32_t*>(c.data) + r);
       if (c.type == LDF_FLOAT32) {
         if ((v & 0x7fffffffu) == 0) v = 0;
         else if ((v & 0x7f800000u) == 0x7f800000u && (v & 0x007fffffu)) v = 0x7fc00000u;
@@ -215,7 +215,7 @@ __device__ __forceinline__ uint64_t dbits(const DCol& c, int64_t r)
       return v;
     }
     default: {
-      uint64_t v = static_cast<const uint64_t*>(c.data)[r];
+      uint64_t v = __ldg(reinterpret_cast<const unsigned long long*>(c.data) + r);
       if (c.type == LDF_FLOAT64) {
         if ((v & 0x7fffffffffffffffull) == 0) v = 0;
         else if ((v & 0x7ff0000000000000ull) == 0x7ff0000000000000ull &&
@@ -237,10 +237,10 @@ __device__ __forceinline__ bool is_signed_int_dev(int t)
 __device__ __forceinline__ int64_t signed_value(const DCol& c, int64_t r)
 {
   switch (c.width) {
-    case 1: return static_cast<const int8_t*>(c.data)[r];
-    case 2: return static_cast<const int16_t*>(c.data)[r];
-    case 4: return static_cast<const int32_t*>(c.data)[r];
-    default: return static_cast<const int64_t*>(c.data)[r];
+    case 1: return __ldg(static_cast<const signed char*>(c.data) + r);
+    case 2: return __ldg(static_cast<const short*>(c.data) + r);
+    case 4: return __ldg(static_cast<const int*>(c.data) + r);
+    default: return __ldg(reinterpret_cast<const long long*>(c.data) + r);
   }
 }
 

@@ -11,41 +11,47 @@
 //    distinct valid values, plus one for null under mode "all".
 //  * output types are the Arrow hash_<kind> result types (.cpp:100-132).
 //
-// Device plan:
-//  1. estimate #groups (and #distinct (group, value) pairs) from a strided
-//     sample with the GEE estimator  D = sqrt(N/n) f1 + sum_{j>=2} f_j; tables
-//     are sized 3x the estimate (load <= 1/3); a probe sequence longer than
-//     kMaxProbe flags overflow and the call re-runs with 4x the capacity.
-//  2. one fused pass over the rows (persistent grid, 1 row per thread per
-//     step, coalesced column reads):
-//       global find-or-insert of the key -> group slot (L1/L2-resident for
-//       heavy hitters, read-mostly);
-//       per-CTA shared-memory table keyed by group slot absorbs the updates of
-//       the groups a CTA sees (heavy hitters), so hot groups cost shared-memory
-//       atomics and one flush per CTA instead of global same-address atomics;
-//       float sums accumulate exactly in 192-bit two's-complement fixed point
-//       (LSB 2^-96): integer adds are associative, so the result is
-//       independent of thread order and bit-identical alone or in a batch;
-//       NUNIQUE inserts (group slot, value) into a pair set and counts
-//       first insertions.
-//  3. compact occupied slots (look-back), 4. finalize each group into the
-//     output columns (fixed point -> correctly rounded double).
+// Device plan (one fused pass over the rows):
+//  * key table: open addressing over 8-byte key words (the key itself for
+//    1-8 byte keys, {representative row, hash tag} otherwise), sized from a
+//    strided sample (GEE estimate x8); a probe sequence longer than kMaxProbe
+//    flags overflow and the call re-runs with a larger table.
+//  * dense group ids: a row that inserts a key takes the next id (one atomic
+//    per warp for all inserting lanes), zero-initialises that group's state
+//    record, then publishes key and id.  Only touched records are written, so
+//    no table-sized memset of the state arena is needed.
+//  * hot groups in shared memory: ids are handed out in first-seen order, so
+//    under skew the heaviest keys get the smallest ids; ids below `hot` keep
+//    their record in shared memory (one flush per CTA at the end).  Hot and cold
+//    rows run the same code through one generic pointer (shared or global), so
+//    a warp never diverges on where its groups live.
+//  * one 8-word record per group (count, per-column valid count, sum, min,
+//    max, distinct count): a cold row's atomics touch a single 64-byte line.
+//  * float sums: exact 192-bit two's-complement fixed point (LSB 2^-96):
+//    integer adds are associative, so the result is independent of thread
+//    order and bit-identical alone or in a batch.
+//  * NUNIQUE: (group id, value) pairs in a pair set; first insertions count.
 #include "table_ops.cuh"
 
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 
 namespace ldf {
 namespace {
 
 constexpr int kMaxAggCols = 8;
 constexpr int kMaxAggs    = 32;
-constexpr int kMaxProbe   = 512;
+constexpr int kMaxProbe   = 1024;
+constexpr int kGbThreads  = 512;
 constexpr uint64_t kEmpty = ~0ull;
-// Empty marker of the 8-byte key table; a key equal to it lives in the extra
-// slot `cap` (and a null single key in slot cap + 1).
+// Empty marker of the 8-byte key table; a key equal to it is the group with
+// the reserved id kIdSentinel, a null single key the group kIdNull.
 constexpr uint64_t kSentinel64 = 0x7ff4dead7ff4beefull;
-constexpr uint32_t kEmpty32    = 0xffffffffu;
-constexpr int kGbThreads       = 256;
+constexpr uint32_t kUnsetId    = 0xffffffffu;
+constexpr uint32_t kIdNull     = 0;
+constexpr uint32_t kIdSentinel = 1;
+constexpr uint32_t kIdFirst    = 2;
 
 enum : uint32_t { ST_SUM = 1, ST_MIN = 2, ST_MAX = 4, ST_NDIST = 8 };
 enum : uint32_t { SP_NAN = 1, SP_PINF = 2, SP_NINF = 4 };
@@ -53,35 +59,38 @@ enum : uint32_t { SP_NAN = 1, SP_PINF = 2, SP_NINF = 4 };
 struct ColPlan {
   DCol col;
   uint32_t states;
-  int fixed;  // float sum in fixed point (3 limbs), else 1 limb integer sum
-  int limbs;
-  unsigned long long* vcount;
-  unsigned long long* sum;  // [slot * limbs + l]
-  double* fb;               // float values outside the fixed-point range
-  unsigned int* special;    // NaN / +inf / -inf seen
-  unsigned long long* mn;   // ~ordered(x), max-combined
-  unsigned long long* mx;   // ordered(x), max-combined
-  unsigned long long* ndist;
-  // pair set for COUNT_DISTINCT
+  int nullable;     // the record has a valid-count word
+  int fixed;        // float sum: 3 words of fixed point, else 1 word
+  int pair_packed;  // (id << 32 | value32) pair keys
+  int off_vcount, off_sum, off_mn, off_mx, off_nd;  // word offsets in the record
+  // shared-memory hot records (byte offsets of typed arrays, [hot] entries)
+  int sh_vcount, sh_sum, sh_mn, sh_mx, sh_nd;
+  int sum_chunks;  // 32-bit chunks of a sum magnitude: 6 (float, 2^-96 LSB) or 2 (integers)
+  int mm64;        // min/max kept as 64-bit words (8-byte types) instead of 32-bit
   unsigned long long* pairs;
   uint64_t pair_cap;
-  int pair_packed;  // (slot << 32 | value32) keys when the value fits 32 bits
-  // shared-memory offsets (bytes)
-  int s_vcount, s_sum, s_mn, s_mx, s_ndist;
+  unsigned long long* pair_buf;  // [n] (id << 32 | value32) per valid row, ~0 otherwise (packed pairs)
+  double* fb;             // [id_cap] float values outside the fixed-point range
+  unsigned int* special;  // [id_cap] NaN / +inf / -inf seen
 };
 
 struct GbPlan {
   KeyCols k;
   int64_t n;
-  void* slots;  // uint64_t[cap]
+  unsigned long long* slots;  // [cap] K32 words, or [2 * cap] {key word, id} pairs
   uint64_t cap;
-  int* overflow;
-  unsigned long long* count_all;
+  unsigned long long* id_counter;
+  uint64_t id_cap;
+  unsigned long long* states;  // [id_cap * stride] group records
+  unsigned long long* id_key;  // [id_cap] key word (1-8 byte keys) or representative row
+  int stride;                  // words per record
+  int hot;                     // ids below `hot` aggregate in shared memory
+  unsigned long long* chunk_counter;  // dynamic row-chunk scheduler
+  int sh_count;                // byte offset of the hot count array
   int ncols;
   ColPlan c[kMaxAggCols];
-  int smem_slots;  // power of two
-  int s_keys, s_count;
-  int smem_bytes;
+  int* overflow;
+  int* err;
 };
 
 // ---- ordered encodings (min/max) ----------------------------------------
@@ -106,94 +115,138 @@ __device__ __forceinline__ uint64_t ordered_bits(const DCol& c, int64_t r)
   }
 }
 
-// ---- 192-bit fixed point ------------------------------------------------
-// x (finite double) -> m << s with LSB 2^-96; exact for 2^-44 <= |x| < 2^95.
-__device__ __forceinline__ bool to_fixed192(double x, uint64_t& a0, uint64_t& a1, uint64_t& a2)
+// 64-bit ordered value of a <= 4-byte type <-> its 32-bit ordered form (both
+// keep the order; the 64-bit one flips bit 63 for signed integers).
+__device__ __forceinline__ uint64_t narrow_ordered(int type, uint64_t o)
 {
-  uint64_t b = __double_as_longlong(x);
-  int e      = static_cast<int>((b >> 52) & 0x7ff);
+  switch (type) {
+    case LDF_INT8:
+    case LDF_INT16:
+    case LDF_INT32: return static_cast<uint32_t>(o) ^ 0x80000000u;  // low 32 bits of the sign-extended value
+    default: return o;  // unsigned, bool, float32 are already 32-bit ordered
+  }
+}
+__device__ __forceinline__ uint64_t widen_ordered(int type, uint32_t o32)
+{
+  switch (type) {
+    case LDF_INT8:
+    case LDF_INT16:
+    case LDF_INT32: {
+      const int32_t v = static_cast<int32_t>(o32 ^ 0x80000000u);
+      return static_cast<uint64_t>(static_cast<int64_t>(v)) ^ (1ull << 63);
+    }
+    default: return o32;
+  }
+}
+
+template <int W, bool SGN, bool FLT>
+__device__ __forceinline__ uint64_t widen32(uint32_t o32)
+{
+  if (!FLT && SGN) {
+    const int32_t v = static_cast<int32_t>(o32 ^ 0x80000000u);
+    return static_cast<uint64_t>(static_cast<int64_t>(v)) ^ (1ull << 63);
+  }
+  return o32;
+}
+
+// ---- exact float sums: carry-save 32-bit chunks ------------------------------
+// A finite double x with 2^-44 <= |x| < 2^95 is an integer multiple of 2^-96:
+// x = +-m * 2^(s - 96) with m < 2^53 and 0 <= s <= 138.  Its 2^-96 fixed-point
+// value is split into 32-bit chunks (bits [32j, 32j + 32), j = 0..5); each
+// chunk is added, signed, into its own 64-bit accumulator with a
+// fire-and-forget reduction.  A chunk is < 2^32 and a group has < 2^31 rows,
+// so accumulators never overflow and the sum is exact whatever the order.
+constexpr int kSumChunks = 6;
+
+__device__ __forceinline__ bool fixed_parts(double x, uint64_t& m, int& s, bool& neg)
+{
+  const uint64_t b = __double_as_longlong(x);
+  const int e      = static_cast<int>((b >> 52) & 0x7ff);
+  neg              = (b >> 63) != 0;
   if (e == 0 && (b << 1) == 0) {
-    a0 = a1 = a2 = 0;
+    m = 0;
+    s = 0;
     return true;
   }
-  int E = e - 1023;
+  const int E = e - 1023;
   if (e == 0 || E < -44 || E >= 95) return false;
-  uint64_t m = (b & ((1ull << 52) - 1)) | (1ull << 52);
-  int s      = E + 44;  // 0 .. 138
-  if (s < 64) {
-    a0 = m << s;
-    a1 = s == 0 ? 0 : (m >> (64 - s));
-    a2 = 0;
-  } else if (s < 128) {
-    int t = s - 64;
-    a0    = 0;
-    a1    = m << t;
-    a2    = t == 0 ? 0 : (m >> (64 - t));
-  } else {
-    a0 = 0;
-    a1 = 0;
-    a2 = m << (s - 128);
-  }
-  if (b >> 63) {  // two's complement negate
-    a0 = ~a0;
-    a1 = ~a1;
-    a2 = ~a2;
-    a0 += 1;
-    if (a0 == 0) {
-      a1 += 1;
-      if (a1 == 0) a2 += 1;
-    }
-  }
+  m = (b & ((1ull << 52) - 1)) | (1ull << 52);
+  s = E + 44;
   return true;
 }
 
-// Exact 192-bit add with atomics on three 64-bit limbs (global or shared):
-// each limb add detects its own carry-out, so the total is exact mod 2^192
-// whatever the interleaving.
-__device__ __forceinline__ void atomic_add192(unsigned long long* p, uint64_t a0, uint64_t a1, uint64_t a2)
+// Fire-and-forget reductions on global memory (explicit global space: the
+// record pointers live in the parameter struct, where the compiler cannot
+// infer it).
+__device__ __forceinline__ void red_add(unsigned long long* p, uint64_t v)
 {
-  unsigned long long o0 = atomicAdd(&p[0], static_cast<unsigned long long>(a0));
-  uint64_t c0           = (o0 + a0 < o0) ? 1 : 0;
-  uint64_t t1           = a1 + c0;
-  uint64_t c1           = (t1 < a1) ? 1 : 0;
-  if (t1 != 0) {
-    unsigned long long o1 = atomicAdd(&p[1], static_cast<unsigned long long>(t1));
-    c1 += (o1 + t1 < o1) ? 1 : 0;
-  }
-  uint64_t t2 = a2 + c1;
-  if (t2 != 0) atomicAdd(&p[2], static_cast<unsigned long long>(t2));
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_max(unsigned long long* p, uint64_t v)
+{
+  asm volatile("red.relaxed.gpu.global.max.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ double fixed192_to_double(uint64_t l0, uint64_t l1, uint64_t l2)
+// Add +-m << s into the chunk accumulators acc[0..5].
+__device__ __forceinline__ void add_fixed_chunks(unsigned long long* acc, uint64_t m, int s, bool neg)
 {
-  bool neg = static_cast<int64_t>(l2) < 0;
-  if (neg) {
-    l0 = ~l0;
-    l1 = ~l1;
-    l2 = ~l2;
-    l0 += 1;
-    if (l0 == 0) {
-      l1 += 1;
-      if (l1 == 0) l2 += 1;
+  if (m == 0) return;
+  const int j0 = s >> 5, j1 = (s + 52) >> 5;
+  for (int j = j0; j <= j1; ++j) {
+    const int off   = 32 * j - s;  // bit of m that lands at chunk bit 0
+    uint64_t chunk  = off >= 0 ? (m >> off) : (m << (-off));
+    chunk &= 0xffffffffull;
+    if (chunk) red_add(acc + j, neg ? (0ull - chunk) : chunk);
+  }
+}
+
+// Exact value of sum_j acc_j * 2^(32j - 96), correctly rounded to double.
+__device__ __forceinline__ double chunks_to_double(const unsigned long long* acc)
+{
+  // 256-bit two's complement accumulation of the signed partials
+  uint64_t w[4] = {0, 0, 0, 0};
+  for (int j = 0; j < kSumChunks; ++j) {
+    const int64_t a = static_cast<int64_t>(acc[j]);
+    uint64_t t[5]   = {0, 0, 0, 0, 0};
+    const int sh = 32 * j, li = sh >> 6, bi = sh & 63;
+    const uint64_t lo = static_cast<uint64_t>(a);
+    const uint64_t ext = a < 0 ? ~0ull : 0ull;
+    t[li] = lo << bi;
+    t[li + 1] = bi ? (lo >> (64 - bi)) | (ext << bi) : ext;
+    for (int q = li + 2; q < 5; ++q) t[q] = ext;
+    uint64_t carry = 0;
+    for (int q = 0; q < 4; ++q) {
+      const uint64_t x = w[q] + t[q];
+      const uint64_t c1 = x < w[q] ? 1 : 0;
+      const uint64_t y = x + carry;
+      const uint64_t c2 = y < x ? 1 : 0;
+      w[q] = y;
+      carry = c1 + c2;
     }
   }
-  int msb;
-  if (l2) msb = 128 + 63 - __clzll(l2);
-  else if (l1) msb = 64 + 63 - __clzll(l1);
-  else if (l0) msb = 63 - __clzll(l0);
-  else return 0.0;
-  // top 64 bits [msb-63, msb] plus a sticky bit for everything below
+  const bool neg = static_cast<int64_t>(w[3]) < 0;
+  if (neg) {
+    uint64_t c = 1;
+    for (int q = 0; q < 4; ++q) {
+      w[q] = ~w[q] + c;
+      c    = (c && w[q] == 0) ? 1 : 0;
+    }
+  }
+  int msb = -1;
+  for (int q = 3; q >= 0; --q)
+    if (w[q]) {
+      msb = 64 * q + 63 - __clzll(w[q]);
+      break;
+    }
+  if (msb < 0) return 0.0;
+  const int lo = msb - 63;
   uint64_t top, sticky = 0;
-  int lo = msb - 63;
   if (lo <= 0) {
-    int sh = -lo;  // value fits in 64 bits: l0 only (msb < 64)
-    top    = l0 << sh;
+    top = w[0] << (-lo);
   } else {
-    // extract 64 bits starting at bit `lo` of the 192-bit number
-    uint64_t w[3] = {l0, l1, l2};
-    int li = lo >> 6, bi = lo & 63;
+    const int li = lo >> 6, bi = lo & 63;
     top = w[li] >> bi;
-    if (bi && li + 1 < 3) top |= w[li + 1] << (64 - bi);
+    if (bi && li + 1 < 4) top |= w[li + 1] << (64 - bi);
     for (int i = 0; i < li; ++i) sticky |= w[i];
     if (bi) sticky |= w[li] & ((1ull << bi) - 1);
   }
@@ -202,56 +255,195 @@ __device__ __forceinline__ double fixed192_to_double(uint64_t l0, uint64_t l1, u
   return neg ? -d : d;
 }
 
-// ---- global find-or-insert ----------------------------------------------
+// ---- group ids ------------------------------------------------------------
+// Key table slots.  K32: one word (id << 32 | key32), published by one CAS.
+// K64 / GEN: two words {key word, id}; the key word is claimed by CAS and the
+// id stored right after, so a reader that sees the key before its id waits
+// (bounded) for the id.  Empty key word: kEmpty, or kSentinel64 for K64.
 template <KeyMode M>
-__device__ __forceinline__ int64_t find_or_insert(const GbPlan& p, int64_t r)
+__device__ __forceinline__ uint64_t empty_word()
 {
-  if (M != KeyMode::GEN && !dvalid(p.k.c[0], r)) return static_cast<int64_t>(p.cap) + 1;
-  uint64_t kb = key_bits<M>(p.k, r);
-  uint64_t entry, h;
-  if (M == KeyMode::K32) {
-    entry = kb;
-    h     = mix64(kb);
-  } else if (M == KeyMode::K64) {
-    if (kb == kSentinel64) return static_cast<int64_t>(p.cap);
-    entry = kb;
-    h     = mix64(kb);
-  } else {
-    h     = kb;
-    entry = (static_cast<uint64_t>(r) << 32) | static_cast<uint32_t>(h);
+  return M == KeyMode::K64 ? kSentinel64 : kEmpty;
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ uint32_t wait_id(const unsigned long long* slot_hi, int* err)
+{
+  for (uint32_t spin = 0; spin < kSpinLimit; ++spin) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(slot_hi) : "memory");
+    if (v != kEmpty) return static_cast<uint32_t>(v);
+    __nanosleep(64);
   }
-  const uint64_t empty = M == KeyMode::K64 ? kSentinel64 : kEmpty;
-  unsigned long long* s = static_cast<unsigned long long*>(p.slots);
-  uint64_t idx          = fastrange(h, p.cap);
-  for (int probe = 0; probe < kMaxProbe; ++probe) {
-    uint64_t v = s[idx];
-    if (v == empty) {
-      v = atomicCAS(&s[idx], empty, entry);
-      if (v == empty) return static_cast<int64_t>(idx);
+  atomicExch(err, LDF_ERR_TIMEOUT);
+  return kUnsetId;
+}
+
+template <KeyMode M>
+__device__ __forceinline__ bool same_key(const GbPlan& p, uint64_t v, uint64_t word, uint64_t h, int64_t r)
+{
+  if (M == KeyMode::K32) return static_cast<uint32_t>(v) == static_cast<uint32_t>(word);
+  if (M == KeyMode::K64) return v == word;
+  return static_cast<uint32_t>(v) == static_cast<uint32_t>(h) &&
+         keys_equal(p.k, r, p.k, static_cast<int64_t>(v >> 32));
+}
+
+// Per-warp pool of pre-zeroed group ids (warp-uniform state).
+struct IdPool {
+  uint64_t next, end;
+};
+
+// Take ids for the lanes with `need` set; refills the pool (32 ids, records
+// zeroed, one fence) when it runs short.  All 32 lanes call it together.
+__device__ __forceinline__ uint64_t pool_take(const GbPlan& p, IdPool& pool, bool need)
+{
+  const uint32_t want = __ballot_sync(0xffffffffu, need);
+  if (want == 0) return kEmpty;
+  const uint32_t k = __popc(want);
+  if (pool.end - pool.next < k) {
+    unsigned long long base = 0;
+    if (lane_id() == 0) base = atomicAdd(p.id_counter, 32ull);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const uint64_t end = base + 32 < p.id_cap ? base + 32 : p.id_cap;
+    if (base < end) {
+      const uint64_t w0 = base * p.stride, w1 = end * p.stride;
+      for (uint64_t w = w0 + lane_id(); w < w1; w += 32) p.states[w] = 0;
+      __threadfence();
     }
+    pool.next = base;
+    pool.end  = end > base ? end : base;
+    if (pool.end - pool.next < k) {
+      if (lane_id() == 0) atomicExch(p.overflow, 1);
+      return kEmpty;
+    }
+  }
+  const uint64_t mine = pool.next + __popc(want & ((1u << lane_id()) - 1u));
+  pool.next += k;
+  return need ? mine : kEmpty;
+}
+
+constexpr int kRows = 4;  // rows per lane per step (memory-level parallelism)
+
+// Group ids of the kRows rows of this lane (kUnsetId for rows past the end).
+template <KeyMode M>
+__device__ void group_ids(const GbPlan& p, IdPool& pool, const int64_t (&r)[kRows], uint32_t (&id)[kRows])
+{
+  const uint64_t empty = empty_word<M>();
+  uint64_t word[kRows], h[kRows], idx[kRows], hi[kRows];
+  bool pending[kRows];
+  unsigned long long* s = p.slots;
+  const int sw          = M == KeyMode::K32 ? 1 : 2;  // words per slot
+#pragma unroll
+  for (int j = 0; j < kRows; ++j) {
+    id[j]      = kUnsetId;
+    pending[j] = false;
+    word[j] = h[j] = idx[j] = hi[j] = 0;
+    if (r[j] >= p.n) continue;
+    if (M != KeyMode::GEN && !dvalid(p.k.c[0], r[j])) {
+      id[j] = kIdNull;
+      continue;
+    }
+    const uint64_t kb = key_bits<M>(p.k, r[j]);
     if (M == KeyMode::GEN) {
-      if (static_cast<uint32_t>(v) == static_cast<uint32_t>(h) &&
-          keys_equal(p.k, r, p.k, static_cast<int64_t>(v >> 32)))
-        return static_cast<int64_t>(idx);
-    } else if (v == entry) {
-      return static_cast<int64_t>(idx);
+      h[j]    = kb;
+      word[j] = (static_cast<uint64_t>(r[j]) << 32) | static_cast<uint32_t>(kb);
+    } else {
+      h[j]    = mix64(kb);
+      word[j] = kb;
     }
-    idx = idx + 1 == p.cap ? 0 : idx + 1;
+    if (M == KeyMode::K64 && kb == kSentinel64) {
+      id[j] = kIdSentinel;
+      continue;
+    }
+    idx[j]     = fastrange(h[j], p.cap);
+    pending[j] = true;
   }
-  atomicExch(p.overflow, 1);
-  return -1;
+  // first probes of all rows in flight together
+  uint64_t v[kRows];
+#pragma unroll
+  for (int j = 0; j < kRows; ++j) {
+    v[j] = 0;
+    if (!pending[j]) continue;
+    if (M == KeyMode::K32) {
+      v[j] = s[idx[j]];
+    } else {
+      const ulonglong2 t = *reinterpret_cast<const ulonglong2*>(s + 2 * idx[j]);
+      v[j]               = t.x;
+      hi[j]              = t.y;
+    }
+  }
+  bool need[kRows];
+#pragma unroll
+  for (int j = 0; j < kRows; ++j) {
+    need[j] = false;
+    if (!pending[j]) continue;
+    for (int probe = 0; probe < kMaxProbe; ++probe) {
+      if (v[j] == empty) {
+        need[j] = true;
+        break;
+      }
+      if (same_key<M>(p, v[j], word[j], h[j], r[j])) {
+        if (M == KeyMode::K32) id[j] = static_cast<uint32_t>(v[j] >> 32);
+        else id[j] = hi[j] != kEmpty ? static_cast<uint32_t>(hi[j]) : wait_id(s + 2 * idx[j] + 1, p.err);
+        break;
+      }
+      idx[j] = idx[j] + 1 == p.cap ? 0 : idx[j] + 1;
+      if (M == KeyMode::K32) {
+        v[j] = s[idx[j]];
+      } else {
+        const ulonglong2 t = *reinterpret_cast<const ulonglong2*>(s + 2 * idx[j]);
+        v[j]               = t.x;
+        hi[j]              = t.y;
+      }
+      if (probe + 1 == kMaxProbe) atomicExch(p.overflow, 1);
+    }
+  }
+  // inserts: ids from the warp pool, then publish
+#pragma unroll
+  for (int j = 0; j < kRows; ++j) {
+    const uint64_t mine = pool_take(p, pool, need[j]);
+    if (!need[j] || mine == kEmpty) continue;
+    p.id_key[mine]      = M == KeyMode::GEN ? static_cast<uint64_t>(r[j]) : word[j];
+    const uint64_t full = M == KeyMode::K32 ? ((mine << 32) | (word[j] & 0xffffffffull)) : word[j];
+    for (int probe = 0; probe < kMaxProbe; ++probe) {
+      const uint64_t old = atomicCAS(s + sw * idx[j], empty, full);
+      if (old == empty) {
+        if (M != KeyMode::K32) s[2 * idx[j] + 1] = mine;
+        id[j] = static_cast<uint32_t>(mine);
+        break;
+      }
+      if (same_key<M>(p, old, word[j], h[j], r[j])) {  // lost the race: `mine` stays a zeroed hole
+        id[j] = M == KeyMode::K32 ? static_cast<uint32_t>(old >> 32) : wait_id(s + 2 * idx[j] + 1, p.err);
+        break;
+      }
+      // another key took the slot: probe on to the key or the next empty slot
+      bool done = false;
+      for (; probe < kMaxProbe; ++probe) {
+        idx[j]           = idx[j] + 1 == p.cap ? 0 : idx[j] + 1;
+        const uint64_t t = s[sw * idx[j]];
+        if (t == empty) break;
+        if (same_key<M>(p, t, word[j], h[j], r[j])) {
+          id[j] = M == KeyMode::K32 ? static_cast<uint32_t>(t >> 32) : wait_id(s + 2 * idx[j] + 1, p.err);
+          done  = true;
+          break;
+        }
+      }
+      if (done) break;
+      if (probe >= kMaxProbe - 1) atomicExch(p.overflow, 1);
+    }
+  }
 }
 
 // Pair set insert for COUNT_DISTINCT; true when (group, value) is new.
-__device__ __forceinline__ bool pair_insert(const GbPlan& p, const ColPlan& c, int64_t slot, int64_t r,
-                                            int* overflow)
+__device__ __forceinline__ bool pair_insert(const GbPlan& p, const ColPlan& c, uint32_t id, int64_t r)
 {
   uint64_t entry, h;
   if (c.pair_packed) {
-    entry = (static_cast<uint64_t>(slot) << 32) | static_cast<uint32_t>(dbits(c.col, r));
+    entry = (static_cast<uint64_t>(id) << 32) | static_cast<uint32_t>(dbits(c.col, r));
     h     = mix64(entry);
   } else {
-    h     = hash_combine64(mix64(static_cast<uint64_t>(slot)), hash_value(c.col, r));
+    h     = hash_combine64(mix64(static_cast<uint64_t>(id)), hash_value(c.col, r));
     entry = (static_cast<uint64_t>(r) << 32) | static_cast<uint32_t>(h);
   }
   uint64_t idx = fastrange(h, c.pair_cap);
@@ -269,200 +461,450 @@ __device__ __forceinline__ bool pair_insert(const GbPlan& p, const ColPlan& c, i
     }
     idx = idx + 1 == c.pair_cap ? 0 : idx + 1;
   }
-  atomicExch(overflow, 1);
+  atomicExch(p.overflow, 1);
   return false;
 }
 
-// ---- the fused aggregation pass -----------------------------------------
+// ---- shared-memory (hot) records ------------------------------------------------
+// Shared-memory atomics are only fast at 32 bits (a 64-bit add is emulated and
+// collapses under the same-address contention of heavy hitters), so hot
+// records hold 32-bit counters, and sums as sign-magnitude 32-bit chunks, each
+// with a 32-bit carry counter: chunk j of a sum = lo_j + 2^32 carry_j, exact.
+// Layout of one hot sum: [chunk][sign][lo, carry] u32 words.
+__device__ __forceinline__ void sh_add_chunk(uint32_t* base, uint32_t v)
+{
+  const uint32_t old = atomicAdd(base, v);
+  if (old + v < old) atomicAdd(base + 1, 1u);
+}
+
+__device__ __forceinline__ void sh_add_magnitude(uint32_t* sum, int nchunks, int first_chunk, uint64_t m_lo,
+                                                 uint64_t m_hi, bool neg)
+{
+  // m (up to 128 bits: m_hi:m_lo) placed at chunk `first_chunk` boundary already
+  (void)nchunks;
+  uint32_t c[4] = {static_cast<uint32_t>(m_lo), static_cast<uint32_t>(m_lo >> 32), static_cast<uint32_t>(m_hi),
+                   static_cast<uint32_t>(m_hi >> 32)};
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if (c[q]) sh_add_chunk(sum + ((first_chunk + q) * 2 + (neg ? 1 : 0)) * 2, c[q]);
+}
+
+// ---- pass 1: dense group id of every row ---------------------------------------
+// gid[r] = group id (kUnsetId past an overflow); the row count of each group is
+// accumulated here too (hot ids in shared memory).
 template <KeyMode M>
-__global__ void __launch_bounds__(kGbThreads) aggregate_kernel(GbPlan p)
+__global__ void __launch_bounds__(kGbThreads) assign_kernel(GbPlan p, uint32_t* gid)
 {
   extern __shared__ __align__(16) unsigned char smem[];
-  uint32_t* s_keys  = reinterpret_cast<uint32_t*>(smem + p.s_keys);
-  uint32_t* s_count = reinterpret_cast<uint32_t*>(smem + p.s_count);
-  const int S       = p.smem_slots;
-  // init shared table
-  for (int i = threadIdx.x; i < S; i += blockDim.x) {
-    s_keys[i]  = kEmpty32;
-    s_count[i] = 0;
-  }
-  for (int ci = 0; ci < p.ncols; ++ci) {
-    const ColPlan& c = p.c[ci];
-    uint32_t* vc     = reinterpret_cast<uint32_t*>(smem + c.s_vcount);
-    for (int i = threadIdx.x; i < S; i += blockDim.x) vc[i] = 0;
-    if (c.states & ST_SUM) {
-      unsigned long long* sm = reinterpret_cast<unsigned long long*>(smem + c.s_sum);
-      for (int i = threadIdx.x; i < S * c.limbs; i += blockDim.x) sm[i] = 0;
-    }
-    if (c.states & ST_MIN) {
-      unsigned long long* a = reinterpret_cast<unsigned long long*>(smem + c.s_mn);
-      for (int i = threadIdx.x; i < S; i += blockDim.x) a[i] = 0;
-    }
-    if (c.states & ST_MAX) {
-      unsigned long long* a = reinterpret_cast<unsigned long long*>(smem + c.s_mx);
-      for (int i = threadIdx.x; i < S; i += blockDim.x) a[i] = 0;
-    }
-    if (c.states & ST_NDIST) {
-      uint32_t* a = reinterpret_cast<uint32_t*>(smem + c.s_ndist);
-      for (int i = threadIdx.x; i < S; i += blockDim.x) a[i] = 0;
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(smem);
+  const int H   = p.hot;
+  for (int i = threadIdx.x; i < H; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+  IdPool pool{0, 0};
+  constexpr int64_t kChunk = 32 * kRows * 32;  // rows per dynamically scheduled chunk
+  for (;;) {
+    unsigned long long chunk = 0;
+    if (lane_id() == 0) chunk = atomicAdd(p.chunk_counter, 1ull);
+    chunk = __shfl_sync(0xffffffffu, chunk, 0);
+    const int64_t c0 = static_cast<int64_t>(chunk) * kChunk;
+    if (c0 >= p.n) break;
+    const int64_t c1 = c0 + kChunk < p.n ? c0 + kChunk : p.n;
+    for (int64_t base = c0; base < c1; base += 32 * kRows) {
+      int64_t r[kRows];
+      uint32_t id[kRows];
+#pragma unroll
+      for (int j = 0; j < kRows; ++j) {
+        r[j] = base + j * 32 + lane_id();
+        if (r[j] >= c1) r[j] = p.n;  // past the chunk: no row
+      }
+      group_ids<M>(p, pool, r, id);
+#pragma unroll
+      for (int j = 0; j < kRows; ++j) {
+        if (r[j] >= p.n) continue;
+        gid[r[j]] = id[j];
+        if (id[j] == kUnsetId) continue;
+        if (id[j] < static_cast<uint32_t>(H)) atomicAdd(cnt + id[j], 1u);
+        else red_add(p.states + static_cast<int64_t>(id[j]) * p.stride, 1);
+      }
     }
   }
   __syncthreads();
+  for (int g = threadIdx.x; g < H; g += blockDim.x)
+    if (cnt[g]) red_add(p.states + static_cast<int64_t>(g) * p.stride, cnt[g]);
+}
 
-  const int shift = 32 - (31 - __clz(S));  // S is a power of two
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < p.n;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t g = find_or_insert<M>(p, r);
-    if (g < 0) continue;
-    // shared-memory slot for g (bounded linear probe; -1 when full)
-    int si       = -1;
-    uint32_t key = static_cast<uint32_t>(g);
-    uint32_t h   = (key * 0x9E3779B1u) >> shift;
-#pragma unroll 1
-    for (int t = 0; t < 8; ++t) {
-      uint32_t v = s_keys[h];
-      if (v == key) {
-        si = static_cast<int>(h);
-        break;
-      }
-      if (v == kEmpty32) {
-        v = atomicCAS(&s_keys[h], kEmpty32, key);
-        if (v == kEmpty32 || v == key) {
-          si = static_cast<int>(h);
-          break;
-        }
-      }
-      h = (h + 1) & (S - 1);
+// ---- pass 2: one value column (valid count, sum, min, max) ---------------------
+struct ColArgs {
+  const uint32_t* gid;
+  int64_t n;
+  DCol col;
+  int nullable;
+  uint32_t states;
+  int sum_chunks;  // 6 (float, fixed point) or 2 (integer magnitude)
+  int off_vcount, off_sum, off_mn, off_mx;
+  unsigned long long* rec;  // group records
+  int stride;
+  double* fb;
+  unsigned int* special;
+  int hot;
+  int sh_vcount, sh_sum, sh_mn, sh_mx, smem_bytes;
+};
+
+// Value of row r as raw bits, and its order-preserving encoding (64-bit form,
+// as in the global records).
+template <int W, bool SGN, bool FLT>
+__device__ __forceinline__ uint64_t load_raw(const void* data, int64_t r)
+{
+  if (W == 1) return __ldg(static_cast<const unsigned char*>(data) + r);
+  if (W == 2) return __ldg(static_cast<const unsigned short*>(data) + r);
+  if (W == 4) return __ldg(static_cast<const unsigned int*>(data) + r);
+  return __ldg(static_cast<const unsigned long long*>(data) + r);
+}
+template <int W, bool SGN, bool FLT>
+__device__ __forceinline__ uint64_t ordered64(uint64_t raw)
+{
+  if (FLT) {
+    if (W == 4) {
+      uint32_t b = static_cast<uint32_t>(raw);
+      return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
     }
-    if (si >= 0) atomicAdd(&s_count[si], 1u);
-    else atomicAdd(&p.count_all[g], 1ull);
+    return (raw & (1ull << 63)) ? ~raw : (raw | (1ull << 63));
+  }
+  if (SGN) {
+    int64_t v = W == 1 ? static_cast<int8_t>(raw) : W == 2 ? static_cast<int16_t>(raw)
+              : W == 4 ? static_cast<int32_t>(raw) : static_cast<int64_t>(raw);
+    return static_cast<uint64_t>(v) ^ (1ull << 63);
+  }
+  return raw;
+}
+// 32-bit ordered form for <= 4-byte types (shared-memory min/max)
+template <int W, bool SGN, bool FLT>
+__device__ __forceinline__ uint32_t ordered32(uint64_t raw)
+{
+  if (FLT) {
+    uint32_t b = static_cast<uint32_t>(raw);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  }
+  if (SGN) {
+    int32_t v = W == 1 ? static_cast<int8_t>(raw) : W == 2 ? static_cast<int16_t>(raw) : static_cast<int32_t>(raw);
+    return static_cast<uint32_t>(v) ^ 0x80000000u;
+  }
+  return static_cast<uint32_t>(raw);
+}
 
-    for (int ci = 0; ci < p.ncols; ++ci) {
-      const ColPlan& c = p.c[ci];
-      if (!dvalid(c.col, r)) continue;
-      if (si >= 0) atomicAdd(reinterpret_cast<uint32_t*>(smem + c.s_vcount) + si, 1u);
-      else atomicAdd(&c.vcount[g], 1ull);
-      if (c.states & ST_SUM) {
-        if (c.fixed) {
-          double x = c.col.type == LDF_FLOAT64 ? static_cast<const double*>(c.col.data)[r]
-                                               : static_cast<double>(static_cast<const float*>(c.col.data)[r]);
-          uint64_t a0, a1, a2;
-          if (to_fixed192(x, a0, a1, a2)) {
-            unsigned long long* dst = si >= 0
-                                        ? reinterpret_cast<unsigned long long*>(smem + c.s_sum) + 3 * si
-                                        : c.sum + 3 * g;
-            atomic_add192(dst, a0, a1, a2);
-          } else if (isnan(x)) {
-            atomicOr(&c.special[g], SP_NAN);
-          } else if (isinf(x)) {
-            atomicOr(&c.special[g], x > 0 ? SP_PINF : SP_NINF);
+template <int W, bool SGN, bool FLT>
+__global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  {
+    uint32_t* z = reinterpret_cast<uint32_t*>(smem);
+    for (int i = threadIdx.x; i < a.smem_bytes / 4; i += blockDim.x) z[i] = 0;
+  }
+  __syncthreads();
+  constexpr bool MM64 = W > 4;
+  const int H         = a.hot;
+  const int64_t step  = static_cast<int64_t>(gridDim.x) * blockDim.x * kRows;
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x) * kRows; base < a.n; base += step) {
+    uint32_t g[kRows];
+    uint64_t raw[kRows];
+    bool ok[kRows];
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+      const int64_t r = base + static_cast<int64_t>(j) * blockDim.x + threadIdx.x;
+      ok[j]           = r < a.n;
+      g[j] = ok[j] ? __ldg(a.gid + r) : kUnsetId;
+      raw[j] = ok[j] ? load_raw<W, SGN, FLT>(a.col.data, r) : 0;
+      if (ok[j] && a.nullable) ok[j] = __ldg(a.col.valid + r) != 0;
+      ok[j] = ok[j] && g[j] != kUnsetId;
+    }
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+      if (!ok[j]) continue;
+      const uint32_t gg = g[j];
+      if (gg < static_cast<uint32_t>(H)) {
+        if (a.nullable) atomicAdd(reinterpret_cast<uint32_t*>(smem + a.sh_vcount) + gg, 1u);
+        if (a.states & ST_SUM) {
+          uint32_t* sum = reinterpret_cast<uint32_t*>(smem + a.sh_sum) + static_cast<int64_t>(gg) * a.sum_chunks * 4;
+          if (FLT) {
+            const double x = W == 8 ? __longlong_as_double(static_cast<long long>(raw[j]))
+                                    : static_cast<double>(__uint_as_float(static_cast<uint32_t>(raw[j])));
+            uint64_t m;
+            int sh;
+            bool neg;
+            if (fixed_parts(x, m, sh, neg)) {
+              if (m) {
+                const int j0 = sh >> 5, b = sh & 31;
+                sh_add_magnitude(sum, a.sum_chunks, j0, m << b, b ? (m >> (64 - b)) : 0, neg);
+              }
+            } else if (isnan(x)) {
+              atomicOr(a.special + gg, SP_NAN);
+            } else if (isinf(x)) {
+              atomicOr(a.special + gg, x > 0 ? SP_PINF : SP_NINF);
+            } else {
+              atomicAdd(a.fb + gg, x);
+            }
           } else {
-            atomicAdd(&c.fb[g], x);
+            uint64_t mag = raw[j];
+            bool neg     = false;
+            if (SGN) {
+              const int64_t v = W == 1 ? static_cast<int8_t>(raw[j]) : W == 2 ? static_cast<int16_t>(raw[j])
+                              : W == 4 ? static_cast<int32_t>(raw[j]) : static_cast<int64_t>(raw[j]);
+              neg = v < 0;
+              mag = neg ? (0ull - static_cast<uint64_t>(v)) : static_cast<uint64_t>(v);
+            }
+            sh_add_magnitude(sum, a.sum_chunks, 0, mag, 0, neg);
           }
-        } else {
-          uint64_t v;
-          if (is_signed_int_dev(c.col.type)) v = static_cast<uint64_t>(signed_value(c.col, r));
-          else v = dbits(c.col, r);
-          unsigned long long* dst = si >= 0 ? reinterpret_cast<unsigned long long*>(smem + c.s_sum) + si
-                                            : c.sum + g;
-          atomicAdd(dst, static_cast<unsigned long long>(v));
         }
-      }
-      if (c.states & (ST_MIN | ST_MAX)) {
-        uint64_t o = ordered_bits(c.col, r);
-        if (c.states & ST_MIN) {
-          unsigned long long* dst = si >= 0 ? reinterpret_cast<unsigned long long*>(smem + c.s_mn) + si : c.mn + g;
-          atomicMax(dst, static_cast<unsigned long long>(~o));
+        if (a.states & (ST_MIN | ST_MAX)) {
+          if (MM64) {
+            const uint64_t o = ordered64<W, SGN, FLT>(raw[j]);
+            if (a.states & ST_MIN) atomicMax(reinterpret_cast<unsigned long long*>(smem + a.sh_mn) + gg, ~o);
+            if (a.states & ST_MAX) atomicMax(reinterpret_cast<unsigned long long*>(smem + a.sh_mx) + gg, o);
+          } else {
+            const uint32_t o = ordered32<W, SGN, FLT>(raw[j]);
+            if (a.states & ST_MIN) atomicMax(reinterpret_cast<uint32_t*>(smem + a.sh_mn) + gg, ~o);
+            if (a.states & ST_MAX) atomicMax(reinterpret_cast<uint32_t*>(smem + a.sh_mx) + gg, o);
+          }
         }
-        if (c.states & ST_MAX) {
-          unsigned long long* dst = si >= 0 ? reinterpret_cast<unsigned long long*>(smem + c.s_mx) + si : c.mx + g;
-          atomicMax(dst, static_cast<unsigned long long>(o));
+      } else {
+        unsigned long long* rec = a.rec + static_cast<int64_t>(gg) * a.stride;
+        if (a.nullable) red_add(rec + a.off_vcount, 1);
+        if (a.states & ST_SUM) {
+          if (FLT) {
+            const double x = W == 8 ? __longlong_as_double(static_cast<long long>(raw[j]))
+                                    : static_cast<double>(__uint_as_float(static_cast<uint32_t>(raw[j])));
+            uint64_t m;
+            int sh;
+            bool neg;
+            if (fixed_parts(x, m, sh, neg)) add_fixed_chunks(rec + a.off_sum, m, sh, neg);
+            else if (isnan(x)) atomicOr(a.special + gg, SP_NAN);
+            else if (isinf(x)) atomicOr(a.special + gg, x > 0 ? SP_PINF : SP_NINF);
+            else atomicAdd(a.fb + gg, x);
+          } else {
+            uint64_t v = raw[j];
+            if (SGN) {
+              const int64_t sv = W == 1 ? static_cast<int8_t>(raw[j]) : W == 2 ? static_cast<int16_t>(raw[j])
+                               : W == 4 ? static_cast<int32_t>(raw[j]) : static_cast<int64_t>(raw[j]);
+              v = static_cast<uint64_t>(sv);
+            }
+            red_add(rec + a.off_sum, v);
+          }
         }
-      }
-      if (c.states & ST_NDIST) {
-        if (pair_insert(p, c, g, r, p.overflow)) {
-          if (si >= 0) atomicAdd(reinterpret_cast<uint32_t*>(smem + c.s_ndist) + si, 1u);
-          else atomicAdd(&c.ndist[g], 1ull);
+        if (a.states & (ST_MIN | ST_MAX)) {
+          const uint64_t o = ordered64<W, SGN, FLT>(raw[j]);
+          if (a.states & ST_MIN) red_max(rec + a.off_mn, ~o);
+          if (a.states & ST_MAX) red_max(rec + a.off_mx, o);
         }
       }
     }
   }
   __syncthreads();
-
-  // flush the shared table into the global states
-  for (int i = threadIdx.x; i < S; i += blockDim.x) {
-    uint32_t key = s_keys[i];
-    if (key == kEmpty32) continue;
-    const int64_t g = key;
-    if (s_count[i]) atomicAdd(&p.count_all[g], static_cast<unsigned long long>(s_count[i]));
-    for (int ci = 0; ci < p.ncols; ++ci) {
-      const ColPlan& c = p.c[ci];
-      uint32_t vc      = reinterpret_cast<uint32_t*>(smem + c.s_vcount)[i];
+  for (int gg = threadIdx.x; gg < H; gg += blockDim.x) {
+    unsigned long long* rec = a.rec + static_cast<int64_t>(gg) * a.stride;
+    if (a.nullable) {
+      const uint32_t vc = reinterpret_cast<const uint32_t*>(smem + a.sh_vcount)[gg];
       if (vc == 0) continue;
-      atomicAdd(&c.vcount[g], static_cast<unsigned long long>(vc));
-      if (c.states & ST_SUM) {
-        const unsigned long long* sm = reinterpret_cast<unsigned long long*>(smem + c.s_sum);
-        if (c.fixed) atomic_add192(c.sum + 3 * g, sm[3 * i], sm[3 * i + 1], sm[3 * i + 2]);
-        else atomicAdd(c.sum + g, sm[i]);
+      red_add(rec + a.off_vcount, vc);
+    }
+    if (a.states & ST_SUM) {
+      const uint32_t* sum = reinterpret_cast<const uint32_t*>(smem + a.sh_sum) + static_cast<int64_t>(gg) * a.sum_chunks * 4;
+      if (FLT) {
+        for (int q = 0; q < a.sum_chunks; ++q) {
+          const int64_t pos = static_cast<int64_t>(sum[q * 4 + 0]) + (static_cast<int64_t>(sum[q * 4 + 1]) << 32);
+          const int64_t neg = static_cast<int64_t>(sum[q * 4 + 2]) + (static_cast<int64_t>(sum[q * 4 + 3]) << 32);
+          if (pos != neg) red_add(rec + a.off_sum + q, static_cast<uint64_t>(pos - neg));
+        }
+      } else {
+        uint64_t tot = 0;  // integer sum mod 2^64
+        for (int q = 0; q < a.sum_chunks; ++q) {
+          const uint64_t pos = static_cast<uint64_t>(sum[q * 4 + 0]) + (static_cast<uint64_t>(sum[q * 4 + 1]) << 32);
+          const uint64_t neg = static_cast<uint64_t>(sum[q * 4 + 2]) + (static_cast<uint64_t>(sum[q * 4 + 3]) << 32);
+          tot += (pos - neg) << (32 * q);
+        }
+        if (tot) red_add(rec + a.off_sum, tot);
       }
-      if (c.states & ST_MIN) atomicMax(c.mn + g, reinterpret_cast<unsigned long long*>(smem + c.s_mn)[i]);
-      if (c.states & ST_MAX) atomicMax(c.mx + g, reinterpret_cast<unsigned long long*>(smem + c.s_mx)[i]);
-      if (c.states & ST_NDIST) {
-        uint32_t nd = reinterpret_cast<uint32_t*>(smem + c.s_ndist)[i];
-        if (nd) atomicAdd(c.ndist + g, static_cast<unsigned long long>(nd));
+    }
+    if (a.states & (ST_MIN | ST_MAX)) {
+      // groups of a non-nullable column reach here with or without rows in
+      // this CTA: an untouched max word 0 is the identity either way
+      if (MM64) {
+        if (a.states & ST_MIN) red_max(rec + a.off_mn, reinterpret_cast<const unsigned long long*>(smem + a.sh_mn)[gg]);
+        if (a.states & ST_MAX) red_max(rec + a.off_mx, reinterpret_cast<const unsigned long long*>(smem + a.sh_mx)[gg]);
+      } else {
+        const uint32_t mn = reinterpret_cast<const uint32_t*>(smem + a.sh_mn)[gg];
+        const uint32_t mx = reinterpret_cast<const uint32_t*>(smem + a.sh_mx)[gg];
+        // an untouched word (no row of this group here) flushes the identity
+        // of the opposite extreme, which never wins
+        if (a.states & ST_MIN) red_max(rec + a.off_mn, ~widen32<W, SGN, FLT>(~mn));
+        if (a.states & ST_MAX) red_max(rec + a.off_mx, widen32<W, SGN, FLT>(mx));
       }
     }
   }
 }
 
-// ---- cardinality estimate on a strided sample ----------------------------
-// Counts sampled keys (and sampled (group, value) pairs of the first
-// COUNT_DISTINCT column) in scratch tables; the GEE estimate is formed on the
-// host from (occupied, singletons).
-template <KeyMode M>
-__global__ void sample_kernel(GbPlan sp, int64_t n_sample, int64_t stride, unsigned int* counts,
-                              int pair_col, unsigned int* pair_counts)
+// ---- NUNIQUE: dedupe the (group id, value) pairs -----------------------------
+// Pairs (gid[r] << 32 | value32) of valid rows go into a pair set; first
+// insertions count per group (hot groups in shared memory first).  Eight rows
+// per thread with their first probes in flight together.
+constexpr int kPairsPerThread = 8;
+struct NdArgs {
+  const uint32_t* gid;
+  DCol col;
+  int64_t n;
+  unsigned long long* set;
+  uint64_t cap;
+  unsigned long long* states;
+  int stride, off_nd, hot;
+  int* overflow;
+};
+
+__global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
 {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(smem);
+  for (int i = threadIdx.x; i < a.hot; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+  const int64_t per_block = static_cast<int64_t>(blockDim.x) * kPairsPerThread;
+  for (int64_t base = blockIdx.x * per_block; base < a.n; base += static_cast<int64_t>(gridDim.x) * per_block) {
+    uint64_t e[kPairsPerThread], idx[kPairsPerThread], v[kPairsPerThread];
+#pragma unroll
+    for (int j = 0; j < kPairsPerThread; ++j) {
+      const int64_t r = base + j * blockDim.x + threadIdx.x;
+      e[j]            = kEmpty;
+      if (r < a.n && dvalid(a.col, r)) {
+        const uint32_t g = __ldg(a.gid + r);
+        if (g != kUnsetId) e[j] = (static_cast<uint64_t>(g) << 32) | static_cast<uint32_t>(dbits(a.col, r));
+      }
+      idx[j] = e[j] != kEmpty ? fastrange(mix64(e[j]), a.cap) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < kPairsPerThread; ++j) v[j] = e[j] != kEmpty ? a.set[idx[j]] : 0;
+#pragma unroll
+    for (int j = 0; j < kPairsPerThread; ++j) {
+      if (e[j] == kEmpty) continue;
+      bool fresh = false;
+      uint64_t x = idx[j], cur = v[j];
+      int probe  = 0;
+      for (; probe < kMaxProbe; ++probe) {
+        if (cur == e[j]) break;
+        if (cur == kEmpty) {
+          cur = atomicCAS(a.set + x, kEmpty, e[j]);
+          if (cur == kEmpty) {
+            fresh = true;
+            break;
+          }
+          if (cur == e[j]) break;
+        }
+        x   = x + 1 == a.cap ? 0 : x + 1;
+        cur = a.set[x];
+      }
+      if (probe == kMaxProbe) atomicExch(a.overflow, 1);
+      if (!fresh) continue;
+      const uint32_t g = static_cast<uint32_t>(e[j] >> 32);
+      if (g < static_cast<uint32_t>(a.hot)) atomicAdd(cnt + g, 1u);
+      else red_add(a.states + static_cast<int64_t>(g) * a.stride + a.off_nd, 1);
+    }
+  }
+  __syncthreads();
+  for (int g = threadIdx.x; g < a.hot; g += blockDim.x)
+    if (cnt[g]) red_add(a.states + static_cast<int64_t>(g) * a.stride + a.off_nd, cnt[g]);
+}
+
+// NUNIQUE of 8-byte or string values: pairs hashed on (group, value) with the
+// representative row in the set (generic, slower path).
+template <KeyMode M>
+__global__ void nunique_generic_kernel(GbPlan p, ColPlan c, const uint32_t* gid)
+{
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < p.n; r += (int64_t)gridDim.x * blockDim.x) {
+    if (!dvalid(c.col, r)) continue;
+    const uint32_t g = gid[r];
+    if (g == kUnsetId) continue;
+    if (pair_insert(p, c, g, r)) red_add(p.states + static_cast<int64_t>(g) * p.stride + c.off_nd, 1);
+  }
+}
+
+// ---- cardinality estimate on a strided sample -------------------------------
+// Keys (and (key slot, value) pairs of the first COUNT_DISTINCT column) of a
+// strided sample are counted in scratch tables; (occupied, singletons) feed
+// the estimates.
+template <KeyMode M>
+__global__ void sample_kernel(KeyCols k, int64_t n_sample, int64_t stride, unsigned long long* slots, uint64_t cap,
+                              unsigned int* counts, ColPlan pc, int with_pairs, unsigned int* pair_counts)
+{
+  const uint64_t empty = M == KeyMode::K64 ? kSentinel64 : kEmpty;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_sample;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = i * stride;
-    const int64_t g = find_or_insert<M>(sp, r);
+    int64_t g       = -1;
+    if (M != KeyMode::GEN && !dvalid(k.c[0], r)) {
+      g = static_cast<int64_t>(cap);
+    } else {
+      const uint64_t kb = key_bits<M>(k, r);
+      uint64_t word, h;
+      if (M == KeyMode::GEN) {
+        h    = kb;
+        word = (static_cast<uint64_t>(r) << 32) | static_cast<uint32_t>(h);
+      } else {
+        h    = mix64(kb);
+        word = M == KeyMode::K32 ? (kb | (1ull << 32)) : kb;
+      }
+      if (M == KeyMode::K64 && kb == kSentinel64) {
+        g = static_cast<int64_t>(cap) + 1;
+      } else {
+        uint64_t idx = fastrange(h, cap);
+        for (int probe = 0; probe < kMaxProbe; ++probe) {
+          uint64_t v = slots[idx];
+          if (v == empty) {
+            v = atomicCAS(&slots[idx], empty, word);
+            if (v == empty) {
+              g = static_cast<int64_t>(idx);
+              break;
+            }
+          }
+          bool same = M == KeyMode::GEN ? (static_cast<uint32_t>(v) == static_cast<uint32_t>(h) &&
+                                           keys_equal(k, r, k, static_cast<int64_t>(v >> 32)))
+                                        : v == word;
+          if (same) {
+            g = static_cast<int64_t>(idx);
+            break;
+          }
+          idx = idx + 1 == cap ? 0 : idx + 1;
+        }
+      }
+    }
     if (g < 0) continue;
     atomicAdd(&counts[g], 1u);
-    if (pair_col >= 0) {
-      const ColPlan& c = sp.c[pair_col];
-      if (!dvalid(c.col, r)) continue;
-      // pair set keyed by the sample slot; count every sampled pair
+    if (with_pairs && dvalid(pc.col, r)) {
       uint64_t entry, h;
-      if (c.pair_packed) {
-        entry = (static_cast<uint64_t>(g) << 32) | static_cast<uint32_t>(dbits(c.col, r));
+      if (pc.pair_packed) {
+        entry = (static_cast<uint64_t>(g) << 32) | static_cast<uint32_t>(dbits(pc.col, r));
         h     = mix64(entry);
       } else {
-        h     = hash_combine64(mix64(static_cast<uint64_t>(g)), hash_value(c.col, r));
+        h     = hash_combine64(mix64(static_cast<uint64_t>(g)), hash_value(pc.col, r));
         entry = (static_cast<uint64_t>(r) << 32) | static_cast<uint32_t>(h);
       }
-      uint64_t idx = fastrange(h, c.pair_cap);
+      uint64_t idx = fastrange(h, pc.pair_cap);
       for (int probe = 0; probe < kMaxProbe; ++probe) {
-        uint64_t v = c.pairs[idx];
+        uint64_t v = pc.pairs[idx];
         if (v == kEmpty) {
-          v = atomicCAS(&c.pairs[idx], kEmpty, entry);
+          v = atomicCAS(&pc.pairs[idx], kEmpty, entry);
           if (v == kEmpty) {
             atomicAdd(&pair_counts[idx], 1u);
             break;
           }
         }
         bool same;
-        if (c.pair_packed) same = v == entry;
+        if (pc.pair_packed) same = v == entry;
         else {
           int64_t o = static_cast<int64_t>(v >> 32);
-          same = static_cast<uint32_t>(v) == static_cast<uint32_t>(h) && keys_equal(sp.k, r, sp.k, o) &&
-                 values_equal(c.col, r, c.col, o);
+          same = static_cast<uint32_t>(v) == static_cast<uint32_t>(h) && keys_equal(k, r, k, o) &&
+                 values_equal(pc.col, r, pc.col, o);
         }
         if (same) {
           atomicAdd(&pair_counts[idx], 1u);
           break;
         }
-        idx = idx + 1 == c.pair_cap ? 0 : idx + 1;
+        idx = idx + 1 == pc.pair_cap ? 0 : idx + 1;
       }
     }
   }
@@ -486,6 +928,14 @@ __global__ void freq_stats_kernel(const unsigned int* counts, int64_t n, unsigne
   }
 }
 
+// p[i * stride] = v for i < n
+__global__ void fill_stride_kernel(unsigned long long* p, int64_t n, int stride, unsigned long long v)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i * stride] = v;
+}
+
 template <typename T>
 __global__ void fill_kernel(T* p, int64_t n, T v)
 {
@@ -494,32 +944,27 @@ __global__ void fill_kernel(T* p, int64_t n, T v)
     p[i] = v;
 }
 
-// ---- compaction of occupied group slots ----------------------------------
-template <KeyMode M>
-__global__ void __launch_bounds__(kGbThreads)
-  compact_groups_kernel(GbPlan p, int64_t nslots, int64_t* groups, uint64_t* status,
-                        unsigned long long* counter, int64_t* total, int* err)
+// ---- compaction of the used ids (record count > 0) ---------------------------
+__global__ void __launch_bounds__(256)
+  compact_groups_kernel(const unsigned long long* states, int stride, int64_t nid, int64_t* groups,
+                        uint64_t* status, unsigned long long* counter, int64_t* total, int* err)
 {
   constexpr int ITEMS = 4;
-  __shared__ int64_t s_scan[kGbThreads / 32 + 1];
+  __shared__ int64_t s_scan[256 / 32 + 1];
   __shared__ int64_t s_tile;
   __shared__ uint64_t s_prefix;
   const int64_t tile = next_tile_id(counter, &s_tile);
-  const int64_t base = tile * (kGbThreads * ITEMS) + static_cast<int64_t>(threadIdx.x) * ITEMS;
-  const unsigned long long* s = static_cast<const unsigned long long*>(p.slots);
-  const uint64_t empty = M == KeyMode::K64 ? kSentinel64 : kEmpty;
+  const int64_t base = tile * (256 * ITEMS) + static_cast<int64_t>(threadIdx.x) * ITEMS;
   int f[ITEMS];
   int64_t c = 0;
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    int64_t j = base + i;
-    f[i]      = 0;
-    if (j < static_cast<int64_t>(p.cap)) f[i] = s[j] != empty;
-    else if (j < nslots) f[i] = p.count_all[j] > 0;
+    const int64_t j = base + i;
+    f[i]            = (j < nid && states[j * stride] > 0) ? 1 : 0;
     c += f[i];
   }
   int64_t tot;
-  int64_t ex = block_exclusive_scan<int64_t, kGbThreads>(c, s_scan, &tot);
+  int64_t ex = block_exclusive_scan<int64_t, 256>(c, s_scan, &tot);
   if (threadIdx.x == 0) {
     s_prefix = lookback_exclusive(status, tile, static_cast<uint64_t>(tot), err);
     if (tile == static_cast<int64_t>(gridDim.x) - 1) *total = static_cast<int64_t>(s_prefix) + tot;
@@ -531,7 +976,7 @@ __global__ void __launch_bounds__(kGbThreads)
     if (f[i]) groups[pos++] = base + i;
 }
 
-// ---- finalize ------------------------------------------------------------
+// ---- finalize --------------------------------------------------------------
 struct AggOut {
   int kind;
   int count_mode;
@@ -588,29 +1033,30 @@ __device__ __forceinline__ uint64_t unordered_bits(int type, uint64_t o)
   }
 }
 
-__device__ __forceinline__ double float_sum(const ColPlan& c, int64_t g, bool& special, double& sval)
+__device__ __forceinline__ double float_sum(const ColPlan& c, const unsigned long long* rec, int64_t id,
+                                            bool& special, double& sval)
 {
-  unsigned int sp = c.special[g];
+  unsigned int sp = c.special[id];
   special         = sp != 0;
   if (special) {
     if ((sp & SP_NAN) || ((sp & SP_PINF) && (sp & SP_NINF))) sval = __longlong_as_double(0x7ff8000000000000ll);
     else sval = (sp & SP_PINF) ? __longlong_as_double(0x7ff0000000000000ll)
                                : __longlong_as_double(0xfff0000000000000ll);
   }
-  return fixed192_to_double(c.sum[3 * g], c.sum[3 * g + 1], c.sum[3 * g + 2]) + c.fb[g];
+  return chunks_to_double(rec + c.off_sum) + c.fb[id];
 }
 
 __global__ void finalize_kernel(FinArgs f)
 {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < f.ngroups;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t g = f.groups[i];
-    const GbPlan& p = f.p;
+    const int64_t id              = f.groups[i];
+    const GbPlan& p               = f.p;
+    const unsigned long long* rec = p.states + id * p.stride;
     // keys
     if (f.key_mode == static_cast<int>(KeyMode::GEN)) {
-      uint64_t v = static_cast<const unsigned long long*>(p.slots)[g];
-      int64_t rr = static_cast<int64_t>(v >> 32);
-      f.repr[i]  = static_cast<int32_t>(rr);
+      const int64_t rr = static_cast<int64_t>(p.id_key[id]);
+      f.repr[i]        = static_cast<int32_t>(rr);
       for (int j = 0; j < f.nkeys; ++j) {
         const OCol& d = f.key_dst[j];
         if (d.type == LDF_STRING) continue;
@@ -618,15 +1064,13 @@ __global__ void finalize_kernel(FinArgs f)
         if (d.valid) d.valid[i] = dvalid(p.k.c[j], rr) ? 1 : 0;
       }
     } else {
-      const OCol& d = f.key_dst[0];
-      bool is_null  = g == static_cast<int64_t>(p.cap) + 1;
-      uint64_t kb   = g == static_cast<int64_t>(p.cap) ? kSentinel64
-                      : is_null                        ? 0
-                                                       : static_cast<const unsigned long long*>(p.slots)[g];
+      const OCol& d      = f.key_dst[0];
+      const bool is_null = id == kIdNull;
+      const uint64_t kb  = id == kIdSentinel ? kSentinel64 : is_null ? 0 : p.id_key[id];
       store_int(OCol{d.data, nullptr, LDF_UINT64, d.width}, i, kb);
       if (d.valid) d.valid[i] = is_null ? 0 : 1;
     }
-    const uint64_t call = p.count_all[g];
+    const uint64_t call = rec[0];
     for (int a = 0; a < f.nagg; ++a) {
       const AggOut& o = f.a[a];
       const OCol& d   = o.dst;
@@ -635,8 +1079,8 @@ __global__ void finalize_kernel(FinArgs f)
         if (d.valid) d.valid[i] = 1;
         continue;
       }
-      const ColPlan& c = p.c[o.col];
-      const uint64_t vc = c.vcount[g];
+      const ColPlan& c  = p.c[o.col];
+      const uint64_t vc = c.nullable ? rec[c.off_vcount] : call;
       bool ok           = vc > 0;
       switch (o.kind) {
         case LDF_AGG_COUNT: {
@@ -647,7 +1091,7 @@ __global__ void finalize_kernel(FinArgs f)
         }
         case LDF_AGG_COUNT_DISTINCT: {
           uint64_t has_null = call > vc ? 1 : 0;
-          uint64_t nd       = c.ndist ? c.ndist[g] : 0;
+          uint64_t nd       = (c.states & ST_NDIST) ? rec[c.off_nd] : 0;
           uint64_t v = o.count_mode == LDF_COUNT_ALL ? nd + has_null : o.count_mode == LDF_COUNT_ONLY_NULL ? has_null : nd;
           store_int(d, i, v);
           ok = true;
@@ -659,26 +1103,20 @@ __global__ void finalize_kernel(FinArgs f)
             store_int(d, i, 0);
             break;
           }
-          double sv;
           if (c.fixed) {
             bool special;
             double sval;
-            sv = float_sum(c, g, special, sval);
+            double sv = float_sum(c, rec, id, special, sval);
             if (special) sv = sval;
             if (o.kind == LDF_AGG_MEAN) sv = sv / static_cast<double>(vc);
             store_double(d, i, sv);
           } else {
-            uint64_t s = c.sum[g];
-            if (o.kind == LDF_AGG_MEAN) {
-              double m = is_signed_int_dev(o.in_type) ? static_cast<double>(static_cast<int64_t>(s))
-                                                      : static_cast<double>(s);
-              store_double(d, i, m / static_cast<double>(vc));
-            } else if (d.type == LDF_FLOAT64 || d.type == LDF_FLOAT32) {
-              store_double(d, i, is_signed_int_dev(o.in_type) ? static_cast<double>(static_cast<int64_t>(s))
-                                                              : static_cast<double>(s));
-            } else {
-              store_int(d, i, s);
-            }
+            const uint64_t s = rec[c.off_sum];
+            const double sd  = is_signed_int_dev(o.in_type) ? static_cast<double>(static_cast<int64_t>(s))
+                                                            : static_cast<double>(s);
+            if (o.kind == LDF_AGG_MEAN) store_double(d, i, sd / static_cast<double>(vc));
+            else if (d.type == LDF_FLOAT64 || d.type == LDF_FLOAT32) store_double(d, i, sd);
+            else store_int(d, i, s);
           }
           break;
         }
@@ -688,11 +1126,10 @@ __global__ void finalize_kernel(FinArgs f)
             store_int(d, i, 0);
             break;
           }
-          uint64_t o64 = o.kind == LDF_AGG_MIN ? ~c.mn[g] : c.mx[g];
-          uint64_t b   = unordered_bits(o.in_type, o64);
+          const uint64_t o64 = o.kind == LDF_AGG_MIN ? ~rec[c.off_mn] : rec[c.off_mx];
+          const uint64_t b   = unordered_bits(o.in_type, o64);
           if (d.type == o.in_type) {
-            OCol raw{d.data, nullptr, LDF_UINT64, d.width};
-            store_int(raw, i, b);
+            store_int(OCol{d.data, nullptr, LDF_UINT64, d.width}, i, b);
           } else if (o.in_type == LDF_FLOAT32) {
             store_double(d, i, static_cast<double>(__uint_as_float(static_cast<uint32_t>(b))));
           } else if (o.in_type == LDF_FLOAT64) {
@@ -709,6 +1146,8 @@ __global__ void finalize_kernel(FinArgs f)
   }
 }
 
+thread_local cudaStream_t g_column_stream = nullptr;
+
 unsigned gs_blocks(int64_t n, int threads)
 {
   int64_t b   = ceil_div(n, threads);
@@ -716,13 +1155,43 @@ unsigned gs_blocks(int64_t n, int threads)
   return static_cast<unsigned>(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
+void launch_column(ColArgs& a, int type)
+{
+  cudaStream_t s = 0;
+  (void)s;
+  auto go = [&](auto kernel) {
+    LDF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    int occ = 1;
+    LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kGbThreads, a.smem_bytes));
+    const int64_t blocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(occ, 1),
+                                             ceil_div(a.n, int64_t(kGbThreads) * kRows));
+    launch("column", kernel, static_cast<unsigned>(blocks), kGbThreads, static_cast<size_t>(a.smem_bytes),
+           g_column_stream, a);
+  };
+  switch (type) {
+    case LDF_BOOL8:
+    case LDF_UINT8: go(column_kernel<1, false, false>); break;
+    case LDF_INT8: go(column_kernel<1, true, false>); break;
+    case LDF_UINT16: go(column_kernel<2, false, false>); break;
+    case LDF_INT16: go(column_kernel<2, true, false>); break;
+    case LDF_UINT32: go(column_kernel<4, false, false>); break;
+    case LDF_INT32: go(column_kernel<4, true, false>); break;
+    case LDF_FLOAT32: go(column_kernel<4, false, true>); break;
+    case LDF_UINT64: go(column_kernel<8, false, false>); break;
+    case LDF_INT64:
+    case LDF_TIMESTAMP_US: go(column_kernel<8, true, false>); break;
+    case LDF_FLOAT64: go(column_kernel<8, false, true>); break;
+    default: fail(LDF_ERR_UNSUPPORTED, "unsupported aggregation column type");
+  }
+}
+
 template <KeyMode M>
-void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const int32_t* keys,
-                 int nkeys, const ldf_aggregation* aggs, int naggs, const std::vector<int>& agg_col,
-                 ldf_column* out)
+void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const int32_t* keys, int nkeys,
+                 const ldf_aggregation* aggs, int naggs, const std::vector<int>& agg_col, ldf_column* out)
 {
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
+  g_column_stream     = s;
   const int64_t n     = p.n;
 
   int ndist_col = -1;
@@ -732,185 +1201,218 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
       break;
     }
 
-  // ---- estimate groups / pairs ----------------------------------------------
+  // ---- estimate #groups and #(group, value) pairs ----------------------------
   int64_t est_groups = n, est_pairs = n;
   const int64_t kSampleMax = int64_t(1) << 20;
   if (n > (int64_t(1) << 16)) {
     const int64_t ns     = std::min<int64_t>(n, kSampleMax);
     const int64_t stride = n / ns;
-    GbPlan sp            = p;
-    sp.cap               = static_cast<uint64_t>(2 * ns + 64);
-    Buffer<unsigned long long> sslots(al, sp.cap + 2);
-    Buffer<unsigned int> scounts(al, sp.cap + 2);
-    Buffer<int> sover(al, 1);
-    LDF_CUDA(cudaMemsetAsync(sslots.get(), 0xff, (sp.cap + 2) * 8, s));
+    const uint64_t scap  = static_cast<uint64_t>(2 * ns + 64);
+    Buffer<unsigned long long> sslots(al, scap);
+    Buffer<unsigned int> scounts(al, scap + 2);
     if (M == KeyMode::K64)
-      launch("fill", fill_kernel<unsigned long long>, gs_blocks(sp.cap, 256), 256, 0, s, sslots.get(), sp.cap, kSentinel64);
-    LDF_CUDA(cudaMemsetAsync(scounts.get(), 0, (sp.cap + 2) * 4, s));
-    LDF_CUDA(cudaMemsetAsync(sover.get(), 0, 4, s));
-    sp.slots    = sslots.get();
-    sp.overflow = sover.get();
+      launch("fill", fill_kernel<unsigned long long>, gs_blocks(scap, 256), 256, 0, s, sslots.get(),
+             static_cast<int64_t>(scap), kSentinel64);
+    else
+      LDF_CUDA(cudaMemsetAsync(sslots.get(), 0xff, scap * 8, s));
+    LDF_CUDA(cudaMemsetAsync(scounts.get(), 0, (scap + 2) * 4, s));
+    ColPlan pc{};
     Buffer<unsigned long long> spairs;
     Buffer<unsigned int> spcounts;
     if (ndist_col >= 0) {
-      ColPlan& c  = sp.c[ndist_col];
-      c.pair_cap  = static_cast<uint64_t>(2 * ns + 64);
-      spairs      = Buffer<unsigned long long>(al, c.pair_cap);
-      spcounts    = Buffer<unsigned int>(al, c.pair_cap);
-      LDF_CUDA(cudaMemsetAsync(spairs.get(), 0xff, c.pair_cap * 8, s));
-      LDF_CUDA(cudaMemsetAsync(spcounts.get(), 0, c.pair_cap * 4, s));
-      c.pairs = spairs.get();
+      pc          = p.c[ndist_col];
+      pc.pair_cap = static_cast<uint64_t>(2 * ns + 64);
+      spairs      = Buffer<unsigned long long>(al, pc.pair_cap);
+      spcounts    = Buffer<unsigned int>(al, pc.pair_cap);
+      LDF_CUDA(cudaMemsetAsync(spairs.get(), 0xff, pc.pair_cap * 8, s));
+      LDF_CUDA(cudaMemsetAsync(spcounts.get(), 0, pc.pair_cap * 4, s));
+      pc.pairs = spairs.get();
     }
-    launch("sample", sample_kernel<M>, gs_blocks(ns, 256), 256, 0, s, sp, ns, stride, scounts.get(), ndist_col,
-                                                         spcounts.get());
-    LDF_CHECK_LAUNCH();
+    launch("sample", sample_kernel<M>, gs_blocks(ns, 256), 256, 0, s, p.k, ns, stride, sslots.get(), scap,
+           scounts.get(), pc, ndist_col >= 0 ? 1 : 0, spcounts.get());
     Buffer<unsigned long long> stats(al, 4);
     LDF_CUDA(cudaMemsetAsync(stats.get(), 0, 32, s));
-    launch("freq_stats", freq_stats_kernel, gs_blocks(sp.cap + 2, 256), 256, 0, s, scounts.get(), sp.cap + 2, stats.get());
+    launch("freq_stats", freq_stats_kernel, gs_blocks(scap + 2, 256), 256, 0, s, scounts.get(),
+           static_cast<int64_t>(scap + 2), stats.get());
     if (ndist_col >= 0)
-      launch("freq_stats", freq_stats_kernel, gs_blocks(sp.c[ndist_col].pair_cap, 256), 256, 0, s, 
-        spcounts.get(), sp.c[ndist_col].pair_cap, stats.get() + 2);
-    LDF_CHECK_LAUNCH();
+      launch("freq_stats", freq_stats_kernel, gs_blocks(pc.pair_cap, 256), 256, 0, s, spcounts.get(),
+             static_cast<int64_t>(pc.pair_cap), stats.get() + 2);
     unsigned long long h[4];
     LDF_CUDA(cudaMemcpyAsync(h, stats.get(), 32, cudaMemcpyDeviceToHost, s));
     ctx.finish();
+    // GEE (Charikar et al. 2000) for the groups, taken x8 below because it
+    // underestimates heavy tails; (group, value) pairs are mostly unique in a
+    // sample, where GEE fails, so they use the scale-up d * N / n, an
+    // overestimate whenever pairs repeat.
     const double scale = std::sqrt(static_cast<double>(n) / static_cast<double>(ns));
-    est_groups = static_cast<int64_t>(scale * h[1] + (h[0] - h[1])) + 1;
-    est_pairs  = static_cast<int64_t>(scale * h[3] + (h[2] - h[3])) + 1;
-    est_groups = std::min<int64_t>(est_groups, n);
-    est_pairs  = std::min<int64_t>(est_pairs, n);
+    est_groups         = static_cast<int64_t>(scale * h[1] + (h[0] - h[1])) + 1;
+    est_pairs          = static_cast<int64_t>(static_cast<double>(h[2]) * n / ns) + 1;
+    est_groups         = std::min<int64_t>(8 * est_groups, n);
+    est_pairs          = std::min<int64_t>(est_pairs, n);
   }
+  if (std::getenv("LDF_B200_DEBUG"))
+    std::fprintf(stderr, "[ldf_b200] groupby n=%lld est_groups=%lld est_pairs=%lld\n", static_cast<long long>(n),
+                 static_cast<long long>(est_groups), static_cast<long long>(est_pairs));
 
-  uint64_t cap      = static_cast<uint64_t>(std::max<int64_t>(3 * est_groups, 64));
-  uint64_t pair_cap = static_cast<uint64_t>(std::max<int64_t>(3 * est_pairs, 64));
+  uint64_t cap      = static_cast<uint64_t>(std::max<int64_t>(2 * est_groups, 64));
+  uint64_t pair_cap = static_cast<uint64_t>(std::max<int64_t>(est_pairs + est_pairs / 2, 64));
 
-  // ---- shared-memory plan --------------------------------------------------
-  int per_slot = 8;  // key + count_all
+  // ---- record layout and shared-memory hot set -------------------------------
+  int w = 1;  // count_all
   for (int ci = 0; ci < p.ncols; ++ci) {
-    const ColPlan& c = p.c[ci];
-    per_slot += 4;
-    if (c.states & ST_SUM) per_slot += 8 * c.limbs;
-    if (c.states & ST_MIN) per_slot += 8;
-    if (c.states & ST_MAX) per_slot += 8;
-    if (c.states & ST_NDIST) per_slot += 4;
-  }
-  int S = 4096;
-  const int kSmemBudget = 100 * 1024;
-  while (S > 64 && S * per_slot + 64 * (p.ncols * 5 + 2) > kSmemBudget) S >>= 1;
-  {
-    int off      = 0;
-    auto take    = [&](int bytes) {
-      int o = off;
-      off += (bytes + 15) & ~15;
-      return o;
-    };
-    p.smem_slots = S;
-    for (int ci = 0; ci < p.ncols; ++ci) {
-      ColPlan& c = p.c[ci];
-      c.s_sum    = (c.states & ST_SUM) ? take(8 * c.limbs * S) : 0;
-      c.s_mn     = (c.states & ST_MIN) ? take(8 * S) : 0;
-      c.s_mx     = (c.states & ST_MAX) ? take(8 * S) : 0;
+    ColPlan& c   = p.c[ci];
+    c.sum_chunks = c.fixed ? kSumChunks : 2;
+    c.mm64       = type_width(c.col.type) > 4 ? 1 : 0;
+    c.off_vcount = c.nullable ? w++ : 0;
+    if (c.states & ST_SUM) {
+      c.off_sum = w;
+      w += c.fixed ? kSumChunks : 1;
     }
-    p.s_keys  = take(4 * S);
-    p.s_count = take(4 * S);
-    for (int ci = 0; ci < p.ncols; ++ci) {
-      ColPlan& c  = p.c[ci];
-      c.s_vcount  = take(4 * S);
-      c.s_ndist   = (c.states & ST_NDIST) ? take(4 * S) : 0;
-    }
-    p.smem_bytes = off;
+    if (c.states & ST_MIN) c.off_mn = w++;
+    if (c.states & ST_MAX) c.off_mx = w++;
+    if (c.states & ST_NDIST) c.off_nd = w++;
   }
-  LDF_CUDA(cudaFuncSetAttribute(aggregate_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                p.smem_bytes));
-  int occ = 1;
-  LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, aggregate_kernel<M>, kGbThreads,
-                                                         p.smem_bytes));
-  occ = std::max(occ, 1);
+  p.stride = w;
+  const int kSmemBudget = 96 * 1024;
+  LDF_CUDA(cudaFuncSetAttribute(assign_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+  int hot_limit = 1 << 30;
+  if (const char* e = std::getenv("LDF_B200_GB_HOT")) hot_limit = std::max(0, std::atoi(e));
 
   for (int attempt = 0;; ++attempt) {
-    // ---- allocate + init tables ------------------------------------------------
-    const uint64_t nslots = cap + 2;
-    Buffer<unsigned long long> slots(al, cap);
+    const uint64_t id_cap = cap + kIdFirst;
+    const int sw          = M == KeyMode::K32 ? 1 : 2;
+    Buffer<unsigned long long> slots(al, cap * sw);
+    Buffer<unsigned long long> states(al, id_cap * p.stride);
+    Buffer<unsigned long long> id_key(al, id_cap);
+    Buffer<unsigned long long> misc(al, 4);  // id counter, overflow, chunk counter
+    Buffer<uint32_t> gid(al, std::max<int64_t>(n, 1));
+    LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, cap * sw * 8, s));
     if (M == KeyMode::K64)
-      launch("fill", fill_kernel<unsigned long long>, gs_blocks(cap, 256), 256, 0, s, slots.get(), cap, kSentinel64);
-    else
-      LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, cap * 8, s));
-    // one zeroed arena for every per-group state
-    size_t words = nslots;  // count_all
-    for (int ci = 0; ci < p.ncols; ++ci) {
-      const ColPlan& c = p.c[ci];
-      words += nslots;  // vcount
-      if (c.states & ST_SUM) words += nslots * c.limbs + (c.fixed ? 2 * nslots : 0);
-      if (c.states & ST_MIN) words += nslots;
-      if (c.states & ST_MAX) words += nslots;
-      if (c.states & ST_NDIST) words += nslots;
-    }
-    Buffer<unsigned long long> arena(al, words);
-    LDF_CUDA(cudaMemsetAsync(arena.get(), 0, words * 8, s));
-    unsigned long long* w = arena.get();
-    p.slots               = slots.get();
-    p.cap                 = cap;
-    p.count_all           = w;
-    w += nslots;
+      launch("fill_key_words", fill_stride_kernel, gs_blocks(cap, 256), 256, 0, s, slots.get(),
+             static_cast<int64_t>(cap), 2, kSentinel64);
+    LDF_CUDA(cudaMemsetAsync(states.get(), 0, static_cast<size_t>(kIdFirst) * p.stride * 8, s));  // reserved ids
+    const unsigned long long first = kIdFirst;
+    LDF_CUDA(cudaMemsetAsync(misc.get(), 0, 32, s));
+    LDF_CUDA(cudaMemcpyAsync(misc.get(), &first, 8, cudaMemcpyHostToDevice, s));
+    p.slots         = slots.get();
+    p.cap           = cap;
+    p.id_counter    = misc.get();
+    p.id_cap        = id_cap;
+    p.states        = states.get();
+    p.id_key        = id_key.get();
+    p.overflow      = reinterpret_cast<int*>(misc.get() + 1);
+    p.chunk_counter = misc.get() + 2;
+    p.err           = ctx.err();
+    const int hot_cap = static_cast<int>(std::min<uint64_t>(id_cap, static_cast<uint64_t>(hot_limit)));
+
     std::vector<Buffer<unsigned long long>> pair_bufs;
+    std::vector<Buffer<double>> fb_bufs;
+    std::vector<Buffer<unsigned int>> sp_bufs;
     for (int ci = 0; ci < p.ncols; ++ci) {
       ColPlan& c = p.c[ci];
-      c.vcount   = w;
-      w += nslots;
-      if (c.states & ST_SUM) {
-        c.sum = w;
-        w += nslots * c.limbs;
-        if (c.fixed) {
-          c.fb = reinterpret_cast<double*>(w);
-          w += nslots;
-          c.special = reinterpret_cast<unsigned int*>(w);
-          w += nslots;
-        }
-      }
-      if (c.states & ST_MIN) {
-        c.mn = w;
-        w += nslots;
-      }
-      if (c.states & ST_MAX) {
-        c.mx = w;
-        w += nslots;
+      if ((c.states & ST_SUM) && c.fixed) {
+        fb_bufs.emplace_back(al, id_cap);
+        sp_bufs.emplace_back(al, id_cap);
+        LDF_CUDA(cudaMemsetAsync(fb_bufs.back().get(), 0, id_cap * 8, s));
+        LDF_CUDA(cudaMemsetAsync(sp_bufs.back().get(), 0, id_cap * 4, s));
+        c.fb      = fb_bufs.back().get();
+        c.special = sp_bufs.back().get();
       }
       if (c.states & ST_NDIST) {
-        c.ndist = w;
-        w += nslots;
         c.pair_cap = pair_cap;
         pair_bufs.emplace_back(al, pair_cap);
         c.pairs = pair_bufs.back().get();
         LDF_CUDA(cudaMemsetAsync(c.pairs, 0xff, pair_cap * 8, s));
       }
     }
-    Buffer<int64_t> over(al, 1);
-    LDF_CUDA(cudaMemsetAsync(over.get(), 0, 8, s));
-    p.overflow = reinterpret_cast<int*>(over.get());
 
-    // ---- aggregate ----------------------------------------------------------------
     if (n > 0) {
-      int64_t blocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * occ, ceil_div(n, kGbThreads));
-      launch("aggregate", aggregate_kernel<M>, static_cast<unsigned>(blocks), kGbThreads, p.smem_bytes, s, p);
-      LDF_CHECK_LAUNCH();
+      // pass 1: group ids + row counts
+      p.hot                 = std::min(hot_cap, (kSmemBudget - 64) / 4);
+      const size_t a_smem   = static_cast<size_t>(p.hot) * 4;
+      int occ               = 1;
+      LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, assign_kernel<M>, kGbThreads, a_smem));
+      const int64_t ablocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(occ, 1),
+                                                ceil_div(n, int64_t(kGbThreads) * kRows));
+      launch("assign", assign_kernel<M>, static_cast<unsigned>(ablocks), kGbThreads, a_smem, s, p, gid.get());
+      // pass 2: one kernel per value column that needs valid counts / sums / min / max
+      for (int ci = 0; ci < p.ncols; ++ci) {
+        ColPlan& c = p.c[ci];
+        if (!c.nullable && !(c.states & (ST_SUM | ST_MIN | ST_MAX))) continue;
+        ColArgs a{};
+        a.gid        = gid.get();
+        a.n          = n;
+        a.col        = c.col;
+        a.nullable   = c.nullable;
+        a.states     = c.states & (ST_SUM | ST_MIN | ST_MAX);
+        a.sum_chunks = c.sum_chunks;
+        a.off_vcount = c.off_vcount;
+        a.off_sum    = c.off_sum;
+        a.off_mn     = c.off_mn;
+        a.off_mx     = c.off_mx;
+        a.rec        = p.states;
+        a.stride     = p.stride;
+        a.fb         = c.fb;
+        a.special    = c.special;
+        const int mmw = c.mm64 ? 8 : 4;
+        const int per = (c.nullable ? 4 : 0) + ((a.states & ST_SUM) ? 16 * c.sum_chunks : 0) +
+                        ((a.states & ST_MIN) ? mmw : 0) + ((a.states & ST_MAX) ? mmw : 0);
+        a.hot         = std::min(hot_cap, (kSmemBudget - 256) / std::max(per, 1));
+        int off       = 0;
+        auto take     = [&](int bytes_per) {
+          const int o = off;
+          off += (bytes_per * a.hot + 15) & ~15;
+          return o;
+        };
+        a.sh_mn      = (a.states & ST_MIN) && c.mm64 ? take(8) : 0;
+        a.sh_mx      = (a.states & ST_MAX) && c.mm64 ? take(8) : 0;
+        a.sh_sum     = (a.states & ST_SUM) ? take(16 * c.sum_chunks) : 0;
+        a.sh_vcount  = c.nullable ? take(4) : 0;
+        if ((a.states & ST_MIN) && !c.mm64) a.sh_mn = take(4);
+        if ((a.states & ST_MAX) && !c.mm64) a.sh_mx = take(4);
+        a.smem_bytes = off;
+        launch_column(a, c.col.type);
+      }
+      // pass 3: NUNIQUE
+      for (int ci = 0; ci < p.ncols; ++ci) {
+        ColPlan& c = p.c[ci];
+        if (!(c.states & ST_NDIST)) continue;
+        if (c.pair_packed) {
+          NdArgs na{gid.get(), c.col, n, c.pairs, c.pair_cap, p.states, p.stride, c.off_nd,
+                    std::min(hot_cap, 12 * 1024), p.overflow};
+          const size_t nd_smem = static_cast<size_t>(na.hot) * 4;
+          int nocc             = 1;
+          LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nocc, nunique_kernel, kGbThreads, nd_smem));
+          const int64_t nblocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(nocc, 1),
+                                                    ceil_div(n, int64_t(kGbThreads) * kPairsPerThread));
+          launch("nunique", nunique_kernel, static_cast<unsigned>(nblocks), kGbThreads, nd_smem, s, na);
+        } else {
+          launch("nunique_generic", nunique_generic_kernel<M>, gs_blocks(n, 256), 256, 0, s, p, c,
+                 static_cast<const uint32_t*>(gid.get()));
+        }
+      }
     }
-    if (ctx.read_i64(over.get()) != 0) {
+    unsigned long long hm[2];
+    LDF_CUDA(cudaMemcpyAsync(hm, misc.get(), 16, cudaMemcpyDeviceToHost, s));
+    ctx.finish();
+    if (static_cast<int>(hm[1]) != 0) {
       if (attempt >= 4) fail(LDF_ERR_INTERNAL, "groupby hash table overflow");
-      cap *= 4;
-      pair_cap *= 4;
+      cap      = cap * 4;
+      pair_cap = pair_cap * 4;
       continue;
     }
+    // the id counter may pass id_cap (pool refills are clipped to it)
+    const int64_t nid = static_cast<int64_t>(std::min<unsigned long long>(hm[0], id_cap));
 
-    // ---- compact + finalize -------------------------------------------------------
-    const int64_t tiles = ceil_div(static_cast<int64_t>(nslots), kGbThreads * 4);
-    Buffer<int64_t> groups(al, nslots);
+    // ---- compact used ids + finalize ------------------------------------------
+    const int64_t tiles = std::max<int64_t>(1, ceil_div(nid, 256 * 4));
+    Buffer<int64_t> groups(al, std::max<int64_t>(nid, 1));
     Buffer<uint64_t> status(al, tiles + 2);
     Buffer<int64_t> total(al, 1);
     LDF_CUDA(cudaMemsetAsync(status.get(), 0, (tiles + 2) * 8, s));
-    launch("compact_groups", compact_groups_kernel<M>, static_cast<unsigned>(tiles), kGbThreads, 0, s, 
-      p, static_cast<int64_t>(nslots), groups.get(), status.get(),
-      reinterpret_cast<unsigned long long*>(status.get() + tiles), total.get(), ctx.err());
-    LDF_CHECK_LAUNCH();
+    launch("compact_groups", compact_groups_kernel, static_cast<unsigned>(tiles), 256, 0, s,
+           static_cast<const unsigned long long*>(states.get()), p.stride, nid, groups.get(), status.get(),
+           reinterpret_cast<unsigned long long*>(status.get() + tiles), total.get(), ctx.err());
     const int64_t G = ctx.read_i64(total.get());
 
     FinArgs f{};
@@ -921,8 +1423,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     f.nkeys    = nkeys;
     for (int j = 0; j < nkeys; ++j) {
       const ldf_column& kc = table[keys[j]];
-      bool nullable        = kc.valid != nullptr;
-      out[j]               = alloc_out_column(al, kc.type, G, nullable);
+      out[j]               = alloc_out_column(al, kc.type, G, kc.valid != nullptr);
       f.key_dst[j]         = OCol{out[j].data, out[j].valid, kc.type, type_width(kc.type)};
     }
     Buffer<int32_t> repr;
@@ -933,22 +1434,18 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     f.nagg = naggs;
     for (int a = 0; a < naggs; ++a) {
       const ldf_aggregation& ag = aggs[a];
-      bool nullable = !(ag.kind == LDF_AGG_COUNT_ALL || ag.kind == LDF_AGG_COUNT_DISTINCT);
-      out[nkeys + a] = alloc_out_column(al, ag.out_type, G, nullable);
-      AggOut& o      = f.a[a];
-      o.kind         = ag.kind;
-      o.count_mode   = ag.count_mode;
-      o.col          = agg_col[a];
-      o.in_type      = ag.kind == LDF_AGG_COUNT_ALL ? LDF_INT64 : table[ag.in_col].type;
+      const bool nullable       = !(ag.kind == LDF_AGG_COUNT_ALL || ag.kind == LDF_AGG_COUNT_DISTINCT);
+      out[nkeys + a]            = alloc_out_column(al, ag.out_type, G, nullable);
+      AggOut& o                 = f.a[a];
+      o.kind                    = ag.kind;
+      o.count_mode              = ag.count_mode;
+      o.col                     = agg_col[a];
+      o.in_type                 = ag.kind == LDF_AGG_COUNT_ALL ? LDF_INT64 : table[ag.in_col].type;
       o.dst = OCol{out[nkeys + a].data, out[nkeys + a].valid, ag.out_type, type_width(ag.out_type)};
     }
-    if (G > 0) {
-      launch("finalize", finalize_kernel, gs_blocks(G, 256), 256, 0, s, f);
-      LDF_CHECK_LAUNCH();
-    }
+    if (G > 0) launch("finalize", finalize_kernel, gs_blocks(G, 256), 256, 0, s, f);
     for (int j = 0; j < nkeys; ++j)
-      if (table[keys[j]].type == LDF_STRING)
-        gather_strings(ctx, make_dcol(table[keys[j]]), repr.get(), G, out[j]);
+      if (table[keys[j]].type == LDF_STRING) gather_strings(ctx, make_dcol(table[keys[j]]), repr.get(), G, out[j]);
     ctx.finish();
     return;
   }
@@ -961,7 +1458,7 @@ void groupby_aggregation(const ldf_column* table, int ncols, const int32_t* keys
 {
   if (nkeys < 1) fail(LDF_ERR_INVALID_ARGUMENT, "must pass at least one key column");
   LDF_REQUIRE(naggs <= kMaxAggs, "too many aggregations");
-  KeyCols k = make_keys(table, ncols, keys, nkeys);
+  KeyCols k       = make_keys(table, ncols, keys, nkeys);
   const int64_t n = ncols > 0 ? table[0].size : 0;
   LDF_REQUIRE(n < (int64_t(1) << 31), "tables of 2^31 rows or more per task are not supported");
   GbPlan p{};
@@ -981,13 +1478,13 @@ void groupby_aggregation(const ldf_column* table, int ncols, const int32_t* keys
       LDF_REQUIRE(p.ncols < kMaxAggCols, "too many distinct aggregation input columns");
       ci = p.ncols++;
       col_of_plan.push_back(ag.in_col);
-      ColPlan& cp = p.c[ci];
-      cp.col      = make_dcol(c);
-      cp.fixed    = is_float(c.type) ? 1 : 0;
-      cp.limbs    = cp.fixed ? 3 : 1;
+      ColPlan& cp    = p.c[ci];
+      cp.col         = make_dcol(c);
+      cp.nullable    = c.valid != nullptr;
+      cp.fixed       = is_float(c.type) ? 1 : 0;
       cp.pair_packed = type_width(c.type) <= 4 && c.type != LDF_STRING;
     }
-    agg_col[a] = ci;
+    agg_col[a]  = ci;
     ColPlan& cp = p.c[ci];
     switch (ag.kind) {
       case LDF_AGG_SUM:

@@ -163,6 +163,9 @@ def group_ids(table: pa.Table, keys):
     gid = _composite(code_cols)
     if len(gid) == 0:
         return gid, np.zeros(0, dtype=np.int64)
+    # dense ids: a null row's placeholder value may be absent from the valid rows
+    _, gid = np.unique(gid, return_inverse=True)
+    gid = gid.reshape(-1).astype(np.int64)
     first = np.full(gid.max() + 1, len(gid), dtype=np.int64)
     np.minimum.at(first, gid, np.arange(len(gid)))
     return gid, first

@@ -96,9 +96,9 @@ def test_join_config0_shape():
     l_rng, r_rng = np.random.default_rng(1), np.random.default_rng(2)
     n = 1_000_000
     lhs = pa.table({"key": l_rng.integers(0, 1 << 20, n), "payload": l_rng.integers(-2**40, 2**40, n)})
-    rhs = pa.table({"key": r_rng.integers(0, 1 << 20, n), "payload_r": r_rng.integers(-2**40, 2**40, n)})
-    res = run_join(lhs, rhs, ["key"], ["key"], "inner")
-    exp = R.join(lhs, rhs, ["key"], ["key"], "inner")
+    rhs = pa.table({"key_r": r_rng.integers(0, 1 << 20, n), "payload_r": r_rng.integers(-2**40, 2**40, n)})
+    res = run_join(lhs, rhs, ["key"], ["key_r"], "inner")
+    exp = R.join(lhs, rhs, ["key"], ["key_r"], "inner")
     assert res.num_rows == exp.num_rows
     assert_tables_equal(res, exp)
 
@@ -106,18 +106,19 @@ def test_join_config0_shape():
 @pytest.mark.parametrize("how", list(HOW))
 def test_join_empty(how):
     e = pa.table({"k": pa.array([], pa.int64()), "v": pa.array([], pa.float64())})
-    f = pa.table({"k": pa.array([1, 2, 2], pa.int64()), "w": pa.array([1.0, 2.0, 3.0])})
-    for lhs, rhs in ((e, f), (f.rename_columns(["k", "v"]), e.rename_columns(["k", "w"])), (e, e.rename_columns(["k", "w"]))):
-        res = run_join(lhs, rhs, ["k"], ["k"], how)
-        exp = R.join(lhs, rhs, ["k"], ["k"], how)
+    f = pa.table({"k": pa.array([1, 2, 2], pa.int64()), "v": pa.array([1.0, 2.0, 3.0])})
+    for lhs, rhs in ((e, f), (f, e), (e, e)):
+        rhs = rhs.rename_columns(["kr", "w"])
+        res = run_join(lhs, rhs, ["k"], ["kr"], how)
+        exp = R.join(lhs, rhs, ["k"], ["kr"], how)
         assert_tables_equal(res, exp)
 
 
 def test_join_all_null_keys():
     lhs = pa.table({"k": pa.array([None] * 5, pa.int32()), "v": np.arange(5)})
-    rhs = pa.table({"k": pa.array([None, 1, None], pa.int32()), "w": np.arange(3)})
+    rhs = pa.table({"kr": pa.array([None, 1, None], pa.int32()), "w": np.arange(3)})
     for how in HOW:
         for ne in (True, False):
-            res = run_join(lhs, rhs, ["k"], ["k"], how, ne)
-            exp = R.join(lhs, rhs, ["k"], ["k"], how, ne)
+            res = run_join(lhs, rhs, ["k"], ["kr"], how, ne)
+            exp = R.join(lhs, rhs, ["k"], ["kr"], how, ne)
             assert_tables_equal(res, exp)
