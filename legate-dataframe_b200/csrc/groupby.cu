@@ -31,7 +31,7 @@
 //    integer adds are associative, so the result is independent of thread
 //    order and bit-identical alone or in a batch.
 //  * NUNIQUE: (group id, value) pairs in a pair set; first insertions count.
-#include "table_ops.cuh"
+#include "radix.cuh"
 
 #include <cmath>
 #include <cstdio>
@@ -188,7 +188,8 @@ __device__ __forceinline__ void red_max(unsigned long long* p, uint64_t v)
 }
 
 // Add +-m << s into the chunk accumulators acc[0..5].
-__device__ __forceinline__ void add_fixed_chunks(unsigned long long* acc, uint64_t m, int s, bool neg)
+__device__ __forceinline__ void add_fixed_chunks(unsigned long long* acc, uint64_t m, int s, bool neg,
+                                                 uint64_t cstride = 1)
 {
   if (m == 0) return;
   const int j0 = s >> 5, j1 = (s + 52) >> 5;
@@ -196,17 +197,17 @@ __device__ __forceinline__ void add_fixed_chunks(unsigned long long* acc, uint64
     const int off   = 32 * j - s;  // bit of m that lands at chunk bit 0
     uint64_t chunk  = off >= 0 ? (m >> off) : (m << (-off));
     chunk &= 0xffffffffull;
-    if (chunk) red_add(acc + j, neg ? (0ull - chunk) : chunk);
+    if (chunk) red_add(acc + j * cstride, neg ? (0ull - chunk) : chunk);
   }
 }
 
 // Exact value of sum_j acc_j * 2^(32j - 96), correctly rounded to double.
-__device__ __forceinline__ double chunks_to_double(const unsigned long long* acc)
+__device__ __forceinline__ double chunks_to_double(const unsigned long long* acc, uint64_t cstride = 1)
 {
   // 256-bit two's complement accumulation of the signed partials
   uint64_t w[4] = {0, 0, 0, 0};
   for (int j = 0; j < kSumChunks; ++j) {
-    const int64_t a = static_cast<int64_t>(acc[j]);
+    const int64_t a = static_cast<int64_t>(acc[j * cstride]);
     uint64_t t[5]   = {0, 0, 0, 0, 0};
     const int sh = 32 * j, li = sh >> 6, bi = sh & 63;
     const uint64_t lo = static_cast<uint64_t>(a);
@@ -542,8 +543,9 @@ struct ColArgs {
   uint32_t states;
   int sum_chunks;  // 6 (float, fixed point) or 2 (integer magnitude)
   int off_vcount, off_sum, off_mn, off_mx;
-  unsigned long long* rec;  // group records
-  int stride;
+  unsigned long long* rec;  // group records, field-major: word w of group g at rec[w * ld + g]
+  uint64_t ld;
+  const uint32_t* newid;    // assign-pass id -> frequency rank
   double* fb;
   unsigned int* special;
   int hot;
@@ -613,6 +615,7 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
       const int64_t r = base + static_cast<int64_t>(j) * blockDim.x + threadIdx.x;
       ok[j]           = r < a.n;
       g[j] = ok[j] ? __ldg(a.gid + r) : kUnsetId;
+      if (g[j] != kUnsetId) g[j] = __ldg(a.newid + g[j]);
       raw[j] = ok[j] ? load_raw<W, SGN, FLT>(a.col.data, r) : 0;
       if (ok[j] && a.nullable) ok[j] = __ldg(a.col.valid + r) != 0;
       ok[j] = ok[j] && g[j] != kUnsetId;
@@ -667,8 +670,9 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
           }
         }
       } else {
-        unsigned long long* rec = a.rec + static_cast<int64_t>(gg) * a.stride;
-        if (a.nullable) red_add(rec + a.off_vcount, 1);
+        unsigned long long* rec = a.rec + gg;
+        const uint64_t L        = a.ld;
+        if (a.nullable) red_add(rec + a.off_vcount * L, 1);
         if (a.states & ST_SUM) {
           if (FLT) {
             const double x = W == 8 ? __longlong_as_double(static_cast<long long>(raw[j]))
@@ -676,7 +680,7 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
             uint64_t m;
             int sh;
             bool neg;
-            if (fixed_parts(x, m, sh, neg)) add_fixed_chunks(rec + a.off_sum, m, sh, neg);
+            if (fixed_parts(x, m, sh, neg)) add_fixed_chunks(rec + a.off_sum * L, m, sh, neg, L);
             else if (isnan(x)) atomicOr(a.special + gg, SP_NAN);
             else if (isinf(x)) atomicOr(a.special + gg, x > 0 ? SP_PINF : SP_NINF);
             else atomicAdd(a.fb + gg, x);
@@ -687,24 +691,25 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
                                : W == 4 ? static_cast<int32_t>(raw[j]) : static_cast<int64_t>(raw[j]);
               v = static_cast<uint64_t>(sv);
             }
-            red_add(rec + a.off_sum, v);
+            red_add(rec + a.off_sum * L, v);
           }
         }
         if (a.states & (ST_MIN | ST_MAX)) {
           const uint64_t o = ordered64<W, SGN, FLT>(raw[j]);
-          if (a.states & ST_MIN) red_max(rec + a.off_mn, ~o);
-          if (a.states & ST_MAX) red_max(rec + a.off_mx, o);
+          if (a.states & ST_MIN) red_max(rec + a.off_mn * L, ~o);
+          if (a.states & ST_MAX) red_max(rec + a.off_mx * L, o);
         }
       }
     }
   }
   __syncthreads();
   for (int gg = threadIdx.x; gg < H; gg += blockDim.x) {
-    unsigned long long* rec = a.rec + static_cast<int64_t>(gg) * a.stride;
+    unsigned long long* rec = a.rec + gg;
+    const uint64_t L        = a.ld;
     if (a.nullable) {
       const uint32_t vc = reinterpret_cast<const uint32_t*>(smem + a.sh_vcount)[gg];
       if (vc == 0) continue;
-      red_add(rec + a.off_vcount, vc);
+      red_add(rec + a.off_vcount * L, vc);
     }
     if (a.states & ST_SUM) {
       const uint32_t* sum = reinterpret_cast<const uint32_t*>(smem + a.sh_sum) + static_cast<int64_t>(gg) * a.sum_chunks * 4;
@@ -712,7 +717,7 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
         for (int q = 0; q < a.sum_chunks; ++q) {
           const int64_t pos = static_cast<int64_t>(sum[q * 4 + 0]) + (static_cast<int64_t>(sum[q * 4 + 1]) << 32);
           const int64_t neg = static_cast<int64_t>(sum[q * 4 + 2]) + (static_cast<int64_t>(sum[q * 4 + 3]) << 32);
-          if (pos != neg) red_add(rec + a.off_sum + q, static_cast<uint64_t>(pos - neg));
+          if (pos != neg) red_add(rec + (a.off_sum + q) * L, static_cast<uint64_t>(pos - neg));
         }
       } else {
         uint64_t tot = 0;  // integer sum mod 2^64
@@ -721,22 +726,22 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
           const uint64_t neg = static_cast<uint64_t>(sum[q * 4 + 2]) + (static_cast<uint64_t>(sum[q * 4 + 3]) << 32);
           tot += (pos - neg) << (32 * q);
         }
-        if (tot) red_add(rec + a.off_sum, tot);
+        if (tot) red_add(rec + a.off_sum * L, tot);
       }
     }
     if (a.states & (ST_MIN | ST_MAX)) {
       // groups of a non-nullable column reach here with or without rows in
       // this CTA: an untouched max word 0 is the identity either way
       if (MM64) {
-        if (a.states & ST_MIN) red_max(rec + a.off_mn, reinterpret_cast<const unsigned long long*>(smem + a.sh_mn)[gg]);
-        if (a.states & ST_MAX) red_max(rec + a.off_mx, reinterpret_cast<const unsigned long long*>(smem + a.sh_mx)[gg]);
+        if (a.states & ST_MIN) red_max(rec + a.off_mn * L, reinterpret_cast<const unsigned long long*>(smem + a.sh_mn)[gg]);
+        if (a.states & ST_MAX) red_max(rec + a.off_mx * L, reinterpret_cast<const unsigned long long*>(smem + a.sh_mx)[gg]);
       } else {
         const uint32_t mn = reinterpret_cast<const uint32_t*>(smem + a.sh_mn)[gg];
         const uint32_t mx = reinterpret_cast<const uint32_t*>(smem + a.sh_mx)[gg];
         // an untouched word (no row of this group here) flushes the identity
         // of the opposite extreme, which never wins
-        if (a.states & ST_MIN) red_max(rec + a.off_mn, ~widen32<W, SGN, FLT>(~mn));
-        if (a.states & ST_MAX) red_max(rec + a.off_mx, widen32<W, SGN, FLT>(mx));
+        if (a.states & ST_MIN) red_max(rec + a.off_mn * L, ~widen32<W, SGN, FLT>(~mn));
+        if (a.states & ST_MAX) red_max(rec + a.off_mx * L, widen32<W, SGN, FLT>(mx));
       }
     }
   }
@@ -749,12 +754,13 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
 constexpr int kPairsPerThread = 8;
 struct NdArgs {
   const uint32_t* gid;
+  const uint32_t* newid;
   DCol col;
   int64_t n;
   unsigned long long* set;
   uint64_t cap;
-  unsigned long long* states;
-  int stride, off_nd, hot;
+  unsigned long long* nd;  // distinct-count field (indexed by frequency rank)
+  int hot;
   int* overflow;
 };
 
@@ -773,7 +779,8 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
       e[j]            = kEmpty;
       if (r < a.n && dvalid(a.col, r)) {
         const uint32_t g = __ldg(a.gid + r);
-        if (g != kUnsetId) e[j] = (static_cast<uint64_t>(g) << 32) | static_cast<uint32_t>(dbits(a.col, r));
+        if (g != kUnsetId)
+          e[j] = (static_cast<uint64_t>(__ldg(a.newid + g)) << 32) | static_cast<uint32_t>(dbits(a.col, r));
       }
       idx[j] = e[j] != kEmpty ? fastrange(mix64(e[j]), a.cap) : 0;
     }
@@ -802,24 +809,26 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
       if (!fresh) continue;
       const uint32_t g = static_cast<uint32_t>(e[j] >> 32);
       if (g < static_cast<uint32_t>(a.hot)) atomicAdd(cnt + g, 1u);
-      else red_add(a.states + static_cast<int64_t>(g) * a.stride + a.off_nd, 1);
+      else red_add(a.nd + g, 1);
     }
   }
   __syncthreads();
   for (int g = threadIdx.x; g < a.hot; g += blockDim.x)
-    if (cnt[g]) red_add(a.states + static_cast<int64_t>(g) * a.stride + a.off_nd, cnt[g]);
+    if (cnt[g]) red_add(a.nd + g, cnt[g]);
 }
 
 // NUNIQUE of 8-byte or string values: pairs hashed on (group, value) with the
 // representative row in the set (generic, slower path).
 template <KeyMode M>
-__global__ void nunique_generic_kernel(GbPlan p, ColPlan c, const uint32_t* gid)
+__global__ void nunique_generic_kernel(GbPlan p, ColPlan c, const uint32_t* gid, const uint32_t* newid,
+                                       unsigned long long* nd)
 {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < p.n; r += (int64_t)gridDim.x * blockDim.x) {
     if (!dvalid(c.col, r)) continue;
-    const uint32_t g = gid[r];
+    uint32_t g = gid[r];
     if (g == kUnsetId) continue;
-    if (pair_insert(p, c, g, r)) red_add(p.states + static_cast<int64_t>(g) * p.stride + c.off_nd, 1);
+    g = newid[g];
+    if (pair_insert(p, c, g, r)) red_add(nd + g, 1);
   }
 }
 
@@ -944,6 +953,25 @@ __global__ void fill_kernel(T* p, int64_t n, T v)
     p[i] = v;
 }
 
+// ---- frequency ranks --------------------------------------------------------
+// key = ~count: an ascending stable sort puts the most frequent ids first and
+// unused ids (holes, count 0) last.
+__global__ void rank_keys_kernel(const unsigned long long* counts, int64_t nid, uint32_t* key)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nid; i += (int64_t)gridDim.x * blockDim.x)
+    key[i] = ~static_cast<uint32_t>(counts[i]);
+}
+// newid[perm[i]] = i; the count field (field 0) of rank i
+__global__ void rank_scatter_kernel(const int32_t* perm, int64_t nid, const unsigned long long* counts,
+                                    uint32_t* newid, unsigned long long* count_field)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nid; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t old = perm[i];
+    newid[old]        = static_cast<uint32_t>(i);
+    count_field[i]    = counts[old];
+  }
+}
+
 // ---- compaction of the used ids (record count > 0) ---------------------------
 __global__ void __launch_bounds__(256)
   compact_groups_kernel(const unsigned long long* states, int stride, int64_t nid, int64_t* groups,
@@ -986,6 +1014,9 @@ struct AggOut {
 };
 struct FinArgs {
   GbPlan p;
+  const unsigned long long* rec;  // field-major records of the frequency ranks
+  uint64_t ld;
+  const int32_t* perm;            // rank -> assign-pass id
   int key_mode;
   const int64_t* groups;
   int64_t ngroups;
@@ -1033,7 +1064,7 @@ __device__ __forceinline__ uint64_t unordered_bits(int type, uint64_t o)
   }
 }
 
-__device__ __forceinline__ double float_sum(const ColPlan& c, const unsigned long long* rec, int64_t id,
+__device__ __forceinline__ double float_sum(const ColPlan& c, const unsigned long long* rec, uint64_t L, int64_t id,
                                             bool& special, double& sval)
 {
   unsigned int sp = c.special[id];
@@ -1043,19 +1074,21 @@ __device__ __forceinline__ double float_sum(const ColPlan& c, const unsigned lon
     else sval = (sp & SP_PINF) ? __longlong_as_double(0x7ff0000000000000ll)
                                : __longlong_as_double(0xfff0000000000000ll);
   }
-  return chunks_to_double(rec + c.off_sum) + c.fb[id];
+  return chunks_to_double(rec + c.off_sum * L, L) + c.fb[id];
 }
 
 __global__ void finalize_kernel(FinArgs f)
 {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < f.ngroups;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t id              = f.groups[i];
+    const int64_t id              = f.groups[i];  // frequency rank
     const GbPlan& p               = f.p;
-    const unsigned long long* rec = p.states + id * p.stride;
+    const uint64_t L              = f.ld;
+    const unsigned long long* rec = f.rec + id;
+    const int64_t old             = f.perm[id];  // assign-pass id
     // keys
     if (f.key_mode == static_cast<int>(KeyMode::GEN)) {
-      const int64_t rr = static_cast<int64_t>(p.id_key[id]);
+      const int64_t rr = static_cast<int64_t>(p.id_key[old]);
       f.repr[i]        = static_cast<int32_t>(rr);
       for (int j = 0; j < f.nkeys; ++j) {
         const OCol& d = f.key_dst[j];
@@ -1065,8 +1098,8 @@ __global__ void finalize_kernel(FinArgs f)
       }
     } else {
       const OCol& d      = f.key_dst[0];
-      const bool is_null = id == kIdNull;
-      const uint64_t kb  = id == kIdSentinel ? kSentinel64 : is_null ? 0 : p.id_key[id];
+      const bool is_null = old == kIdNull;
+      const uint64_t kb  = old == kIdSentinel ? kSentinel64 : is_null ? 0 : p.id_key[old];
       store_int(OCol{d.data, nullptr, LDF_UINT64, d.width}, i, kb);
       if (d.valid) d.valid[i] = is_null ? 0 : 1;
     }
@@ -1080,7 +1113,7 @@ __global__ void finalize_kernel(FinArgs f)
         continue;
       }
       const ColPlan& c  = p.c[o.col];
-      const uint64_t vc = c.nullable ? rec[c.off_vcount] : call;
+      const uint64_t vc = c.nullable ? rec[c.off_vcount * L] : call;
       bool ok           = vc > 0;
       switch (o.kind) {
         case LDF_AGG_COUNT: {
@@ -1091,7 +1124,7 @@ __global__ void finalize_kernel(FinArgs f)
         }
         case LDF_AGG_COUNT_DISTINCT: {
           uint64_t has_null = call > vc ? 1 : 0;
-          uint64_t nd       = (c.states & ST_NDIST) ? rec[c.off_nd] : 0;
+          uint64_t nd       = (c.states & ST_NDIST) ? rec[c.off_nd * L] : 0;
           uint64_t v = o.count_mode == LDF_COUNT_ALL ? nd + has_null : o.count_mode == LDF_COUNT_ONLY_NULL ? has_null : nd;
           store_int(d, i, v);
           ok = true;
@@ -1106,12 +1139,12 @@ __global__ void finalize_kernel(FinArgs f)
           if (c.fixed) {
             bool special;
             double sval;
-            double sv = float_sum(c, rec, id, special, sval);
+            double sv = float_sum(c, rec, L, id, special, sval);
             if (special) sv = sval;
             if (o.kind == LDF_AGG_MEAN) sv = sv / static_cast<double>(vc);
             store_double(d, i, sv);
           } else {
-            const uint64_t s = rec[c.off_sum];
+            const uint64_t s = rec[c.off_sum * L];
             const double sd  = is_signed_int_dev(o.in_type) ? static_cast<double>(static_cast<int64_t>(s))
                                                             : static_cast<double>(s);
             if (o.kind == LDF_AGG_MEAN) store_double(d, i, sd / static_cast<double>(vc));
@@ -1126,7 +1159,7 @@ __global__ void finalize_kernel(FinArgs f)
             store_int(d, i, 0);
             break;
           }
-          const uint64_t o64 = o.kind == LDF_AGG_MIN ? ~rec[c.off_mn] : rec[c.off_mx];
+          const uint64_t o64 = o.kind == LDF_AGG_MIN ? ~rec[c.off_mn * L] : rec[c.off_mx * L];
           const uint64_t b   = unordered_bits(o.in_type, o64);
           if (d.type == o.in_type) {
             store_int(OCol{d.data, nullptr, LDF_UINT64, d.width}, i, b);
@@ -1282,7 +1315,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     const uint64_t id_cap = cap + kIdFirst;
     const int sw          = M == KeyMode::K32 ? 1 : 2;
     Buffer<unsigned long long> slots(al, cap * sw);
-    Buffer<unsigned long long> states(al, id_cap * p.stride);
+    Buffer<unsigned long long> counts(al, id_cap);  // rows per assign-pass id
     Buffer<unsigned long long> id_key(al, id_cap);
     Buffer<unsigned long long> misc(al, 4);  // id counter, overflow, chunk counter
     Buffer<uint32_t> gid(al, std::max<int64_t>(n, 1));
@@ -1290,7 +1323,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     if (M == KeyMode::K64)
       launch("fill_key_words", fill_stride_kernel, gs_blocks(cap, 256), 256, 0, s, slots.get(),
              static_cast<int64_t>(cap), 2, kSentinel64);
-    LDF_CUDA(cudaMemsetAsync(states.get(), 0, static_cast<size_t>(kIdFirst) * p.stride * 8, s));  // reserved ids
+    LDF_CUDA(cudaMemsetAsync(counts.get(), 0, static_cast<size_t>(kIdFirst) * 8, s));  // reserved ids
     const unsigned long long first = kIdFirst;
     LDF_CUDA(cudaMemsetAsync(misc.get(), 0, 32, s));
     LDF_CUDA(cudaMemcpyAsync(misc.get(), &first, 8, cudaMemcpyHostToDevice, s));
@@ -1298,7 +1331,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     p.cap           = cap;
     p.id_counter    = misc.get();
     p.id_cap        = id_cap;
-    p.states        = states.get();
+    p.states        = counts.get();
     p.id_key        = id_key.get();
     p.overflow      = reinterpret_cast<int*>(misc.get() + 1);
     p.chunk_counter = misc.get() + 2;
@@ -1326,21 +1359,70 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
       }
     }
 
+    Buffer<int32_t> perm;
+    Buffer<uint32_t> newid;
+    Buffer<unsigned long long> rec;
+    uint64_t L  = 1;
+    int64_t nid = 0;
     if (n > 0) {
-      // pass 1: group ids + row counts
-      p.hot                 = std::min(hot_cap, (kSmemBudget - 64) / 4);
-      const size_t a_smem   = static_cast<size_t>(p.hot) * 4;
+      // pass 1: group ids + row counts (per assign-pass id)
+      GbPlan pa             = p;
+      pa.states             = counts.get();
+      pa.stride             = 1;
+      pa.hot                = std::min(hot_cap, (kSmemBudget - 64) / 4);
+      const size_t a_smem   = static_cast<size_t>(pa.hot) * 4;
       int occ               = 1;
       LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, assign_kernel<M>, kGbThreads, a_smem));
       const int64_t ablocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(occ, 1),
                                                 ceil_div(n, int64_t(kGbThreads) * kRows));
-      launch("assign", assign_kernel<M>, static_cast<unsigned>(ablocks), kGbThreads, a_smem, s, p, gid.get());
+      launch("assign", assign_kernel<M>, static_cast<unsigned>(ablocks), kGbThreads, a_smem, s, pa, gid.get());
+      unsigned long long hm[2];
+      LDF_CUDA(cudaMemcpyAsync(hm, misc.get(), 16, cudaMemcpyDeviceToHost, s));
+      ctx.finish();
+      if (static_cast<int>(hm[1]) != 0) {
+        if (attempt >= 4) fail(LDF_ERR_INTERNAL, "groupby hash table overflow");
+        cap      = cap * 4;
+        pair_cap = pair_cap * 4;
+        continue;
+      }
+      // the id counter may pass id_cap (pool refills are clipped to it)
+      nid = static_cast<int64_t>(std::min<unsigned long long>(hm[0], id_cap));
+
+      // frequency ranks: sort ids by descending row count (stable radix sort)
+      Buffer<uint32_t> rkey(al, nid);
+      launch("rank_keys", rank_keys_kernel, gs_blocks(nid, 256), 256, 0, s,
+             static_cast<const unsigned long long*>(counts.get()), nid, rkey.get());
+      perm = Buffer<int32_t>(al, nid);
+      {
+        DCol kc{};
+        kc.data  = rkey.get();
+        kc.type  = LDF_UINT32;
+        kc.width = 4;
+        std::vector<RadixPass> passes;
+        for (int b = 0; b < 4; ++b) {
+          RadixPass rp{};
+          rp.src   = DigitSrc::COLUMN;
+          rp.shift = 8 * b;
+          rp.key   = SortKeyDesc{kc, 0, 1, 4};
+          passes.push_back(rp);
+        }
+        radix_sort_rows(ctx, passes, nid, perm.get());
+      }
+      newid = Buffer<uint32_t>(al, nid);
+      L     = static_cast<uint64_t>(nid);
+      rec   = Buffer<unsigned long long>(al, L * p.stride);
+      LDF_CUDA(cudaMemsetAsync(rec.get(), 0, L * p.stride * 8, s));
+      launch("rank_scatter", rank_scatter_kernel, gs_blocks(nid, 256), 256, 0, s,
+             static_cast<const int32_t*>(perm.get()), nid, static_cast<const unsigned long long*>(counts.get()),
+             newid.get(), rec.get());
+
       // pass 2: one kernel per value column that needs valid counts / sums / min / max
       for (int ci = 0; ci < p.ncols; ++ci) {
         ColPlan& c = p.c[ci];
         if (!c.nullable && !(c.states & (ST_SUM | ST_MIN | ST_MAX))) continue;
         ColArgs a{};
         a.gid        = gid.get();
+        a.newid      = newid.get();
         a.n          = n;
         a.col        = c.col;
         a.nullable   = c.nullable;
@@ -1350,14 +1432,14 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
         a.off_sum    = c.off_sum;
         a.off_mn     = c.off_mn;
         a.off_mx     = c.off_mx;
-        a.rec        = p.states;
-        a.stride     = p.stride;
+        a.rec        = rec.get();
+        a.ld         = L;
         a.fb         = c.fb;
         a.special    = c.special;
         const int mmw = c.mm64 ? 8 : 4;
         const int per = (c.nullable ? 4 : 0) + ((a.states & ST_SUM) ? 16 * c.sum_chunks : 0) +
                         ((a.states & ST_MIN) ? mmw : 0) + ((a.states & ST_MAX) ? mmw : 0);
-        a.hot         = std::min(hot_cap, (kSmemBudget - 256) / std::max(per, 1));
+        a.hot         = static_cast<int>(std::min<int64_t>(std::min(hot_cap, (kSmemBudget - 256) / std::max(per, 1)), nid));
         int off       = 0;
         auto take     = [&](int bytes_per) {
           const int o = off;
@@ -1378,8 +1460,8 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
         ColPlan& c = p.c[ci];
         if (!(c.states & ST_NDIST)) continue;
         if (c.pair_packed) {
-          NdArgs na{gid.get(), c.col, n, c.pairs, c.pair_cap, p.states, p.stride, c.off_nd,
-                    std::min(hot_cap, 12 * 1024), p.overflow};
+          NdArgs na{gid.get(), newid.get(), c.col, n, c.pairs, c.pair_cap, rec.get() + c.off_nd * L,
+                    static_cast<int>(std::min<int64_t>(std::min(hot_cap, 12 * 1024), nid)), p.overflow};
           const size_t nd_smem = static_cast<size_t>(na.hot) * 4;
           int nocc             = 1;
           LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nocc, nunique_kernel, kGbThreads, nd_smem));
@@ -1388,35 +1470,36 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
           launch("nunique", nunique_kernel, static_cast<unsigned>(nblocks), kGbThreads, nd_smem, s, na);
         } else {
           launch("nunique_generic", nunique_generic_kernel<M>, gs_blocks(n, 256), 256, 0, s, p, c,
-                 static_cast<const uint32_t*>(gid.get()));
+                 static_cast<const uint32_t*>(gid.get()), static_cast<const uint32_t*>(newid.get()),
+                 rec.get() + c.off_nd * L);
         }
       }
+      LDF_CUDA(cudaMemcpyAsync(hm, misc.get(), 16, cudaMemcpyDeviceToHost, s));
+      ctx.finish();
+      if (static_cast<int>(hm[1]) != 0) {  // the pair set overflowed
+        if (attempt >= 4) fail(LDF_ERR_INTERNAL, "groupby hash table overflow");
+        cap      = cap * 4;
+        pair_cap = pair_cap * 4;
+        continue;
+      }
     }
-    unsigned long long hm[2];
-    LDF_CUDA(cudaMemcpyAsync(hm, misc.get(), 16, cudaMemcpyDeviceToHost, s));
-    ctx.finish();
-    if (static_cast<int>(hm[1]) != 0) {
-      if (attempt >= 4) fail(LDF_ERR_INTERNAL, "groupby hash table overflow");
-      cap      = cap * 4;
-      pair_cap = pair_cap * 4;
-      continue;
-    }
-    // the id counter may pass id_cap (pool refills are clipped to it)
-    const int64_t nid = static_cast<int64_t>(std::min<unsigned long long>(hm[0], id_cap));
 
-    // ---- compact used ids + finalize ------------------------------------------
+    // ---- used ranks (count > 0; holes sort last) + finalize ---------------------
     const int64_t tiles = std::max<int64_t>(1, ceil_div(nid, 256 * 4));
     Buffer<int64_t> groups(al, std::max<int64_t>(nid, 1));
     Buffer<uint64_t> status(al, tiles + 2);
     Buffer<int64_t> total(al, 1);
     LDF_CUDA(cudaMemsetAsync(status.get(), 0, (tiles + 2) * 8, s));
     launch("compact_groups", compact_groups_kernel, static_cast<unsigned>(tiles), 256, 0, s,
-           static_cast<const unsigned long long*>(states.get()), p.stride, nid, groups.get(), status.get(),
+           static_cast<const unsigned long long*>(rec.get()), 1, nid, groups.get(), status.get(),
            reinterpret_cast<unsigned long long*>(status.get() + tiles), total.get(), ctx.err());
     const int64_t G = ctx.read_i64(total.get());
 
     FinArgs f{};
     f.p        = p;
+    f.rec      = rec.get();
+    f.ld       = L;
+    f.perm     = perm.get();
     f.key_mode = static_cast<int>(M);
     f.groups   = groups.get();
     f.ngroups  = G;
