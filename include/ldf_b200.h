@@ -163,6 +163,27 @@ int ldf_b200_hash_partition(const ldf_column* table, int32_t ncols,
                             ldf_column* out, int64_t* offsets,
                             const ldf_allocator* alloc, void* stream);
 
+/* ---- hash partition without device allocation ----------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory themselves -- a task body running concurrently with other tasks on the
+ * same GPU, where cudaMalloc synchronizes the device and can deadlock with
+ * them, or a host whose device memory is all handed to its own pool.  Same
+ * result as ldf_b200_hash_partition, for fixed-width columns, at most
+ * LDF_B200_NOALLOC_MAX_ROWS rows and at most 256 buckets; larger inputs are
+ * rejected with LDF_ERR_INVALID_ARGUMENT.  The caller passes the output
+ * buffers in `out` (out[j].data: rows x width bytes; out[j].valid: rows bytes
+ * for a nullable input column); the call fills them and sets the other
+ * fields.  All scratch is one fixed array (about 5 MiB) in the library's
+ * device image, held by every GPU that loads the library until the process
+ * exits; no cudaMalloc/cudaFree or allocating library routine is called.  The
+ * first call on a device looks up the array's device address, so make that
+ * first call before any stream capture.  Every call shares the array: calls
+ * whose work overlaps on the GPU race and must be serialized. */
+#define LDF_B200_NOALLOC_MAX_ROWS (1 << 20)
+int ldf_b200_hash_partition_noalloc(const ldf_column* table, int32_t ncols,
+                                    const int32_t* keys, int32_t nkeys, int32_t nparts,
+                                    ldf_column* out, int64_t* offsets, void* stream);
+
 /* ---- utilities ---------------------------------------------------------- */
 /* Message of the last failed call on this thread ("" if none). */
 const char* ldf_b200_last_error(void);

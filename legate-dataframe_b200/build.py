@@ -29,6 +29,7 @@ SOURCES = [
     "radix.cu",
     "sort.cu",
     "abi.cu",
+    "noalloc.cu",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

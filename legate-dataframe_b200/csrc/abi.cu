@@ -52,6 +52,10 @@ void check_table(const ldf_column* t, int32_t ncols, const char* what)
 }
 }  // namespace
 
+namespace ldf {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace ldf
+
 extern "C" {
 
 const char* ldf_b200_last_error(void) { return g_last_error.c_str(); }

@@ -361,3 +361,41 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
 }
 
 }  // namespace ldf
+
+// ---- raw-pointer helpers for the no-allocation hash partition ---------------
+namespace ldf {
+
+void radix_histogram_raw(cudaStream_t s, const RadixPass& p, int64_t n, uint32_t* d_hist)
+{
+  LDF_CUDA(cudaMemsetAsync(d_hist, 0, 256 * sizeof(uint32_t), s));
+  if (n <= 0) return;
+  HistArgs h{};
+  h.npasses = 1;
+  h.p[0]    = p;
+  h.n       = n;
+  h.hist    = d_hist;
+  launch("histogram", histogram_kernel, hblocks(n), RT, 0, s, h);
+}
+
+int64_t radix_status_words(int64_t n) { return ceil_div(n, RTILE) * 256 + 2; }
+
+void onesweep_gather_pass_raw(cudaStream_t s, const RadixPass& p, int64_t n, int32_t* rows_out,
+                              const uint64_t* d_bases, uint64_t* status, int* err)
+{
+  if (n <= 0) return;
+  const int64_t tiles = ceil_div(n, RTILE);
+  PassArgs a{};
+  a.p          = p;
+  a.n          = n;
+  a.keys_in    = nullptr;
+  a.keys_out   = nullptr;
+  a.vals_in    = nullptr;
+  a.vals_out   = rows_out;
+  a.digit_base = d_bases;
+  a.status     = status;
+  a.counter    = reinterpret_cast<unsigned long long*>(status + tiles * 256);
+  a.err        = err;
+  launch("onesweep", onesweep_kernel<true, false>, static_cast<unsigned>(tiles), RT, 0, s, a);
+}
+
+}  // namespace ldf

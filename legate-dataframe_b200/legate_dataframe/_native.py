@@ -54,6 +54,8 @@ LDF_AGG = {
     "sum": 0, "min": 1, "max": 2, "count": 3, "count_all": 4, "mean": 5,
     "count_distinct": 6, "product": 7, "variance": 8, "stddev": 9,
 }
+NOALLOC_MAX_ROWS = 1 << 20  # LDF_B200_NOALLOC_MAX_ROWS
+
 LDF_COUNT_ONLY_VALID = 0
 LDF_COUNT_ONLY_NULL = 1
 LDF_COUNT_ALL = 2
@@ -130,6 +132,11 @@ def lib():
                 P(ldf_column), P(ctypes.c_int64), P(ldf_allocator), ctypes.c_void_p,
             ]
             L.ldf_b200_free_column.argtypes = [P(ldf_column), P(ldf_allocator), ctypes.c_void_p]
+            L.ldf_b200_hash_partition_noalloc.argtypes = [
+                P(ldf_column), ctypes.c_int32, i32p, ctypes.c_int32, ctypes.c_int32,
+                P(ldf_column), P(ctypes.c_int64), ctypes.c_void_p,
+            ]
+            L.ldf_b200_hash_partition_noalloc.restype = ctypes.c_int
             L.ldf_b200_launch_count.restype = ctypes.c_ulonglong
             L.ldf_b200_profile_enable.argtypes = [ctypes.c_int]
             L.ldf_b200_profile_report.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int]
