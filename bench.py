@@ -5,7 +5,10 @@ COUNT of the float64 column, MIN/MAX and NUNIQUE of the int32 column.
 
 One step = one groupby_aggregation call through the public API (C ABI) on
 device-resident inputs (4.2 GB, far larger than the 126 MB L2, so no flush is
-needed).  Prints ONE JSON line (rank 0).
+needed).  Prints ONE JSON line (rank 0).  At N=1 the line also carries
+`served`: the batched/served mix (8,192 small joins and groupbys arriving at
+2,000 req/s) through the continuous-batching server and, for comparison, the
+same requests issued one op per launch (--no-served skips it).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -241,6 +244,52 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# served mix: many small joins/groupbys, batched vs one op per launch
+# ---------------------------------------------------------------------------
+SERVED_CANDIDATES = [(16384, 4, 0.5), (16384, 8, 0.5), (16384, 16, 0.5), (65536, 8, 0.5), (16384, 8, 0.35)]
+
+
+def run_served(device, n_requests: int):
+    """8,192 requests, Poisson arrivals at 2,000 req/s, each an int64-key inner
+    join or groupby SUM/COUNT over LogNormal(median 50K, sigma 1) rows clipped
+    to 1K-20M, keys uniform over 0.1 x rows; tables resident on the device.
+    Reports the continuous-batching server (autotuned) and the same requests
+    issued one op per launch, each at the arrival rate (latency) and with all
+    requests queued at t=0 (throughput)."""
+    from legate_dataframe import _native as N
+    from legate_dataframe import serving as S
+
+    reqs = S.make_trace(n_requests=n_requests, seed=12, device=device)
+    calib = S.make_trace(n_requests=512, seed=13, device=device)
+    best = S.Autotuner().tune(calib, f"served-mix-{n_requests}", arena_bytes=16 << 30, candidates=SERVED_CANDIDATES)
+    srv = S.Server(arena_bytes=16 << 30, tile_rows=best["tile_rows"], ctas_per_sm=best["ctas_per_sm"],
+                   load_factor=best["load_factor"])
+    srv.serve(calib, realtime=False)  # warm-up
+    l0 = N.launch_count()
+    rt = srv.serve(reqs, realtime=True).summary()
+    rt["gpu_launches"] = N.launch_count() - l0
+    sat = srv.serve(reqs, realtime=False).summary()
+    srv.close()
+    S.run_one_op_per_launch(calib[:32], realtime=False)  # warm-up
+    l0 = N.launch_count()
+    base_rt = S.run_one_op_per_launch(reqs, realtime=True).summary()
+    base_rt["gpu_launches"] = N.launch_count() - l0
+    base_sat = S.run_one_op_per_launch(reqs, realtime=False).summary()
+    rows = sum(q.rows for q in reqs)
+    return {
+        "workload": f"{n_requests} requests, Poisson 2000 req/s, 50% int64-key inner join / 50% int64-key groupby "
+                    "SUM+COUNT(f64, 10% nulls), rows LogNormal(median 50K, sigma 1) clipped 1K-20M, keys U[0, "
+                    "0.1 x rows); device-resident tables; latency = arrival -> result on the host",
+        "rows": rows,
+        "autotune": best,
+        "batched": rt,
+        "batched_saturated": sat,
+        "one_op_per_launch": base_rt,
+        "one_op_per_launch_saturated": base_sat,
+        "saturated_throughput_ratio": sat["req_per_s"] / base_sat["req_per_s"],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -251,6 +300,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=4_000_000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=8192)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -398,6 +449,13 @@ def main():
                          f"{pa.__version__} Acero aggregate hash_sum/mean/count_all/count/min/max/count_distinct, "
                          "use_threads=False: the Arrow calls of the reference's cpu_variant (one legate CPU task)"}
 
+    # ---- served mix (rank 0, N=1 only) --------------------------------------
+    served = None
+    if rank == 0 and world == 1 and not args.no_served:
+        del keys, v, valid, i, table
+        torch.cuda.empty_cache()
+        served = run_served(device, args.served_requests)
+
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -428,6 +486,7 @@ def main():
         "clocks": clk.summary(),
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "served": served,
     }
     print(json.dumps(line))
     return 0

@@ -184,6 +184,57 @@ int ldf_b200_hash_partition_noalloc(const ldf_column* table, int32_t ncols,
                                     const int32_t* keys, int32_t nkeys, int32_t nparts,
                                     ldf_column* out, int64_t* offsets, void* stream);
 
+/* ---- batched execution of many small joins / groupbys ------------------- */
+/* No counterpart in the reference (its ops run one task launch per op).  A
+ * batch of requests whose inputs are already on the device runs as ONE replay
+ * of a CUDA graph captured at engine creation: descriptor upload from mapped
+ * pinned memory, three persistent kernels (table init, build/aggregate,
+ * probe/emit) over a work list of row tiles of all requests, and the download
+ * of per-request output row counts and overflow flags.
+ *
+ * kind LDF_BATCH_GROUPBY: int64 keys k1[n], value v1[n] (vtype int64 or
+ *   float64, optional 1-byte validity vvalid).  Output o0 = key (int64), o1 =
+ *   SUM of the valid values (int64 wrapping, or float64 correctly rounded from
+ *   an exact fixed-point sum), o2 = COUNT of the valid values (int64).  A group
+ *   whose values are all null has o2 = 0 (its SUM is null).  The hash table
+ *   takes (cap + 1) x 3 words (int64) or (cap + 1) x 8 words (float64).
+ * kind LDF_BATCH_INNER_JOIN: probe k1[n]/v1[n] (int64 key/payload), build
+ *   k2[m]/v2[m]; output rows (o0 = lhs key, o1 = lhs payload, o2 = rhs key,
+ *   o3 = rhs payload).  The multimap takes cap x 2 words, cap > m.
+ * Output row order is unspecified; every output column holds out_cap rows.
+ * A request whose table or output overflows its reservation, or whose float
+ * values fall outside the exact fixed-point range (|x| < 2^95 and x = 0 or
+ * |x| >= 2^-44), is flagged in `overflow` and must be re-run on the per-op
+ * path.  Requests of one batch must not share table or output memory. */
+enum { LDF_BATCH_GROUPBY = 0, LDF_BATCH_INNER_JOIN = 1 };
+enum { LDF_BATCH_INT64 = 0, LDF_BATCH_FLOAT64 = 1 };
+
+typedef struct {
+  int32_t kind;            /* LDF_BATCH_* */
+  int32_t vtype;           /* groupby value type: LDF_BATCH_INT64 / LDF_BATCH_FLOAT64 */
+  int64_t n, m;            /* rows of k1/v1 and of k2/v2 */
+  const int64_t* k1;
+  const void* v1;
+  const int64_t* k2;
+  const int64_t* v2;
+  const uint8_t* vvalid;   /* groupby value validity (1 byte per row) or NULL */
+  uint64_t* table;         /* device scratch of the hash table */
+  uint64_t cap;            /* hash table slots (>= 2) */
+  void* o0; void* o1; void* o2; void* o3;
+  int64_t out_cap;         /* rows reserved in each output column */
+} ldf_batch_request;
+
+/* Create an engine for batches of up to max_reqs requests and max_items row
+ * tiles of tile_rows rows per kernel; the kernels run ctas_per_sm CTAs per SM
+ * on `stream`. */
+int ldf_b200_batch_create(int32_t max_reqs, int32_t max_items, int64_t tile_rows,
+                          int32_t ctas_per_sm, void* stream, void** engine);
+/* Enqueue one batch (asynchronous; the request array is copied). */
+int ldf_b200_batch_run(void* engine, const ldf_batch_request* reqs, int32_t nreq);
+/* Wait for the last batch; out_rows / overflow receive max_reqs entries. */
+int ldf_b200_batch_wait(void* engine, uint64_t* out_rows, int32_t* overflow);
+int ldf_b200_batch_destroy(void* engine);
+
 /* ---- utilities ---------------------------------------------------------- */
 /* Message of the last failed call on this thread ("" if none). */
 const char* ldf_b200_last_error(void);

@@ -30,6 +30,7 @@ SOURCES = [
     "sort.cu",
     "abi.cu",
     "noalloc.cu",
+    "batch.cu",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

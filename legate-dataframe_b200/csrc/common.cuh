@@ -54,6 +54,7 @@ int num_sms();
 namespace prof {
 void begin(const char* name, cudaStream_t s);
 void end(const char* name, cudaStream_t s);
+void count_launches(unsigned long long n);  // kernels launched by a graph replay
 }  // namespace prof
 
 template <typename... KArgs, typename... Args>

@@ -36,6 +36,8 @@ void begin(const char*, cudaStream_t s)
   LDF_CUDA(cudaEventRecord(t_begin, s));
 }
 
+void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
 void end(const char* name, cudaStream_t s)
 {
   if (!g_enabled.load(std::memory_order_relaxed) || t_begin == nullptr) return;
