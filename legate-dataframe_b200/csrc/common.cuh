@@ -200,31 +200,16 @@ __device__ __forceinline__ bool dvalid(const DCol& c, int64_t r)
   return c.valid == nullptr || __ldg(c.valid + r) != 0;
 }
 
-// Raw bits of a fixed-width value, zero-extended; floats are normalised so
-// that -0.0 == 0.0 and every NaN is one value (equality/hash semantics).
+// Raw bits of a fixed-width value, zero-extended.  Hashing and equality of
+// keys and distinct values use these bits, as Arrow's hash kernels do: 0.0 and
+// -0.0 are different keys and a NaN equals only a NaN with the same bits.
 __device__ __forceinline__ uint64_t dbits(const DCol& c, int64_t r)
 {
   switch (c.width) {
     case 1: return __ldg(static_cast<const uint8_t*>(c.data) + r);
     case 2: return __ldg(static_cast<const uint16_t*>(c.data) + r);
-    case 4: {
-      uint32_t v = __ldg(static_cast<const uint32_t*>(c.data) + r);
-      if (c.type == LDF_FLOAT32) {
-        if ((v & 0x7fffffffu) == 0) v = 0;
-        else if ((v & 0x7f800000u) == 0x7f800000u && (v & 0x007fffffu)) v = 0x7fc00000u;
-      }
-      return v;
-    }
-    default: {
-      uint64_t v = __ldg(reinterpret_cast<const unsigned long long*>(c.data) + r);
-      if (c.type == LDF_FLOAT64) {
-        if ((v & 0x7fffffffffffffffull) == 0) v = 0;
-        else if ((v & 0x7ff0000000000000ull) == 0x7ff0000000000000ull &&
-                 (v & 0x000fffffffffffffull))
-          v = 0x7ff8000000000000ull;
-      }
-      return v;
-    }
+    case 4: return __ldg(static_cast<const uint32_t*>(c.data) + r);
+    default: return __ldg(reinterpret_cast<const unsigned long long*>(c.data) + r);
   }
 }
 

@@ -748,9 +748,13 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
 }
 
 // ---- NUNIQUE: dedupe the (group id, value) pairs -----------------------------
-// Pairs (gid[r] << 32 | value32) of valid rows go into a pair set; first
-// insertions count per group (hot groups in shared memory first).  Eight rows
-// per thread with their first probes in flight together.
+// The `hb` most frequent ranks keep one bit per value of the column's value
+// range ([vbase, vbase + 32 * wpr) after the order-preserving flip): a row sets
+// its bit with a fire-and-forget OR (the bitmaps stay L2-resident) and a
+// popcount pass counts them.  Pairs (rank << 32 | value32) of the other ranks
+// go into a pair set; first insertions count per rank (ranks below `hot` in
+// shared memory first).  Eight rows per thread with their first probes in
+// flight together.
 constexpr int kPairsPerThread = 8;
 struct NdArgs {
   const uint32_t* gid;
@@ -762,7 +766,17 @@ struct NdArgs {
   unsigned long long* nd;  // distinct-count field (indexed by frequency rank)
   int hot;
   int* overflow;
+  uint32_t* bits;  // hb x wpr bitmap words
+  uint32_t hb;
+  uint32_t wpr;
+  uint32_t vbase;
+  uint32_t flip;  // 0x80000000 for signed 32-bit values, else 0
 };
+
+__device__ __forceinline__ void red_or32(uint32_t* p, uint32_t v)
+{
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
 {
@@ -779,8 +793,16 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
       e[j]            = kEmpty;
       if (r < a.n && dvalid(a.col, r)) {
         const uint32_t g = __ldg(a.gid + r);
-        if (g != kUnsetId)
-          e[j] = (static_cast<uint64_t>(__ldg(a.newid + g)) << 32) | static_cast<uint32_t>(dbits(a.col, r));
+        if (g != kUnsetId) {
+          const uint32_t rank = __ldg(a.newid + g);
+          const uint32_t x    = static_cast<uint32_t>(dbits(a.col, r));
+          if (rank < a.hb) {
+            const uint32_t off = (x ^ a.flip) - a.vbase;
+            red_or32(a.bits + static_cast<uint64_t>(rank) * a.wpr + (off >> 5), 1u << (off & 31));
+          } else {
+            e[j] = (static_cast<uint64_t>(rank) << 32) | x;
+          }
+        }
       }
       idx[j] = e[j] != kEmpty ? fastrange(mix64(e[j]), a.cap) : 0;
     }
@@ -815,6 +837,62 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
   __syncthreads();
   for (int g = threadIdx.x; g < a.hot; g += blockDim.x)
     if (cnt[g]) red_add(a.nd + g, cnt[g]);
+}
+
+// Range of the (flipped) 32-bit values of the valid rows: out[0] = min, out[1] = max.
+// Eight strided rows per thread and step keep eight loads in flight.
+__global__ void value_range_kernel(DCol col, int64_t n, uint32_t flip, unsigned int* out)
+{
+  constexpr int kU = 8;
+  uint32_t lo = 0xffffffffu, hi = 0;
+  const int64_t nth = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; base < n; base += kU * nth) {
+    uint32_t x[kU];
+    bool ok[kU];
+#pragma unroll
+    for (int j = 0; j < kU; ++j) {
+      const int64_t r = base + j * nth;
+      ok[j]           = r < n && dvalid(col, r);
+      x[j]            = ok[j] ? static_cast<uint32_t>(dbits(col, r)) ^ flip : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < kU; ++j)
+      if (ok[j]) {
+        lo = min(lo, x[j]);
+        hi = max(hi, x[j]);
+      }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(out, lo);
+    atomicMax(out + 1, hi);
+  }
+}
+
+// Distinct counts of the bitmap ranks: one CTA per rank (grid-stride).
+__global__ void bitmap_count_kernel(const uint32_t* bits, uint32_t hb, uint32_t wpr, unsigned long long* nd)
+{
+  __shared__ unsigned long long part[32];
+  for (uint32_t g = blockIdx.x; g < hb; g += gridDim.x) {
+    const uint4* w4 = reinterpret_cast<const uint4*>(bits + static_cast<uint64_t>(g) * wpr);
+    unsigned long long c = 0;
+    for (uint32_t i = threadIdx.x; i < wpr / 4; i += blockDim.x) {
+      const uint4 q = w4[i];
+      c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long t = 0;
+      for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) t += part[i];
+      if (t) red_add(nd + g, t);
+    }
+    __syncthreads();
+  }
 }
 
 // NUNIQUE of 8-byte or string values: pairs hashed on (group, value) with the
@@ -1310,6 +1388,9 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
   LDF_CUDA(cudaFuncSetAttribute(assign_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
   int hot_limit = 1 << 30;
   if (const char* e = std::getenv("LDF_B200_GB_HOT")) hot_limit = std::max(0, std::atoi(e));
+  // bytes of NUNIQUE value bitmaps (kept well inside the 126 MB L2)
+  uint64_t bitmap_budget = 48ull << 20;
+  if (const char* e = std::getenv("LDF_B200_ND_BITMAP_MB")) bitmap_budget = std::max(0ll, std::atoll(e)) << 20;
 
   for (int attempt = 0;; ++attempt) {
     const uint64_t id_cap = cap + kIdFirst;
@@ -1462,12 +1543,39 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
         if (c.pair_packed) {
           NdArgs na{gid.get(), newid.get(), c.col, n, c.pairs, c.pair_cap, rec.get() + c.off_nd * L,
                     static_cast<int>(std::min<int64_t>(std::min(hot_cap, 12 * 1024), nid)), p.overflow};
+          // value bitmaps for the most frequent ranks when the value range is small
+          na.flip = (c.col.width == 4 && is_signed_int(c.col.type)) ? 0x80000000u : 0u;
+          Buffer<unsigned int> vr(al, 2);
+          const unsigned int vr_init[2] = {0xffffffffu, 0u};
+          LDF_CUDA(cudaMemcpyAsync(vr.get(), vr_init, 8, cudaMemcpyHostToDevice, s));
+          launch("value_range", value_range_kernel, static_cast<unsigned>(4 * num_sms()), 256, 0, s, c.col, n,
+                 na.flip, vr.get());
+          unsigned int hv[2];
+          LDF_CUDA(cudaMemcpyAsync(hv, vr.get(), 8, cudaMemcpyDeviceToHost, s));
+          ctx.finish();
+          Buffer<uint32_t> bits;
+          if (hv[0] <= hv[1] && bitmap_budget > 0) {
+            const uint64_t range = static_cast<uint64_t>(hv[1]) - hv[0] + 1;
+            const uint64_t wpr   = (((range + 31) / 32) + 3) / 4 * 4;  // 16-byte rows
+            const uint64_t hb    = std::min<uint64_t>(static_cast<uint64_t>(nid), bitmap_budget / (4 * wpr));
+            if (hb >= 8) {
+              bits = Buffer<uint32_t>(al, hb * wpr);
+              LDF_CUDA(cudaMemsetAsync(bits.get(), 0, hb * wpr * 4, s));
+              na.bits  = bits.get();
+              na.hb    = static_cast<uint32_t>(hb);
+              na.wpr   = static_cast<uint32_t>(wpr);
+              na.vbase = hv[0];
+            }
+          }
           const size_t nd_smem = static_cast<size_t>(na.hot) * 4;
           int nocc             = 1;
           LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nocc, nunique_kernel, kGbThreads, nd_smem));
           const int64_t nblocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(nocc, 1),
                                                     ceil_div(n, int64_t(kGbThreads) * kPairsPerThread));
           launch("nunique", nunique_kernel, static_cast<unsigned>(nblocks), kGbThreads, nd_smem, s, na);
+          if (na.hb > 0)
+            launch("bitmap_count", bitmap_count_kernel, std::min<unsigned>(na.hb, 4u * num_sms()), 256u, 0, s,
+                   static_cast<const uint32_t*>(na.bits), na.hb, na.wpr, na.nd);
         } else {
           launch("nunique_generic", nunique_generic_kernel<M>, gs_blocks(n, 256), 256, 0, s, p, c,
                  static_cast<const uint32_t*>(gid.get()), static_cast<const uint32_t*>(newid.get()),

@@ -34,6 +34,18 @@ def _values_and_valid(arr: pa.Array):
     return vals, valid
 
 
+def _equality_values(arr: pa.Array):
+    """Values under the equality of Arrow's hash kernels (grouper, hash join,
+    hash_count_distinct): floats compare by their bit pattern, so 0.0 and -0.0
+    are different keys and a NaN equals only a NaN with the same bits."""
+    arr = arr.combine_chunks() if isinstance(arr, pa.ChunkedArray) else arr
+    if pa.types.is_floating(arr.type):
+        valid = np.asarray(arr.is_valid(), dtype=bool)
+        v = np.asarray(arr.fill_null(0).to_numpy(zero_copy_only=False))
+        return v.view({2: np.uint16, 4: np.uint32, 8: np.uint64}[v.dtype.itemsize]).astype(np.uint64), valid
+    return _values_and_valid(arr)
+
+
 def _codes(vals: np.ndarray) -> np.ndarray:
     """Dense codes of equal values (NaN == NaN)."""
     if len(vals) == 0:
@@ -70,8 +82,8 @@ def join_indices(lhs: pa.Table, rhs: pa.Table, lhs_keys, rhs_keys, join_type: st
     lbad = np.zeros(nl, dtype=bool)
     rbad = np.zeros(nr, dtype=bool)
     for lk, rk in zip(lhs_keys, rhs_keys):
-        lv, lvalid = _values_and_valid(lhs.column(lk))
-        rv, rvalid = _values_and_valid(rhs.column(rk))
+        lv, lvalid = _equality_values(lhs.column(lk))
+        rv, rvalid = _equality_values(rhs.column(rk))
         both = np.concatenate([lv, rv]) if len(lv) + len(rv) else lv
         codes = _codes(both)
         null_code = (codes.max() + 1) if len(codes) else 0
@@ -156,7 +168,7 @@ def neumaier(xs) -> float:
 def group_ids(table: pa.Table, keys):
     code_cols = []
     for k in keys:
-        v, valid = _values_and_valid(table.column(k))
+        v, valid = _equality_values(table.column(k))
         c = _codes(v)
         null_code = (c.max() + 1) if len(c) else 0
         code_cols.append(np.where(valid, c, null_code))
@@ -205,7 +217,7 @@ def groupby(table: pa.Table, keys, aggs) -> pa.Table:
             continue
         if kind == "count_distinct":
             mode = _count_mode(options)
-            codes = _codes(vals)
+            codes = _codes(_equality_values(arr)[0])
             pairs = np.unique(np.stack([gid[valid], codes[valid]], axis=1), axis=0) if valid.any() else np.zeros((0, 2), np.int64)
             nd = np.bincount(pairs[:, 0], minlength=G).astype(np.int64) if len(pairs) else np.zeros(G, np.int64)
             has_null = (nall > nvalid).astype(np.int64)
@@ -364,16 +376,6 @@ def _raw_bits(arr: pa.Array) -> tuple[np.ndarray, int]:
         storage = arr.view(pa.int64() if width == 8 else pa.int32())
     v = np.asarray(storage.fill_null(0).to_numpy(zero_copy_only=False))
     u = v.view({1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[width]).astype(np.uint64)
-    if pa.types.is_floating(t):
-        if width == 4:
-            u = np.where((u & np.uint64(0x7FFFFFFF)) == 0, np.uint64(0), u)
-            nan = ((u & np.uint64(0x7F800000)) == np.uint64(0x7F800000)) & ((u & np.uint64(0x007FFFFF)) != 0)
-            u = np.where(nan, np.uint64(0x7FC00000), u)
-        else:
-            u = np.where((u & np.uint64(0x7FFFFFFFFFFFFFFF)) == 0, np.uint64(0), u)
-            nan = ((u & np.uint64(0x7FF0000000000000)) == np.uint64(0x7FF0000000000000)) & (
-                (u & np.uint64(0x000FFFFFFFFFFFFF)) != 0)
-            u = np.where(nan, np.uint64(0x7FF8000000000000), u)
     return u, width
 
 

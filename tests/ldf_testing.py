@@ -86,3 +86,18 @@ def assert_tables_equal(res: pa.Table, exp: pa.Table, sort_by="all", rtol: float
             assert ok.all(), f"{name}: max rel err {np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300))}"
         else:
             assert a.filter(pa.array(va)).equals(b.filter(pa.array(vb))), f"column {name} differs"
+
+
+# Floats as keys or distinct values compare by bit pattern in Arrow's hash
+# kernels: 0.0 != -0.0, and a NaN equals only a NaN with the same bits.
+SPECIAL = np.array([0.0, -0.0, np.nan, -np.nan, 1.0, 0.0, -0.0, np.nan, 1.0, -np.nan], np.float64)
+
+
+def special_float_tables(dtype=np.float64):
+    """(groupby table, join lhs, join rhs) with 0.0/-0.0/NaN/-NaN keys."""
+    x = SPECIAL.astype(dtype)
+    t = pa.table({"k": x, "v": np.left_shift(1, np.arange(len(x), dtype=np.int64)), "w": x[::-1].copy()})
+    lhs = pa.table({"k": x, "a": np.arange(len(x), dtype=np.int64)})
+    rhs = pa.table({"k2": np.array([-0.0, np.nan, 2.0, 0.0, -np.nan, -0.0], dtype),
+                    "b": np.arange(6, dtype=np.int64) + 100})
+    return t, lhs, rhs

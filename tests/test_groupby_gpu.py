@@ -150,3 +150,52 @@ def test_groupby_sentinel_key_value():
     res = run_groupby(t, ["k"], [("v", "sum", "s")])
     exp = R.groupby(t, ["k"], [("v", "sum", "s")])
     assert_tables_equal(res, exp, sort_by=["k"])
+
+
+@pytest.mark.parametrize("vkind", ["int32_neg", "int32_wide", "int8", "int16", "uint32", "uint8", "float32", "bool"])
+@pytest.mark.parametrize("budget_mb", [None, "0", "1"])
+def test_groupby_nunique_value_kinds(vkind, budget_mb, monkeypatch):
+    # NUNIQUE through the value bitmaps of frequent ranks (small value ranges,
+    # any budget) and through the pair set (wide ranges, budget 0)
+    if budget_mb is not None:
+        monkeypatch.setenv("LDF_B200_ND_BITMAP_MB", budget_mb)
+    rng = np.random.default_rng(31)
+    n = 300_000
+    ranks = np.minimum(rng.zipf(1.2, n), 5000) - 1
+    k = rng.permutation(5000)[ranks].astype(np.int64)
+    if vkind == "int32_neg":
+        v = pa.array(rng.integers(-3000, 2000, n).astype(np.int32), mask=rng.random(n) < 0.1)
+    elif vkind == "int32_wide":
+        v = pa.array(rng.integers(-2**31, 2**31 - 1, n).astype(np.int32))
+    elif vkind == "int8":
+        v = pa.array(rng.integers(-128, 128, n).astype(np.int8), mask=rng.random(n) < 0.05)
+    elif vkind == "int16":
+        v = pa.array(rng.integers(-30000, 30000, n).astype(np.int16))
+    elif vkind == "uint32":
+        v = pa.array(rng.integers(4_000_000_000, 4_000_100_000, n).astype(np.uint32))
+    elif vkind == "uint8":
+        v = pa.array(rng.integers(0, 256, n).astype(np.uint8))
+    elif vkind == "float32":
+        x = rng.integers(-500, 500, n).astype(np.float32) / 4
+        x[::97] = -0.0
+        x[::89] = np.nan
+        v = pa.array(x)
+    else:
+        v = pa.array(rng.random(n) < 0.3, mask=rng.random(n) < 0.1)
+    t = pa.table({"k": k, "v": v})
+    aggs = [("v", "count_distinct", "nd"), ("v", ("count_distinct", pc.CountOptions(mode="all")), "nda")]
+    res = run_groupby(t, ["k"], aggs)
+    exp = R.groupby(t, ["k"], aggs)
+    assert_tables_equal(res, exp, sort_by=["k"])
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_groupby_special_float_keys_by_bits(dtype):
+    from ldf_testing import special_float_tables
+
+    t, _, _ = special_float_tables(dtype)
+    aggs = [("v", "sum", "s"), ("w", "count_distinct", "nd"), (None, "count_all", "n")]
+    res = run_groupby(t, ["k"], aggs)
+    exp = R.groupby(t, ["k"], aggs)
+    assert res.num_rows == 5
+    assert_tables_equal(res, exp, sort_by=["s"])

@@ -122,3 +122,14 @@ def test_join_all_null_keys():
             res = run_join(lhs, rhs, ["k"], ["kr"], how, ne)
             exp = R.join(lhs, rhs, ["k"], ["kr"], how, ne)
             assert_tables_equal(res, exp)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("how", ["inner", "left", "full", "semi", "anti"])
+def test_join_special_float_keys_by_bits(how, dtype):
+    from ldf_testing import special_float_tables
+
+    _, lhs, rhs = special_float_tables(dtype)
+    res = run_join(lhs, rhs, ["k"], ["k2"], how)
+    exp = R.join(lhs, rhs, ["k"], ["k2"], how, True)
+    assert_tables_equal(res, exp, sort_by=[c for c in exp.column_names if c in ("a", "b")], check_types=False)

@@ -7,7 +7,7 @@ import pyarrow as pa
 import pyarrow.compute as pc
 import pytest
 
-from ldf_testing import agg_spec, assert_tables_equal, load_golden
+from ldf_testing import agg_spec, assert_tables_equal, load_golden, special_float_tables
 from oracle import arrow_ref as A
 from oracle import relational as R
 
@@ -128,3 +128,17 @@ def test_oracle_hash_known_answers():
     xs = np.array([0, 1, 2, 12345, (1 << 64) - 1], dtype=np.uint64)
     got = R._mix64(xs)
     assert [int(g) for g in got] == [fmix(int(x)) for x in xs]
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_special_float_keys_vs_arrow(dtype):
+    t, lhs, rhs = special_float_tables(dtype)
+    aggs = [("v", "sum", "s"), ("w", "count_distinct", "nd")]
+    a = R.groupby(t, ["k"], aggs)
+    b = A.groupby(t, ["k"], aggs)
+    assert a.num_rows == b.num_rows == 5  # 0.0, -0.0, NaN, -NaN, 1.0
+    assert_tables_equal(a, b, sort_by=["s"])
+    for how in ("inner", "left", "full", "semi", "anti"):
+        exp = A.join(lhs, rhs, ["k"], ["k2"], how, True)
+        res = R.join(lhs, rhs, ["k"], ["k2"], how, True)
+        assert_tables_equal(res, exp, sort_by=[c for c in exp.column_names if c in ("a", "b")], check_types=False)
