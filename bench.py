@@ -177,6 +177,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """Max of a per-rank time over all ranks (the slowest replica times the job)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------------------
 # CPU baselines: the reference's CPU path (Arrow Acero aggregate, the calls of
 # GroupByAggregationTask::cpu_variant) on a bounded sample
@@ -204,7 +216,7 @@ def run_reference(args):
     import numpy as np
     import pyarrow as pa
 
-    n = 8_000_000
+    n = args.ref_rows
     rng = np.random.default_rng(3)
     ranks = np.arange(1, N_KEYS + 1, dtype=np.float64)
     cdf = np.cumsum(ranks ** -1.1)
@@ -302,6 +314,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-requests", type=int, default=8192)
+    ap.add_argument("--ref-rows", type=int, default=8_000_000, help="rows per step of the reference arm")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -354,12 +367,8 @@ def main():
         ev1.record()
         torch.cuda.synchronize()
     barrier()
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world, device)
     launches = (N.launch_count() - launches0) // args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     ms_step = ms / args.steps
     value = world * n / (ms_step / 1e3)
 
@@ -428,11 +437,7 @@ def main():
             del res, host
         e1.record()
         torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
-        if world > 1:
-            t = torch.tensor([e2e_ms], device=device)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.e2e_steps, world, device)
         e2e = {"value": world * n / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": n * IN_BYTES_PER_ROW, "d2h_bytes_per_step": d2h}
         del hk, hv, hm, hi, dk, dv, dm, di
