@@ -778,6 +778,17 @@ __device__ __forceinline__ void red_or32(uint32_t* p, uint32_t v)
   asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Raw bits of a W-byte value (W known at compile time, so the loads of an
+// unrolled loop issue together).
+template <int W>
+__device__ __forceinline__ uint32_t load_bits(const void* data, int64_t r)
+{
+  if (W == 1) return __ldg(static_cast<const uint8_t*>(data) + r);
+  if (W == 2) return __ldg(static_cast<const uint16_t*>(data) + r);
+  return __ldg(static_cast<const uint32_t*>(data) + r);
+}
+
+template <int W>
 __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
 {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -787,21 +798,31 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
   const int64_t per_block = static_cast<int64_t>(blockDim.x) * kPairsPerThread;
   for (int64_t base = blockIdx.x * per_block; base < a.n; base += static_cast<int64_t>(gridDim.x) * per_block) {
     uint64_t e[kPairsPerThread], idx[kPairsPerThread], v[kPairsPerThread];
+    uint32_t g[kPairsPerThread], x[kPairsPerThread];
+    // independent loads first: group id, value, validity of every row
 #pragma unroll
     for (int j = 0; j < kPairsPerThread; ++j) {
       const int64_t r = base + j * blockDim.x + threadIdx.x;
-      e[j]            = kEmpty;
-      if (r < a.n && dvalid(a.col, r)) {
-        const uint32_t g = __ldg(a.gid + r);
-        if (g != kUnsetId) {
-          const uint32_t rank = __ldg(a.newid + g);
-          const uint32_t x    = static_cast<uint32_t>(dbits(a.col, r));
-          if (rank < a.hb) {
-            const uint32_t off = (x ^ a.flip) - a.vbase;
-            red_or32(a.bits + static_cast<uint64_t>(rank) * a.wpr + (off >> 5), 1u << (off & 31));
-          } else {
-            e[j] = (static_cast<uint64_t>(rank) << 32) | x;
-          }
+      g[j]            = kUnsetId;
+      x[j]            = 0;
+      if (r < a.n) {
+        g[j] = __ldg(a.gid + r);
+        x[j] = load_bits<W>(a.col.data, r);
+        if (a.col.valid != nullptr && __ldg(a.col.valid + r) == 0) g[j] = kUnsetId;
+      }
+    }
+    // then the rank of each group (eight dependent loads in flight)
+#pragma unroll
+    for (int j = 0; j < kPairsPerThread; ++j) g[j] = g[j] != kUnsetId ? __ldg(a.newid + g[j]) : kUnsetId;
+#pragma unroll
+    for (int j = 0; j < kPairsPerThread; ++j) {
+      e[j] = kEmpty;
+      if (g[j] != kUnsetId) {
+        if (g[j] < a.hb) {
+          const uint32_t off = (x[j] ^ a.flip) - a.vbase;
+          red_or32(a.bits + static_cast<uint64_t>(g[j]) * a.wpr + (off >> 5), 1u << (off & 31));
+        } else {
+          e[j] = (static_cast<uint64_t>(g[j]) << 32) | x[j];
         }
       }
       idx[j] = e[j] != kEmpty ? fastrange(mix64(e[j]), a.cap) : 0;
@@ -812,35 +833,37 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
     for (int j = 0; j < kPairsPerThread; ++j) {
       if (e[j] == kEmpty) continue;
       bool fresh = false;
-      uint64_t x = idx[j], cur = v[j];
-      int probe  = 0;
+      uint64_t xs = idx[j], cur = v[j];
+      int probe   = 0;
       for (; probe < kMaxProbe; ++probe) {
         if (cur == e[j]) break;
         if (cur == kEmpty) {
-          cur = atomicCAS(a.set + x, kEmpty, e[j]);
+          cur = atomicCAS(a.set + xs, kEmpty, e[j]);
           if (cur == kEmpty) {
             fresh = true;
             break;
           }
           if (cur == e[j]) break;
         }
-        x   = x + 1 == a.cap ? 0 : x + 1;
-        cur = a.set[x];
+        xs  = xs + 1 == a.cap ? 0 : xs + 1;
+        cur = a.set[xs];
       }
       if (probe == kMaxProbe) atomicExch(a.overflow, 1);
       if (!fresh) continue;
-      const uint32_t g = static_cast<uint32_t>(e[j] >> 32);
-      if (g < static_cast<uint32_t>(a.hot)) atomicAdd(cnt + g, 1u);
-      else red_add(a.nd + g, 1);
+      const uint32_t rk = static_cast<uint32_t>(e[j] >> 32);
+      if (rk < static_cast<uint32_t>(a.hot)) atomicAdd(cnt + rk, 1u);
+      else red_add(a.nd + rk, 1);
     }
   }
   __syncthreads();
-  for (int g = threadIdx.x; g < a.hot; g += blockDim.x)
-    if (cnt[g]) red_add(a.nd + g, cnt[g]);
+  for (int gg = threadIdx.x; gg < a.hot; gg += blockDim.x)
+    if (cnt[gg]) red_add(a.nd + gg, cnt[gg]);
 }
 
-// Range of the (flipped) 32-bit values of the valid rows: out[0] = min, out[1] = max.
-// Eight strided rows per thread and step keep eight loads in flight.
+// Range of the (flipped) W-byte values of the valid rows: out[0] = min,
+// out[1] = max.  Eight strided rows per thread and step keep eight loads in
+// flight.
+template <int W>
 __global__ void value_range_kernel(DCol col, int64_t n, uint32_t flip, unsigned int* out)
 {
   constexpr int kU = 8;
@@ -852,8 +875,9 @@ __global__ void value_range_kernel(DCol col, int64_t n, uint32_t flip, unsigned 
 #pragma unroll
     for (int j = 0; j < kU; ++j) {
       const int64_t r = base + j * nth;
-      ok[j]           = r < n && dvalid(col, r);
-      x[j]            = ok[j] ? static_cast<uint32_t>(dbits(col, r)) ^ flip : 0u;
+      ok[j]           = r < n;
+      x[j]            = ok[j] ? load_bits<W>(col.data, r) ^ flip : 0u;
+      if (ok[j] && col.valid != nullptr) ok[j] = __ldg(col.valid + r) != 0;
     }
 #pragma unroll
     for (int j = 0; j < kU; ++j)
@@ -1548,8 +1572,11 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
           Buffer<unsigned int> vr(al, 2);
           const unsigned int vr_init[2] = {0xffffffffu, 0u};
           LDF_CUDA(cudaMemcpyAsync(vr.get(), vr_init, 8, cudaMemcpyHostToDevice, s));
-          launch("value_range", value_range_kernel, static_cast<unsigned>(4 * num_sms()), 256, 0, s, c.col, n,
-                 na.flip, vr.get());
+          {
+            auto vk = c.col.width == 1 ? value_range_kernel<1> : c.col.width == 2 ? value_range_kernel<2>
+                                                                                   : value_range_kernel<4>;
+            launch("value_range", vk, static_cast<unsigned>(4 * num_sms()), 256, 0, s, c.col, n, na.flip, vr.get());
+          }
           unsigned int hv[2];
           LDF_CUDA(cudaMemcpyAsync(hv, vr.get(), 8, cudaMemcpyDeviceToHost, s));
           ctx.finish();
@@ -1569,10 +1596,11 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
           }
           const size_t nd_smem = static_cast<size_t>(na.hot) * 4;
           int nocc             = 1;
-          LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nocc, nunique_kernel, kGbThreads, nd_smem));
+          auto ndk = c.col.width == 1 ? nunique_kernel<1> : c.col.width == 2 ? nunique_kernel<2> : nunique_kernel<4>;
+          LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nocc, ndk, kGbThreads, nd_smem));
           const int64_t nblocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(nocc, 1),
                                                     ceil_div(n, int64_t(kGbThreads) * kPairsPerThread));
-          launch("nunique", nunique_kernel, static_cast<unsigned>(nblocks), kGbThreads, nd_smem, s, na);
+          launch("nunique", ndk, static_cast<unsigned>(nblocks), kGbThreads, nd_smem, s, na);
           if (na.hb > 0)
             launch("bitmap_count", bitmap_count_kernel, std::min<unsigned>(na.hb, 4u * num_sms()), 256u, 0, s,
                    static_cast<const uint32_t*>(na.bits), na.hb, na.wpr, na.nd);
