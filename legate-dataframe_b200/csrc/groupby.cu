@@ -771,6 +771,10 @@ struct NdArgs {
   uint32_t wpr;
   uint32_t vbase;
   uint32_t flip;  // 0x80000000 for signed 32-bit values, else 0
+  // ranks >= s0 scatter their values into per-rank segments
+  uint32_t s0;
+  unsigned long long* seg_cursor;  // [rank - s0]: next free position of the segment
+  uint32_t* seg_vals;
 };
 
 __device__ __forceinline__ void red_or32(uint32_t* p, uint32_t v)
@@ -789,7 +793,7 @@ __device__ __forceinline__ uint32_t load_bits(const void* data, int64_t r)
 }
 
 template <int W>
-__global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
+__global__ void __launch_bounds__(kGbThreads, 2) nunique_kernel(NdArgs a)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* cnt = reinterpret_cast<uint32_t*>(smem);
@@ -797,7 +801,7 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
   __syncthreads();
   const int64_t per_block = static_cast<int64_t>(blockDim.x) * kPairsPerThread;
   for (int64_t base = blockIdx.x * per_block; base < a.n; base += static_cast<int64_t>(gridDim.x) * per_block) {
-    uint64_t e[kPairsPerThread], idx[kPairsPerThread], v[kPairsPerThread];
+    uint64_t e[kPairsPerThread], v[kPairsPerThread];
     uint32_t g[kPairsPerThread], x[kPairsPerThread];
     // independent loads first: group id, value, validity of every row
 #pragma unroll
@@ -814,6 +818,8 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
     // then the rank of each group (eight dependent loads in flight)
 #pragma unroll
     for (int j = 0; j < kPairsPerThread; ++j) g[j] = g[j] != kUnsetId ? __ldg(a.newid + g[j]) : kUnsetId;
+    // v[j] first holds the segment position of a scattered row (bit j of scat)
+    uint32_t scat = 0;
 #pragma unroll
     for (int j = 0; j < kPairsPerThread; ++j) {
       e[j] = kEmpty;
@@ -821,19 +827,25 @@ __global__ void __launch_bounds__(kGbThreads) nunique_kernel(NdArgs a)
         if (g[j] < a.hb) {
           const uint32_t off = (x[j] ^ a.flip) - a.vbase;
           red_or32(a.bits + static_cast<uint64_t>(g[j]) * a.wpr + (off >> 5), 1u << (off & 31));
+        } else if (g[j] >= a.s0) {
+          v[j] = atomicAdd(a.seg_cursor + (g[j] - a.s0), 1ull);  // eight in flight
+          scat |= 1u << j;
         } else {
           e[j] = (static_cast<uint64_t>(g[j]) << 32) | x[j];
         }
       }
-      idx[j] = e[j] != kEmpty ? fastrange(mix64(e[j]), a.cap) : 0;
     }
 #pragma unroll
-    for (int j = 0; j < kPairsPerThread; ++j) v[j] = e[j] != kEmpty ? a.set[idx[j]] : 0;
+    for (int j = 0; j < kPairsPerThread; ++j)
+      if (scat & (1u << j)) a.seg_vals[v[j]] = x[j];
+#pragma unroll
+    for (int j = 0; j < kPairsPerThread; ++j)
+      if (e[j] != kEmpty) v[j] = a.set[fastrange(mix64(e[j]), a.cap)];
 #pragma unroll
     for (int j = 0; j < kPairsPerThread; ++j) {
       if (e[j] == kEmpty) continue;
       bool fresh = false;
-      uint64_t xs = idx[j], cur = v[j];
+      uint64_t xs = fastrange(mix64(e[j]), a.cap), cur = v[j];
       int probe   = 0;
       for (; probe < kMaxProbe; ++probe) {
         if (cur == e[j]) break;
@@ -893,6 +905,126 @@ __global__ void value_range_kernel(DCol col, int64_t n, uint32_t flip, unsigned 
   if ((threadIdx.x & 31) == 0) {
     atomicMin(out, lo);
     atomicMax(out + 1, hi);
+  }
+}
+
+// ---- NUNIQUE of the per-rank segments ---------------------------------------
+// Ranks are in descending row-count order, so each size tier is a contiguous
+// rank range.  bounds[k] = first rank whose row count is <= seg_tier(k).
+constexpr int kSegTiers                 = 3;
+__host__ __device__ constexpr uint64_t seg_tier(int k) { return k == 0 ? 8192 : k == 1 ? 512 : 16; }
+constexpr int kSegBlockThreads          = 256;
+constexpr int kSegBlockSlots            = 16384;  // shared table of a block (64 KB)
+constexpr int kSegWarpSlots             = 1024;   // shared table of a warp (4 KB)
+constexpr uint32_t kSegEmpty            = 0xffffffffu;
+
+__global__ void seg_bounds_kernel(const unsigned long long* count, int64_t nid, int64_t* bounds)
+{
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < nid; g += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = count[g];
+    for (int k = 0; k < kSegTiers; ++k)
+      if (c <= seg_tier(k) && (g == 0 || count[g - 1] > seg_tier(k))) bounds[k] = g;
+  }
+}
+
+__device__ __forceinline__ uint32_t seg_hash(uint32_t x, int log2cap)
+{
+  return (x * 0x9e3779b1u) >> (32 - log2cap);
+}
+
+// Insert into a shared open-addressing table; true if x was not there yet.
+// The empty marker value itself is tracked by `saw_empty_value`.
+__device__ __forceinline__ bool seg_insert(uint32_t* table, int log2cap, uint32_t x, int* saw_empty_value)
+{
+  if (x == kSegEmpty) return atomicExch(saw_empty_value, 1) == 0;
+  const uint32_t mask = (1u << log2cap) - 1u;
+  uint32_t i          = seg_hash(x, log2cap);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t cur = atomicCAS(table + i, kSegEmpty, x);
+    if (cur == kSegEmpty) return true;
+    if (cur == x) return false;
+    i = (i + 1) & mask;
+  }
+  return false;  // unreachable: the table holds at most half its slots
+}
+
+__device__ __forceinline__ int seg_log2cap(uint64_t c, int max_log2)
+{
+  int l = 6;
+  while (l < max_log2 && (1ull << l) < 2 * c) ++l;
+  return l;
+}
+
+struct SegArgs {
+  const unsigned long long* start;  // segment start (exclusive scan of row counts)
+  const unsigned long long* end;    // segment end (the cursor after the scatter)
+  const uint32_t* vals;
+  unsigned long long* nd;           // distinct-count field, indexed by rank
+  int64_t s0;                       // rank of segment 0
+  int64_t r_begin, r_end;           // ranks of this tier
+};
+
+// 512 < rows <= 8192: one CTA per rank.
+__global__ void __launch_bounds__(kSegBlockThreads) seg_block_kernel(SegArgs a)
+{
+  extern __shared__ __align__(16) uint32_t table[];  // kSegBlockSlots entries
+  __shared__ int saw;
+  __shared__ unsigned int fresh;
+  for (int64_t g = a.r_begin + blockIdx.x; g < a.r_end; g += gridDim.x) {
+    const uint64_t b = a.start[g - a.s0], e = a.end[g - a.s0];
+    const int l2     = seg_log2cap(e - b, 14);
+    for (int i = threadIdx.x; i < (1 << l2); i += blockDim.x) table[i] = kSegEmpty;
+    if (threadIdx.x == 0) {
+      saw   = 0;
+      fresh = 0;
+    }
+    __syncthreads();
+    unsigned int mine = 0;
+    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) mine += seg_insert(table, l2, a.vals[i], &saw) ? 1u : 0u;
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&fresh, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) a.nd[g] = fresh;
+    __syncthreads();
+  }
+}
+
+// 16 < rows <= 512: one warp per rank, a 1024-slot table per warp.
+__global__ void __launch_bounds__(256) seg_warp_kernel(SegArgs a)
+{
+  __shared__ uint32_t tables[8][kSegWarpSlots];
+  __shared__ int saw[8];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* table = tables[w];
+  const int64_t nw = static_cast<int64_t>(gridDim.x) * 8;
+  for (int64_t g = a.r_begin + blockIdx.x * 8 + w; g < a.r_end; g += nw) {
+    const uint64_t b = a.start[g - a.s0], e = a.end[g - a.s0];
+    const int l2     = seg_log2cap(e - b, 10);
+    for (int i = lane; i < (1 << l2); i += 32) table[i] = kSegEmpty;
+    if (lane == 0) saw[w] = 0;
+    __syncwarp();
+    unsigned int mine = 0;
+    for (uint64_t i = b + lane; i < e; i += 32) mine += seg_insert(table, l2, a.vals[i], &saw[w]) ? 1u : 0u;
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    if (lane == 0) a.nd[g] = mine;
+    __syncwarp();
+  }
+}
+
+// rows <= 16: one thread per rank, pairwise comparison.
+__global__ void seg_thread_kernel(SegArgs a)
+{
+  for (int64_t g = a.r_begin + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.r_end;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t b = a.start[g - a.s0], e = a.end[g - a.s0];
+    unsigned int d   = 0;
+    for (uint64_t i = b; i < e; ++i) {
+      const uint32_t x = a.vals[i];
+      bool dup         = false;
+      for (uint64_t j = b; j < i && !dup; ++j) dup = a.vals[j] == x;
+      d += dup ? 0u : 1u;
+    }
+    a.nd[g] = d;
   }
 }
 
@@ -1415,6 +1547,9 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
   // bytes of NUNIQUE value bitmaps (kept well inside the 126 MB L2)
   uint64_t bitmap_budget = 48ull << 20;
   if (const char* e = std::getenv("LDF_B200_ND_BITMAP_MB")) bitmap_budget = std::max(0ll, std::atoll(e)) << 20;
+  // per-rank segments for the less frequent ranks (LDF_B200_ND_SEGMENTS=0 keeps them in the pair set)
+  bool seg_enabled = true;
+  if (const char* e = std::getenv("LDF_B200_ND_SEGMENTS")) seg_enabled = std::atoi(e) != 0;
 
   for (int attempt = 0;; ++attempt) {
     const uint64_t id_cap = cap + kIdFirst;
@@ -1577,8 +1712,18 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
                                                                                    : value_range_kernel<4>;
             launch("value_range", vk, static_cast<unsigned>(4 * num_sms()), 256, 0, s, c.col, n, na.flip, vr.get());
           }
+          // size tiers of the ranks (row counts are field 0 of the records)
+          Buffer<int64_t> tb(al, kSegTiers);
+          {
+            const int64_t init[kSegTiers] = {nid, nid, nid};
+            LDF_CUDA(cudaMemcpyAsync(tb.get(), init, sizeof(init), cudaMemcpyHostToDevice, s));
+            launch("seg_bounds", seg_bounds_kernel, gs_blocks(nid, 256), 256, 0, s,
+                   static_cast<const unsigned long long*>(rec.get()), nid, tb.get());
+          }
           unsigned int hv[2];
+          int64_t tier[kSegTiers];
           LDF_CUDA(cudaMemcpyAsync(hv, vr.get(), 8, cudaMemcpyDeviceToHost, s));
+          LDF_CUDA(cudaMemcpyAsync(tier, tb.get(), sizeof(tier), cudaMemcpyDeviceToHost, s));
           ctx.finish();
           Buffer<uint32_t> bits;
           if (hv[0] <= hv[1] && bitmap_budget > 0) {
@@ -1594,6 +1739,25 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
               na.vbase = hv[0];
             }
           }
+          // ranks from s0 on (at most seg_tier(0) rows each) go to per-rank segments
+          na.s0 = 0xffffffffu;
+          const int64_t s0 = std::max<int64_t>(static_cast<int64_t>(na.hb), tier[0]);
+          Buffer<unsigned long long> seg_start, seg_cursor;
+          Buffer<uint32_t> seg_vals;
+          if (seg_enabled && s0 < nid && n < (int64_t(1) << 32)) {
+            const int64_t T = nid - s0;
+            seg_start       = Buffer<unsigned long long>(al, T);
+            seg_cursor      = Buffer<unsigned long long>(al, T);
+            Buffer<int64_t> seg_total(al, 1);
+            exclusive_scan_i64(reinterpret_cast<const int64_t*>(rec.get() + s0),
+                               reinterpret_cast<int64_t*>(seg_start.get()), T, seg_total.get(), ctx);
+            LDF_CUDA(cudaMemcpyAsync(seg_cursor.get(), seg_start.get(), T * 8, cudaMemcpyDeviceToDevice, s));
+            const int64_t total = ctx.read_i64(seg_total.get());
+            seg_vals      = Buffer<uint32_t>(al, std::max<int64_t>(total, 1));
+            na.s0         = static_cast<uint32_t>(s0);
+            na.seg_cursor = seg_cursor.get();
+            na.seg_vals   = seg_vals.get();
+          }
           const size_t nd_smem = static_cast<size_t>(na.hot) * 4;
           int nocc             = 1;
           auto ndk = c.col.width == 1 ? nunique_kernel<1> : c.col.width == 2 ? nunique_kernel<2> : nunique_kernel<4>;
@@ -1604,6 +1768,26 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
           if (na.hb > 0)
             launch("bitmap_count", bitmap_count_kernel, std::min<unsigned>(na.hb, 4u * num_sms()), 256u, 0, s,
                    static_cast<const uint32_t*>(na.bits), na.hb, na.wpr, na.nd);
+          if (na.s0 != 0xffffffffu) {
+            SegArgs sa{seg_start.get(), seg_cursor.get(), seg_vals.get(), na.nd, s0, 0, 0};
+            const int64_t m1 = std::max(s0, tier[1]), m2 = std::max(m1, tier[2]);
+            sa.r_begin = s0;
+            sa.r_end   = m1;
+            if (m1 > s0) {
+              LDF_CUDA(cudaFuncSetAttribute(seg_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            kSegBlockSlots * 4));
+              launch("seg_block", seg_block_kernel, static_cast<unsigned>(std::min<int64_t>(m1 - s0, 3 * num_sms())),
+                     static_cast<unsigned>(kSegBlockThreads), static_cast<size_t>(kSegBlockSlots) * 4, s, sa);
+            }
+            sa.r_begin = m1;
+            sa.r_end   = m2;
+            if (m2 > m1)
+              launch("seg_warp", seg_warp_kernel,
+                     static_cast<unsigned>(std::min<int64_t>(ceil_div(m2 - m1, 8), 8 * num_sms())), 256u, 0, s, sa);
+            sa.r_begin = m2;
+            sa.r_end   = nid;
+            if (nid > m2) launch("seg_thread", seg_thread_kernel, gs_blocks(nid - m2, 256), 256u, 0, s, sa);
+          }
         } else {
           launch("nunique_generic", nunique_generic_kernel<M>, gs_blocks(n, 256), 256, 0, s, p, c,
                  static_cast<const uint32_t*>(gid.get()), static_cast<const uint32_t*>(newid.get()),

@@ -199,3 +199,31 @@ def test_groupby_special_float_keys_by_bits(dtype):
     exp = R.groupby(t, ["k"], aggs)
     assert res.num_rows == 5
     assert_tables_equal(res, exp, sort_by=["s"])
+
+
+@pytest.mark.parametrize("segments", ["1", "0"])
+@pytest.mark.parametrize("vtype", [np.int32, np.uint32])
+def test_groupby_nunique_size_tiers(segments, vtype, monkeypatch):
+    # group sizes on both sides of every tier boundary of the per-rank
+    # segments (8192 / 512 / 16 rows), a 32-bit-wide value range (no value
+    # bitmaps), the all-ones bit pattern as a value, and null values
+    monkeypatch.setenv("LDF_B200_ND_SEGMENTS", segments)
+    rng = np.random.default_rng(77)
+    sizes = ([20000, 9000, 8193, 8192, 5000, 513, 512, 511, 300, 17, 16, 15, 10, 2, 1]
+             + [1] * 2000 + [3] * 1000 + [40] * 500 + [700] * 40)
+    keys = np.repeat(np.arange(len(sizes), dtype=np.int64) * 7 + 3, sizes)
+    vals = np.empty(len(keys), dtype=np.int64)
+    pos = 0
+    for s in sizes:
+        base = int(rng.integers(0, 2**32))
+        vals[pos:pos + s] = (base + rng.integers(0, max(2, s // 2), s) * 2654435761) % 2**32
+        pos += s
+    vals[rng.random(len(vals)) < 0.01] = 2**32 - 1
+    v = vals.astype(np.uint32).view(vtype)
+    perm = rng.permutation(len(keys))
+    t = pa.table({"k": keys[perm], "v": pa.array(v[perm], mask=rng.random(len(keys)) < 0.1)})
+    aggs = [("v", "count_distinct", "nd"), ("v", ("count_distinct", pc.CountOptions(mode="all")), "nda"),
+            (None, "count_all", "n")]
+    res = run_groupby(t, ["k"], aggs)
+    exp = R.groupby(t, ["k"], aggs)
+    assert_tables_equal(res, exp, sort_by=["k"])
