@@ -72,16 +72,33 @@ inline void launch(const char* name, void (*kernel)(KArgs...), dim3 grid, dim3 b
 // allocator; with none, stream-ordered cudaMallocAsync.  Scratch buffers are
 // RAII and released on the same stream, so no device-wide synchronisation.
 // ---------------------------------------------------------------------------
+// Device memory of one call.  allocate/deallocate go straight to the
+// caller's allocator (outputs use them: the caller owns what they return).
+// Scratch buffers (Buffer<T>) of at most kSmallScratch bytes are carved from
+// kScratchChunk-byte chunks instead, which are handed back when the Allocator
+// is destroyed at the end of the call: one allocator round trip per chunk
+// rather than per buffer.
 class Allocator {
  public:
+  static constexpr size_t kSmallScratch = size_t(1) << 20;
+  static constexpr size_t kScratchChunk = size_t(16) << 20;
+
   Allocator(const ldf_allocator* a, cudaStream_t s) : a_(a), s_(s) {}
+  Allocator(const Allocator&)            = delete;
+  Allocator& operator=(const Allocator&) = delete;
+  ~Allocator();
   void* allocate(size_t nbytes) const;
   void deallocate(void* p, size_t nbytes) const;
+  void* allocate_scratch(size_t nbytes) const;
+  void deallocate_scratch(void* p, size_t nbytes) const;
   cudaStream_t stream() const { return s_; }
 
  private:
   const ldf_allocator* a_;
   cudaStream_t s_;
+  mutable std::vector<void*> chunks_;
+  mutable char* bump_  = nullptr;
+  mutable size_t left_ = 0;
 };
 
 template <typename T>
@@ -90,7 +107,7 @@ class Buffer {
   Buffer() = default;
   Buffer(const Allocator& a, size_t n) : a_(&a), n_(n)
   {
-    p_ = static_cast<T*>(a.allocate(bytes()));
+    p_ = static_cast<T*>(a.allocate_scratch(bytes()));
   }
   Buffer(const Buffer&)            = delete;
   Buffer& operator=(const Buffer&) = delete;
@@ -108,7 +125,7 @@ class Buffer {
   ~Buffer() { reset(); }
   void reset()
   {
-    if (p_ && a_) a_->deallocate(p_, bytes());
+    if (p_ && a_) a_->deallocate_scratch(p_, bytes());
     p_ = nullptr;
     n_ = 0;
   }

@@ -1591,7 +1591,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
         c.fb      = fb_bufs.back().get();
         c.special = sp_bufs.back().get();
       }
-      if (c.states & ST_NDIST) {
+      if ((c.states & ST_NDIST) && !c.pair_packed) {  // packed pair sets are sized exactly in pass 3
         c.pair_cap = pair_cap;
         pair_bufs.emplace_back(al, pair_cap);
         c.pairs = pair_bufs.back().get();
@@ -1739,25 +1739,47 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
               na.vbase = hv[0];
             }
           }
-          // ranks from s0 on (at most seg_tier(0) rows each) go to per-rank segments
-          na.s0 = 0xffffffffu;
-          const int64_t s0 = std::max<int64_t>(static_cast<int64_t>(na.hb), tier[0]);
+          // Ranks [hb, s0) go to the pair set, ranks [s0, nid) (at most
+          // seg_tier(0) rows each) to per-rank segments.  The prefix sums of
+          // the row counts from hb on give both the exact pair-set bound and
+          // the segment offsets.
+          na.s0            = 0xffffffffu;
+          const int64_t hb = static_cast<int64_t>(na.hb);
+          const int64_t s0 = (seg_enabled && n < (int64_t(1) << 32))
+                               ? std::min<int64_t>(std::max<int64_t>(hb, tier[0]), nid) : nid;
           Buffer<unsigned long long> seg_start, seg_cursor;
           Buffer<uint32_t> seg_vals;
-          if (seg_enabled && s0 < nid && n < (int64_t(1) << 32)) {
-            const int64_t T = nid - s0;
+          Buffer<unsigned long long> pairs;
+          int64_t pair_rows = 0;
+          if (nid > hb) {
+            const int64_t T = nid - hb;
             seg_start       = Buffer<unsigned long long>(al, T);
-            seg_cursor      = Buffer<unsigned long long>(al, T);
             Buffer<int64_t> seg_total(al, 1);
-            exclusive_scan_i64(reinterpret_cast<const int64_t*>(rec.get() + s0),
+            exclusive_scan_i64(reinterpret_cast<const int64_t*>(rec.get() + hb),
                                reinterpret_cast<int64_t*>(seg_start.get()), T, seg_total.get(), ctx);
-            LDF_CUDA(cudaMemcpyAsync(seg_cursor.get(), seg_start.get(), T * 8, cudaMemcpyDeviceToDevice, s));
-            const int64_t total = ctx.read_i64(seg_total.get());
-            seg_vals      = Buffer<uint32_t>(al, std::max<int64_t>(total, 1));
-            na.s0         = static_cast<uint32_t>(s0);
-            na.seg_cursor = seg_cursor.get();
-            na.seg_vals   = seg_vals.get();
+            int64_t hv2[2] = {0, 0};  // total rows of ranks >= hb, rows of ranks [hb, s0)
+            LDF_CUDA(cudaMemcpyAsync(&hv2[0], seg_total.get(), 8, cudaMemcpyDeviceToHost, s));
+            if (s0 < nid)
+              LDF_CUDA(cudaMemcpyAsync(&hv2[1], seg_start.get() + (s0 - hb), 8, cudaMemcpyDeviceToHost, s));
+            ctx.finish();
+            const int64_t total = hv2[0];
+            pair_rows           = s0 < nid ? hv2[1] : total;
+            if (s0 < nid) {
+              seg_cursor = Buffer<unsigned long long>(al, nid - s0);
+              LDF_CUDA(cudaMemcpyAsync(seg_cursor.get(), seg_start.get() + (s0 - hb), (nid - s0) * 8,
+                                       cudaMemcpyDeviceToDevice, s));
+              seg_vals      = Buffer<uint32_t>(al, std::max<int64_t>(total, 1));  // indexed by the prefix sums
+              na.s0         = static_cast<uint32_t>(s0);
+              na.seg_cursor = seg_cursor.get();
+              na.seg_vals   = seg_vals.get();
+            }
           }
+          // distinct pairs of ranks [hb, s0) <= their rows: load factor <= 0.5
+          const uint64_t pcap = static_cast<uint64_t>(std::max<int64_t>(64, 2 * pair_rows)) << attempt;
+          pairs   = Buffer<unsigned long long>(al, pcap);
+          LDF_CUDA(cudaMemsetAsync(pairs.get(), 0xff, pcap * 8, s));
+          na.set = pairs.get();
+          na.cap = pcap;
           const size_t nd_smem = static_cast<size_t>(na.hot) * 4;
           int nocc             = 1;
           auto ndk = c.col.width == 1 ? nunique_kernel<1> : c.col.width == 2 ? nunique_kernel<2> : nunique_kernel<4>;
@@ -1769,7 +1791,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
             launch("bitmap_count", bitmap_count_kernel, std::min<unsigned>(na.hb, 4u * num_sms()), 256u, 0, s,
                    static_cast<const uint32_t*>(na.bits), na.hb, na.wpr, na.nd);
           if (na.s0 != 0xffffffffu) {
-            SegArgs sa{seg_start.get(), seg_cursor.get(), seg_vals.get(), na.nd, s0, 0, 0};
+            SegArgs sa{seg_start.get() + (s0 - hb), seg_cursor.get(), seg_vals.get(), na.nd, s0, 0, 0};
             const int64_t m1 = std::max(s0, tier[1]), m2 = std::max(m1, tier[2]);
             sa.r_begin = s0;
             sa.r_end   = m1;

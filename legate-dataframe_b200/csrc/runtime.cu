@@ -110,6 +110,36 @@ void Allocator::deallocate(void* p, size_t nbytes) const
   }
 }
 
+void* Allocator::allocate_scratch(size_t nbytes) const
+{
+  if (nbytes == 0) nbytes = 16;
+  nbytes = (nbytes + 255) & ~size_t(255);
+  if (nbytes > kSmallScratch) return allocate(nbytes);
+  if (left_ < nbytes) {
+    bump_ = static_cast<char*>(allocate(kScratchChunk));
+    chunks_.push_back(bump_);
+    left_ = kScratchChunk;
+  }
+  void* p = bump_;
+  bump_ += nbytes;
+  left_ -= nbytes;
+  return p;
+}
+
+void Allocator::deallocate_scratch(void* p, size_t nbytes) const
+{
+  if (p == nullptr) return;
+  if (nbytes == 0) nbytes = 16;
+  nbytes = (nbytes + 255) & ~size_t(255);
+  if (nbytes > kSmallScratch) deallocate(p, nbytes);
+  // small scratch lives until its chunk is returned
+}
+
+Allocator::~Allocator()
+{
+  for (void* c : chunks_) deallocate(c, kScratchChunk);
+}
+
 OpContext::OpContext(const ldf_allocator* a, cudaStream_t s) : alloc_(a, s)
 {
   err_ = Buffer<int>(alloc_, 1);

@@ -133,3 +133,66 @@ def test_join_special_float_keys_by_bits(how, dtype):
     res = run_join(lhs, rhs, ["k"], ["k2"], how)
     exp = R.join(lhs, rhs, ["k"], ["k2"], how, True)
     assert_tables_equal(res, exp, sort_by=[c for c in exp.column_names if c in ("a", "b")], check_types=False)
+
+
+@pytest.mark.parametrize("how", ["inner", "left", "full", "semi", "anti"])
+@pytest.mark.parametrize("layout", ["fits", "fits_nullable", "too_wide"])
+@pytest.mark.parametrize("dups", [False, True])
+def test_join_mixed_width_outputs(how, layout, dups):
+    # int32 keys with rhs output columns of every width (1, 2, 4, 8 bytes,
+    # bool, float32), nullable or not, several int64 columns, duplicate and
+    # null keys
+    rng = np.random.default_rng(hash((how, layout, dups)) % 2**32)
+    nb, nl = 3000, 5000
+    bkeys = rng.integers(0, 2500 if dups else 10**6, nb).astype(np.int32)
+    if not dups:
+        bkeys = rng.permutation(np.arange(nb, dtype=np.int32) * 3)
+    # "fits": no nulls; "fits_nullable": nullable key and int16; "too_wide": three int64 columns
+    kmask = (rng.random(nb) < 0.03) if layout == "fits_nullable" else None
+    rcols = {"rk": pa.array(bkeys, mask=kmask)}
+    rcols["r8"] = pa.array(rng.integers(-100, 100, nb).astype(np.int8))
+    rcols["r16"] = pa.array(rng.integers(-30000, 30000, nb).astype(np.int16),
+                            mask=(rng.random(nb) < 0.2) if layout == "fits_nullable" else None)
+    rcols["rb"] = pa.array(rng.random(nb) < 0.5)
+    rcols["rf"] = pa.array(rng.normal(size=nb).astype(np.float32))
+    if layout != "fits_nullable":
+        rcols["r64"] = pa.array(rng.integers(-2**60, 2**60, nb))
+    if layout == "too_wide":
+        rcols["r64b"] = pa.array(rng.integers(-2**60, 2**60, nb))
+        rcols["r64c"] = pa.array(rng.integers(-2**60, 2**60, nb))
+    rhs = pa.table(rcols)
+    lk = np.where(rng.random(nl) < 0.7, bkeys[rng.integers(0, nb, nl)], rng.integers(-10**6, 0, nl)).astype(np.int32)
+    lhs = pa.table({"lk": pa.array(lk, mask=rng.random(nl) < 0.03), "lv": rng.normal(size=nl)})
+    ro = [] if how in ("semi", "anti") else None
+    res = run_join(lhs, rhs, ["lk"], ["rk"], how, True, None, ro)
+    exp = R.join(lhs, rhs, ["lk"], ["rk"], how, True, None, ro)
+    assert_tables_equal(res, exp, check_types=False)
+
+
+def test_join_repeated_row_counts():
+    # 2M unique int32 build keys, 4M probe rows (80% hits, 5% null keys):
+    # FULL, INNER and LEFT row counts equal a reference count on every repeat
+    import torch
+
+    from legate_dataframe import LogicalColumn, LogicalTable
+    from legate_dataframe.lib.join import JoinType, join
+
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(11)
+    nb, npr = 2_000_000, 4_000_000
+    bkey = torch.randperm(nb, device=dev, generator=g).to(torch.int32)
+    hit = torch.rand(npr, device=dev, generator=g) < 0.8
+    pkey = torch.where(hit, bkey[torch.randint(0, nb, (npr,), device=dev, generator=g)],
+                       torch.randint(nb, 2 * nb, (npr,), device=dev, generator=g, dtype=torch.int32))
+    pvalid = torch.rand(npr, device=dev, generator=g) >= 0.05
+    lt = LogicalTable([LogicalColumn.from_torch(pkey, pa.int32(), valid=pvalid)], ["lk"])
+    rt = LogicalTable([LogicalColumn.from_torch(bkey, pa.int32()),
+                       LogicalColumn.from_torch(torch.arange(nb, device=dev), pa.int64())], ["rk", "rv"])
+    vk = pkey[pvalid]
+    inner = int(torch.isin(vk, bkey).sum())
+    unmatched = int((~torch.isin(bkey, vk)).sum())
+    expect = {JoinType.INNER: inner, JoinType.LEFT: npr, JoinType.FULL: npr + unmatched}
+    for _ in range(6):
+        for jt, n in expect.items():
+            assert join(lt, rt, lhs_keys=["lk"], rhs_keys=["rk"], join_type=jt).num_rows() == n, jt
