@@ -196,3 +196,39 @@ def test_join_repeated_row_counts():
     for _ in range(6):
         for jt, n in expect.items():
             assert join(lt, rt, lhs_keys=["lk"], rhs_keys=["rk"], join_type=jt).num_rows() == n, jt
+
+
+@pytest.mark.parametrize("how", list(HOW))
+@pytest.mark.parametrize("nulls_equal", [True, False])
+@pytest.mark.parametrize("kind", ["int32", "int64", "float64", "uint8"])
+@pytest.mark.parametrize("dup", [False, True])
+def test_join_radix_partitioned(how, nulls_equal, kind, dup, monkeypatch):
+    # the radix-partitioned path (forced on small inputs): 256 hash partitions
+    # + a null-key partition on both sides, per-partition table regions
+    monkeypatch.setenv("LDF_B200_JOIN_PARTITION", "1")
+    rng = np.random.default_rng(zlib.crc32(f"p{how}{nulls_equal}{kind}{dup}".encode()))
+    nl, nr = 20000, 6000
+    kr = (3000 if dup else 10**6) if kind != "uint8" else 200
+    lhs = pa.table({"lk": _keys(rng, nl, kind, kr, 0.05), "lp": pa.array(rng.normal(size=nl), mask=rng.random(nl) < .1),
+                    "li": rng.integers(-9, 9, nl).astype(np.int32)})
+    rk = _keys(rng, nr, kind, kr, 0.05)
+    rhs = pa.table({"rk": rk, "rp": rng.integers(-9, 9, nr).astype(np.int16), "rb": pa.array(rng.random(nr) < 0.5),
+                    "r8": rng.integers(-2**60, 2**60, nr)})
+    ro = [] if how in ("semi", "anti") else None
+    res = run_join(lhs, rhs, ["lk"], ["rk"], how, nulls_equal, None, ro)
+    exp = R.join(lhs, rhs, ["lk"], ["rk"], how, nulls_equal, None, ro)
+    assert_tables_equal(res, exp)
+
+
+@pytest.mark.parametrize("how", list(HOW))
+def test_join_radix_partitioned_edges(how, monkeypatch):
+    monkeypatch.setenv("LDF_B200_JOIN_PARTITION", "1")
+    e = pa.table({"k": pa.array([], pa.int64()), "v": pa.array([], pa.float64())})
+    f = pa.table({"k": pa.array([1, 2, 2], pa.int64()), "v": pa.array([1.0, 2.0, 3.0])})
+    for lhs, rhs in ((e, f), (f, e), (e, e), (f, f)):
+        rhs = rhs.rename_columns(["kr", "w"])
+        assert_tables_equal(run_join(lhs, rhs, ["k"], ["kr"], how), R.join(lhs, rhs, ["k"], ["kr"], how))
+    lhs = pa.table({"k": pa.array([None] * 5, pa.int32()), "v": np.arange(5)})
+    rhs = pa.table({"kr": pa.array([None, 1, None], pa.int32()), "w": np.arange(3)})
+    for ne in (True, False):
+        assert_tables_equal(run_join(lhs, rhs, ["k"], ["kr"], how, ne), R.join(lhs, rhs, ["k"], ["kr"], how, ne))
