@@ -187,6 +187,7 @@ struct DCol {
   int64_t chars_base;
   int32_t type;
   int32_t width;
+  int64_t num_chars;  // bytes of `chars` (strings)
 };
 
 inline DCol make_dcol(const ldf_column& c)
@@ -198,6 +199,7 @@ inline DCol make_dcol(const ldf_column& c)
   d.chars_base = c.chars_base;
   d.type       = c.type;
   d.width      = type_width(c.type);
+  d.num_chars  = c.type == LDF_STRING ? c.num_chars : 0;
   return d;
 }
 

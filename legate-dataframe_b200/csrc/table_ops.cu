@@ -58,23 +58,117 @@ __global__ void string_lengths_kernel(DCol src, const int32_t* map, int64_t rows
   }
 }
 
-// One warp per 32 rows; each lane copies its row's bytes.  Ranges are written
+// Tiles of kStrTile x kStrRows rows.  Each thread handles kStrRows rows and
+// issues their loads together: map entries, source ranges, then every
+// string's bytes as at most kStrWords aligned 8-byte words (only words inside
+// the chars buffer; longer strings and the buffer's edges go byte by byte).
+// The tile's chars (a contiguous output range) are assembled in shared memory
+// at the output's 16-byte phase and written with 16-byte stores (bytes at the
+// range's two ends, shared with the neighbouring tiles, singly).  A tile whose
+// chars exceed the staging buffer writes bytes directly.  Ranges are written
 // as local offsets with chars_base = 0.
-__global__ void string_copy_kernel(DCol src, const int32_t* map, int64_t rows,
-                                   const int64_t* offs, ldf_range* dst_ranges, uint8_t* dst_valid,
-                                   uint8_t* dst_chars)
+constexpr int kStrTile  = 256;
+constexpr int kStrRows  = 2;
+constexpr int kStrWords = 4;
+constexpr int kStrStage = 16 * 1024;
+
+__global__ void __launch_bounds__(kStrTile) string_copy_kernel(DCol src, const int32_t* map, int64_t rows,
+                                                               const int64_t* offs, int64_t nchars,
+                                                               ldf_range* dst_ranges, uint8_t* dst_valid,
+                                                               uint8_t* dst_chars)
 {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r  = map ? map[i] : i;
-    bool ok    = r >= 0 && dvalid(src, r);
-    int64_t o  = offs[i];
-    int64_t n  = ok ? dstr_len(src, r) : 0;
-    dst_ranges[i] = ldf_range{o, o + n - 1};
-    if (dst_valid) dst_valid[i] = ok ? 1 : 0;
-    if (n > 0) {
-      const uint8_t* p = dstr_ptr(src, r);
-      for (int64_t b = 0; b < n; ++b) dst_chars[o + b] = p[b];
+  __shared__ __align__(16) uint8_t stage[kStrStage + 16];
+  const ldf_range* rg_src = static_cast<const ldf_range*>(src.data);
+  const uintptr_t cbeg    = reinterpret_cast<uintptr_t>(src.chars);
+  const uintptr_t cend    = cbeg + static_cast<uintptr_t>(src.num_chars);
+  const int64_t per_tile  = static_cast<int64_t>(kStrTile) * kStrRows;
+  for (int64_t tile = blockIdx.x; tile * per_tile < rows; tile += gridDim.x) {
+    const int64_t i0 = tile * per_tile;
+    int64_t r[kStrRows], o[kStrRows], n[kStrRows];
+    const uint8_t* p[kStrRows];
+#pragma unroll
+    for (int j = 0; j < kStrRows; ++j) {
+      const int64_t i = i0 + j * kStrTile + threadIdx.x;
+      r[j]            = -2;
+      if (i < rows) r[j] = map ? __ldg(map + i) : i;
+    }
+#pragma unroll
+    for (int j = 0; j < kStrRows; ++j) {
+      const int64_t i = i0 + j * kStrTile + threadIdx.x;
+      n[j] = 0;
+      o[j] = 0;
+      p[j] = nullptr;
+      if (r[j] == -2) continue;
+      o[j]          = offs[i];
+      const bool ok = r[j] >= 0 && dvalid(src, r[j]);
+      if (ok) {
+        const ldf_range rg = rg_src[r[j]];
+        n[j]               = rg.hi - rg.lo + 1;
+        p[j]               = reinterpret_cast<const uint8_t*>(src.chars) + (rg.lo - src.chars_base);
+      }
+      dst_ranges[i] = ldf_range{o[j], o[j] + n[j] - 1};
+      if (dst_valid) dst_valid[i] = ok ? 1 : 0;
+    }
+    // the strings' words (all loads of the thread in flight together)
+    unsigned long long w[kStrRows][kStrWords];
+    int sh[kStrRows];
+    bool fast[kStrRows];
+#pragma unroll
+    for (int j = 0; j < kStrRows; ++j) {
+      const uintptr_t a  = reinterpret_cast<uintptr_t>(p[j]);
+      const uintptr_t a0 = a & ~uintptr_t(7);
+      sh[j]              = static_cast<int>(a - a0);
+      fast[j]            = n[j] > 0 && sh[j] + n[j] <= 8 * kStrWords;
+#pragma unroll
+      for (int k = 0; k < kStrWords; ++k) {
+        const uintptr_t wa = a0 + 8 * k;
+        w[j][k]            = 0;
+        if (fast[j] && 8 * k < sh[j] + n[j]) {
+          if (wa >= cbeg && wa + 8 <= cend) w[j][k] = __ldg(reinterpret_cast<const unsigned long long*>(wa));
+          else fast[j] = false;
+        }
+      }
+    }
+    const int64_t lo    = offs[i0];
+    const int64_t hi    = i0 + per_tile < rows ? offs[i0 + per_tile] : nchars;
+    // stage[k] <-> dst_chars[abase + k], with dst_chars + abase 16-byte aligned
+    const int64_t abase = lo - static_cast<int64_t>(reinterpret_cast<uintptr_t>(dst_chars + lo) & 15);
+    const bool staged   = hi - abase <= kStrStage;
+#pragma unroll
+    for (int j = 0; j < kStrRows; ++j) {
+      uint8_t* q = staged ? stage + (o[j] - abase) : dst_chars + o[j];
+      if (fast[j]) {
+        // string word k = bytes [8k, 8k + 8) of the string (funnel shift by the
+        // source misalignment); every index below is a compile-time constant
+        const int s8 = 8 * sh[j];
+#pragma unroll
+        for (int k = 0; k < kStrWords; ++k) {
+          const unsigned long long nxt = k + 1 < kStrWords ? w[j][k + 1] : 0ull;
+          const unsigned long long wk  = s8 == 0 ? w[j][k] : ((w[j][k] >> s8) | (nxt << (64 - s8)));
+#pragma unroll
+          for (int bb = 0; bb < 8; ++bb)
+            if (8 * k + bb < n[j]) q[8 * k + bb] = static_cast<uint8_t>(wk >> (8 * bb));
+        }
+      } else {
+        for (int64_t b = 0; b < n[j]; ++b) q[b] = __ldg(p[j] + b);
+      }
+    }
+    if (staged) {
+      __syncthreads();
+      // chunk c covers dst positions [abase + 16c, abase + 16c + 16)
+      const int64_t nchunks = (hi - abase + 15) >> 4;
+      for (int64_t c = threadIdx.x; c < nchunks; c += blockDim.x) {
+        const int64_t a0 = abase + 16 * c;
+        if (a0 >= lo && a0 + 16 <= hi) {
+          *reinterpret_cast<uint4*>(dst_chars + a0) = *reinterpret_cast<const uint4*>(stage + 16 * c);
+        } else {
+          for (int k = 0; k < 16; ++k) {
+            const int64_t a = a0 + k;
+            if (a >= lo && a < hi) dst_chars[a] = stage[16 * c + k];
+          }
+        }
+      }
+      __syncthreads();
     }
   }
 }
@@ -124,9 +218,10 @@ void gather_strings(const OpContext& ctx, const DCol& src, const int32_t* map, i
   dst.chars      = static_cast<char*>(a.allocate(static_cast<size_t>(nchars)));
   dst.num_chars  = nchars;
   dst.chars_base = 0;
-  launch("string_copy", string_copy_kernel, grid_for(rows, 256), 256, 0, s, 
-    src, map, rows, offs.get(), static_cast<ldf_range*>(dst.data), dst.valid,
-    reinterpret_cast<uint8_t*>(dst.chars));
+  launch("string_copy", string_copy_kernel, grid_for(ceil_div(rows, kStrRows), kStrTile), kStrTile, 0, s, src, map,
+         rows,
+         static_cast<const int64_t*>(offs.get()), nchars, static_cast<ldf_range*>(dst.data), dst.valid,
+         reinterpret_cast<uint8_t*>(dst.chars));
   LDF_CHECK_LAUNCH();
 }
 
