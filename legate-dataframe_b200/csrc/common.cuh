@@ -304,12 +304,56 @@ __device__ __forceinline__ bool bytes_equal(const uint8_t* a, const uint8_t* b, 
   return true;
 }
 
+// A string of at most 32 bytes as 4 little-endian words w[k] = bytes
+// [8k, 8k + 8) (zero past the end), read with at most 5 aligned 8-byte loads
+// that stay inside the column's chars buffer.  False (w untouched) when the
+// string is longer or the loads would leave the buffer.
+__device__ __forceinline__ bool str_words(const DCol& c, const uint8_t* p, int64_t n, uint64_t w[4])
+{
+  if (n > 32) return false;
+  const uintptr_t a  = reinterpret_cast<uintptr_t>(p);
+  const uintptr_t a0 = a & ~uintptr_t(7);
+  const int sh       = static_cast<int>(a - a0);
+  const int nw       = static_cast<int>((sh + n + 7) >> 3);
+  const uintptr_t cb = reinterpret_cast<uintptr_t>(c.chars);
+  if (n > 0 && (a0 < cb || a0 + 8 * static_cast<uintptr_t>(nw) > cb + static_cast<uintptr_t>(c.num_chars)))
+    return false;
+  uint64_t raw[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) raw[k] = k < nw ? __ldg(reinterpret_cast<const unsigned long long*>(a0) + k) : 0ull;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    uint64_t v      = sh ? ((raw[k] >> (8 * sh)) | (raw[k + 1] << (64 - 8 * sh))) : raw[k];
+    const int64_t m = n - 8 * k;  // bytes of the string in word k
+    if (m <= 0) v = 0;
+    else if (m < 8) v &= (1ull << (8 * m)) - 1;
+    w[k] = v;
+  }
+  return true;
+}
+
+// hash_bytes of a string given as str_words.
+__device__ __forceinline__ uint64_t hash_words(const uint64_t w[4], int64_t n)
+{
+  uint64_t h = 0x27d4eb2f165667c5ull ^ (static_cast<uint64_t>(n) * 0x9e3779b97f4a7c15ull);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (8 * k < n) h = mix64(h ^ w[k]) + 0x165667b19e3779f9ull;
+  return mix64(h);
+}
+
 // Hash of one column value of a row, null-aware.  A null hashes to a fixed
 // constant.
 __device__ __forceinline__ uint64_t hash_value(const DCol& c, int64_t r)
 {
   if (!dvalid(c, r)) return 0x5bd1e9955bd1e995ull;
-  if (c.type == LDF_STRING) return hash_bytes(dstr_ptr(c, r), dstr_len(c, r));
+  if (c.type == LDF_STRING) {
+    const uint8_t* p = dstr_ptr(c, r);
+    const int64_t n  = dstr_len(c, r);
+    uint64_t w[4];
+    if (str_words(c, p, n, w)) return hash_words(w, n);
+    return hash_bytes(p, n);
+  }
   return mix64(dbits(c, r) + 0x9e3779b97f4a7c15ull * static_cast<uint64_t>(c.width));
 }
 
@@ -323,7 +367,12 @@ __device__ __forceinline__ bool values_equal(const DCol& a, int64_t ra, const DC
   if (a.type == LDF_STRING) {
     int64_t la = dstr_len(a, ra), lb = dstr_len(b, rb);
     if (la != lb) return false;
-    return bytes_equal(dstr_ptr(a, ra), dstr_ptr(b, rb), la);
+    const uint8_t* pa = dstr_ptr(a, ra);
+    const uint8_t* pb = dstr_ptr(b, rb);
+    uint64_t wa[4], wb[4];
+    if (str_words(a, pa, la, wa) && str_words(b, pb, lb, wb))
+      return wa[0] == wb[0] && wa[1] == wb[1] && wa[2] == wb[2] && wa[3] == wb[3];
+    return bytes_equal(pa, pb, la);
   }
   return dbits(a, ra) == dbits(b, rb);
 }

@@ -34,7 +34,7 @@ __global__ void str_find_insert_kernel(DCol col, int64_t n, unsigned long long* 
       row_slot[r] = -1;
       continue;
     }
-    const uint64_t h     = hash_bytes(dstr_ptr(col, r), dstr_len(col, r));
+    const uint64_t h     = hash_value(col, r);  // valid row: hash_bytes of the string
     const uint64_t entry = (static_cast<uint64_t>(r) << 32) | static_cast<uint32_t>(h);
     uint64_t idx         = fastrange(h, cap);
     int64_t found        = -1;
