@@ -163,6 +163,17 @@ int ldf_b200_hash_partition(const ldf_column* table, int32_t ncols,
                             ldf_column* out, int64_t* offsets,
                             const ldf_allocator* alloc, void* stream);
 
+/* ---- distinct ------------------------------------------------------------ */
+/* One row per distinct combination of the `keys` columns; `out` receives
+ * every column of `table` (ncols entries), whole rows of one representative
+ * input row per group (for non-key columns "any value is possible").  Null
+ * keys form one group.  Output row order is unspecified.  Replaces
+ * cudf::distinct in DistinctTask::gpu_variant (stream_compaction.cu:45-76);
+ * semantics of legate::dataframe::distinct (stream_compaction.cpp:121-150). */
+int ldf_b200_distinct(const ldf_column* table, int32_t ncols,
+                      const int32_t* keys, int32_t nkeys,
+                      ldf_column* out, const ldf_allocator* alloc, void* stream);
+
 /* ---- hash partition without device allocation ----------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory themselves -- a task body running concurrently with other tasks on the

@@ -31,6 +31,7 @@ SOURCES = [
     "abi.cu",
     "noalloc.cu",
     "batch.cu",
+    "distinct.cu",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -13,6 +13,8 @@ void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const u
                 bool nulls_at_end, int64_t limit, ldf_column* out, const OpContext& ctx);
 void hash_partition(const ldf_column* table, int ncols, const int32_t* keys, int nkeys, int nparts,
                     ldf_column* out, int64_t* offsets, const OpContext& ctx);
+void distinct(const ldf_column* table, int ncols, const int32_t* keys, int nkeys, ldf_column* out,
+              const OpContext& ctx);
 }  // namespace ldf
 
 namespace {
@@ -109,6 +111,17 @@ int ldf_b200_hash_partition(const ldf_column* table, int32_t ncols, const int32_
     LDF_REQUIRE(offsets != nullptr, "null offsets array");
     ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
     ldf::hash_partition(table, ncols, keys, nkeys, nparts, out, offsets, ctx);
+  });
+}
+
+int ldf_b200_distinct(const ldf_column* table, int32_t ncols, const int32_t* keys, int32_t nkeys, ldf_column* out,
+                      const ldf_allocator* alloc, void* stream)
+{
+  return guarded([&] {
+    check_table(table, ncols, "table");
+    LDF_REQUIRE(out != nullptr || ncols == 0, "null output array");
+    ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
+    ldf::distinct(table, ncols, keys, nkeys, out, ctx);
   });
 }
 

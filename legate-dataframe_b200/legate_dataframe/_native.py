@@ -131,6 +131,10 @@ def lib():
                 P(ldf_column), ctypes.c_int32, i32p, ctypes.c_int32, ctypes.c_int32,
                 P(ldf_column), P(ctypes.c_int64), P(ldf_allocator), ctypes.c_void_p,
             ]
+            L.ldf_b200_distinct.argtypes = [
+                P(ldf_column), ctypes.c_int32, i32p, ctypes.c_int32, P(ldf_column),
+                P(ldf_allocator), ctypes.c_void_p,
+            ]
             L.ldf_b200_free_column.argtypes = [P(ldf_column), P(ldf_allocator), ctypes.c_void_p]
             L.ldf_b200_hash_partition_noalloc.argtypes = [
                 P(ldf_column), ctypes.c_int32, i32p, ctypes.c_int32, ctypes.c_int32,
@@ -144,7 +148,7 @@ def lib():
             L.ldf_b200_last_error.restype = ctypes.c_char_p
             L.ldf_b200_version.restype = ctypes.c_char_p
             for name in ("ldf_b200_join", "ldf_b200_groupby_aggregation", "ldf_b200_sort",
-                         "ldf_b200_hash_partition", "ldf_b200_free_column"):
+                         "ldf_b200_hash_partition", "ldf_b200_distinct", "ldf_b200_free_column"):
                 getattr(L, name).restype = ctypes.c_int
             _lib = L
     return _lib

@@ -122,3 +122,13 @@ def test_columns_roundtrip_on_host():
     # slices keep their offsets right
     t2 = t.slice(7, 20)
     assert _cpu_table(t2).to_arrow().equals(t2)
+
+
+def test_python_distinct_argument_errors():
+    from legate_dataframe.lib.stream_compaction import distinct
+
+    tbl = _cpu_table(pa.table({"a": [0, 1, 1], "b": [1.0, 2.0, 3.0]}))
+    with pytest.raises(ValueError):
+        distinct(tbl, [])
+    with pytest.raises(IndexError):
+        distinct(tbl, ["nope"])
