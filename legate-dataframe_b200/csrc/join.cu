@@ -81,6 +81,7 @@ struct BuildTable {
   int parts;
   const uint64_t* part_base;
   const uint64_t* part_cap;
+  int* dup;  // K32: set by the build when a key occurs twice
 };
 
 // First slot and slot range [lo, hi) of hash h.
@@ -128,9 +129,15 @@ __global__ void build_kernel(BuildTable t, int64_t n)
       uint32_t tag   = M == KeyMode::GEN ? static_cast<uint32_t>(h) : static_cast<uint32_t>(kb);
       uint64_t entry = (static_cast<uint64_t>(r) << 32) | tag;
       uint64_t* s    = static_cast<uint64_t*>(t.slots);
-      while (atomicCAS(reinterpret_cast<unsigned long long*>(&s[idx]), kEmpty64,
-                       static_cast<unsigned long long>(entry)) != kEmpty64)
+      while (true) {
+        const unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long*>(&s[idx]), kEmpty64,
+                                                 static_cast<unsigned long long>(entry));
+        if (old == kEmpty64) break;
+        // K32: the tag is the whole key, and an equal key inserted earlier
+        // (or concurrently) always lies on this probe path
+        if (M == KeyMode::K32 && t.dup && static_cast<uint32_t>(old) == tag) *t.dup = 1;
         idx = next_slot(idx, lo, hi);
+      }
     }
   }
 }
@@ -775,6 +782,13 @@ void run_join(const OpContext& ctx, const KeyCols& pk, int64_t n_probe, const Ke
     t.null_list  = null_list.get();
     t.null_count = null_count.get();
   }
+  // K32 builds flag duplicate keys themselves (the slot word holds the key)
+  Buffer<int64_t> dupflag;
+  if (M == KeyMode::K32) {
+    dupflag = Buffer<int64_t>(al, 1);
+    LDF_CUDA(cudaMemsetAsync(dupflag.get(), 0, sizeof(int64_t), s));
+    t.dup = reinterpret_cast<int*>(dupflag.get());
+  }
   if (n_build > 0) {
     launch("build", build_kernel<M>, grid_stride_blocks(n_build, 256), 256, 0, s, t, n_build);
     LDF_CHECK_LAUNCH();
@@ -782,7 +796,13 @@ void run_join(const OpContext& ctx, const KeyCols& pk, int64_t n_probe, const Ke
 
   // ---- uniqueness ----------------------------------------------------------
   bool unique = true;
-  if (n_build > 1) {
+  if (M == KeyMode::K32 && n_build > 1) {
+    int64_t h[2] = {0, 0};  // duplicate flag, null-key rows (all equal with nulls_equal)
+    LDF_CUDA(cudaMemcpyAsync(&h[0], dupflag.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    if (t.null_count) LDF_CUDA(cudaMemcpyAsync(&h[1], t.null_count, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    ctx.finish();
+    unique = static_cast<int>(h[0]) == 0 && h[1] <= 1;
+  } else if (n_build > 1) {
     Buffer<int64_t> dup(al, 1);
     LDF_CUDA(cudaMemsetAsync(dup.get(), 0, sizeof(int64_t), s));
     launch("dup_check", dup_check_kernel<M>, grid_stride_blocks(n_build, 256), 256, 0, s, 
