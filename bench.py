@@ -3,6 +3,10 @@
 10% nulls; int32 U[0, 1e6)); SUM and MEAN of the float64 column, COUNT(*) and
 COUNT of the float64 column, MIN/MAX and NUNIQUE of the int32 column.
 
+`--workload join` / `--workload strings` instead print one line per op of
+the 200M x 20M int32-key joins / the 100M-row string-key groupby, stable sort
+and hash partition (device ms, rows/s, per-kernel ms).
+
 One step = one groupby_aggregation call through the public API (C ABI) on
 device-resident inputs (4.2 GB, far larger than the 126 MB L2, so no flush is
 needed).  Prints ONE JSON line (rank 0).  At N=1 the line also carries
@@ -143,7 +147,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-f", self.path],
+                 "-lms", "50", "-f", self.path],
                 stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -302,10 +306,147 @@ def run_served(device, n_requests: int):
     }
 
 
+# ---------------------------------------------------------------------------
+# other workloads of the path (not the default line): `--workload join` runs
+# the 200M x 20M int32-key hash joins, `--workload strings` the 100M-row
+# string-key groupby / stable sort / hash partition; one JSON line per op
+# with device ms, rows/s and per-kernel ms (CUDA events on the stream)
+# ---------------------------------------------------------------------------
+def _profiled(N, fn, steps):
+    import torch
+
+    for _ in range(2):
+        r = fn()
+        del r
+    torch.cuda.synchronize()
+    N.profile_enable(True)
+    N.profile_report(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        r = fn()
+        rows = r[0].num_rows() if isinstance(r, tuple) else r.num_rows()
+        del r
+    e1.record()
+    torch.cuda.synchronize()
+    prof = N.profile_report(reset=True)
+    N.profile_enable(False)
+    return e0.elapsed_time(e1) / steps, rows, {k: [c // steps, round(t / steps, 3)] for k, (c, t) in
+                                               sorted(prof.items(), key=lambda kv: -kv[1][1])}
+
+
+def run_join_workload(args):
+    """Build 20M rows (int32 keys = a permutation of [0, 20M), two int64
+    payloads); probe rows (--rows, default 200M): with p=0.8 a build key of
+    Zipf(0.9) rank, else U[20M, 40M); 5% null keys; one float64 payload."""
+    import pyarrow as pa
+    import torch
+
+    from legate_dataframe import LogicalColumn, LogicalTable
+    from legate_dataframe import _native as N
+    from legate_dataframe.lib.join import JoinType, join
+
+    dev = torch.device("cuda", 0)
+    nb, npr = 20_000_000, args.rows
+    g = torch.Generator(device=dev)
+    g.manual_seed(6)
+    bkey = torch.randperm(nb, device=dev, generator=g).to(torch.int32)
+    bp1 = torch.randint(-(2**40), 2**40, (nb,), device=dev, generator=g)
+    bp2 = torch.randint(-(2**40), 2**40, (nb,), device=dev, generator=g)
+    g.manual_seed(7)
+    cdf = torch.cumsum(torch.arange(1, nb + 1, device=dev, dtype=torch.float64).pow(-0.9), 0)
+    cdf /= cdf[-1].clone()
+    u = torch.rand(npr, device=dev, generator=g, dtype=torch.float64)
+    hit = torch.rand(npr, device=dev, generator=g) < 0.8
+    idx = torch.searchsorted(cdf, u).clamp_(max=nb - 1)
+    miss = torch.randint(nb, 2 * nb, (npr,), device=dev, generator=g, dtype=torch.int32)
+    pkey = torch.where(hit, bkey[idx], miss)
+    pvalid = torch.rand(npr, device=dev, generator=g) >= 0.05
+    ppay = torch.rand(npr, device=dev, generator=g, dtype=torch.float64)
+    del cdf, u, hit, idx, miss
+    lt = LogicalTable([LogicalColumn.from_torch(pkey, pa.int32(), valid=pvalid),
+                       LogicalColumn.from_torch(ppay, pa.float64())], ["lk", "lv"])
+    rt = LogicalTable([LogicalColumn.from_torch(bkey, pa.int32()), LogicalColumn.from_torch(bp1, pa.int64()),
+                       LogicalColumn.from_torch(bp2, pa.int64())], ["rk", "r1", "r2"])
+    peak, kind = measured_peak_gbs()
+    for jt in (JoinType.INNER, JoinType.LEFT, JoinType.FULL):
+        ms, rows, kern = _profiled(N, lambda: join(lt, rt, lhs_keys=["lk"], rhs_keys=["rk"], join_type=jt),
+                                   args.steps)
+        in_b = nb * 20 + npr * 13
+        out_b = rows * (4 + 1 + 8 + 4 + 8 + 8 + (3 if jt != JoinType.INNER else 0))
+        print(json.dumps({"workload": f"join {jt.name.lower()}: {npr} probe x {nb} build rows", "ms": round(ms, 3),
+                          "rows_per_s": (npr + nb) / (ms / 1e3), "out_rows": rows,
+                          "op_GBps_algorithmic": (in_b + out_b) / (ms / 1e3) / 1e9,
+                          "op_frac_of_peak": (in_b + out_b) / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
+                          "kernels_ms": kern}), flush=True)
+    return 0
+
+
+def run_strings_workload(args):
+    """--rows (default 100M) rows: string key drawn Zipf(1.0) from a 2M-entry
+    dictionary of [a-z0-9] strings of length U{8..24}; int64 timestamps over
+    one year; float32 LogNormal(0,1) values.  groupby SUM/COUNT(*) on the key,
+    stable sort (key asc, ts desc), hash_partition(key, 256)."""
+    import numpy as np
+    import pyarrow as pa
+    import torch
+
+    from legate_dataframe import LogicalColumn, LogicalTable
+    from legate_dataframe import _native as N
+    from legate_dataframe.lib.groupby_aggregation import groupby_aggregation
+    from legate_dataframe.lib.hash_partition import hash_partition
+    from legate_dataframe.lib.sort import sort
+
+    dev = torch.device("cuda", 0)
+    n, nd = args.rows, 2_000_000
+    rng = np.random.default_rng(9)
+    lens = rng.integers(8, 25, nd)
+    alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz0123456789", dtype=np.uint8)
+    d_chars = torch.from_numpy(alphabet[rng.integers(0, 36, int(lens.sum()))].copy()).to(dev)
+    doff = np.zeros(nd + 1, np.int64)
+    np.cumsum(lens, out=doff[1:])
+    d_off = torch.from_numpy(doff).to(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(9)
+    cdf = torch.cumsum(1.0 / torch.arange(1, nd + 1, device=dev, dtype=torch.float64), 0)
+    cdf /= cdf[-1].clone()
+    pick = torch.searchsorted(cdf, torch.rand(n, device=dev, generator=g, dtype=torch.float64)).clamp_(max=nd - 1)
+    row_len = (d_off[1:] - d_off[:-1])[pick]
+    row_off = torch.cumsum(row_len, 0) - row_len
+    rowid = torch.repeat_interleave(torch.arange(n, device=dev), row_len)
+    pos = torch.arange(int(row_len.sum()), device=dev)
+    chars = d_chars[d_off[pick][rowid] + (pos - row_off[rowid])]
+    del rowid, pos, cdf
+    ranges = torch.stack([row_off, row_off + row_len - 1], 1).contiguous()
+    t0 = 1_600_000_000_000_000
+    ts = torch.randint(t0, t0 + 365 * 86400 * 10**6, (n,), device=dev, generator=g)
+    val = torch.exp(torch.randn(n, device=dev, generator=g)).to(torch.float32)
+    key = LogicalColumn(pa.string(), N.LDF_STRING, n, ranges.view(torch.uint8).reshape(-1), None, chars=chars,
+                        chars_base=0, num_chars=chars.numel())
+    t = LogicalTable([key, LogicalColumn.from_torch(ts, pa.timestamp("us")),
+                      LogicalColumn.from_torch(val, pa.float32())], ["k", "ts", "v"])
+    row_bytes = 16 + chars.numel() / n + 8 + 4
+    ops = {
+        "groupby SUM/COUNT(*) on the string key": (lambda: groupby_aggregation(
+            t, ["k"], [("v", "sum", "s"), (None, "count_all", "c")]), n * (16 + chars.numel() / n + 4)),
+        "stable sort (key asc, ts desc)": (lambda: sort(t, ["k", "ts"], sort_ascending=[True, False], stable=True),
+                                           2 * n * row_bytes),
+        "hash_partition(key, 256)": (lambda: hash_partition(t, ["k"], 256), 2 * n * row_bytes),
+    }
+    peak, kind = measured_peak_gbs()
+    for name, (fn, algo) in ops.items():
+        ms, rows, kern = _profiled(N, fn, args.steps)
+        print(json.dumps({"workload": f"{name}: {n} rows", "ms": round(ms, 3), "rows_per_s": n / (ms / 1e3),
+                          "out_rows": rows, "op_GBps_algorithmic": algo / (ms / 1e3) / 1e9,
+                          "op_frac_of_peak": algo / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
+                          "kernels_ms": kern}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows", type=int, default=N_ROWS)
@@ -315,9 +456,15 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-requests", type=int, default=8192)
     ap.add_argument("--ref-rows", type=int, default=8_000_000, help="rows per step of the reference arm")
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "join", "strings"],
+                    help="groupby = the benchmark line; join / strings print per-op lines")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "groupby":
+        if args.rows == N_ROWS and args.workload == "strings":
+            args.rows = 100_000_000
+        return run_join_workload(args) if args.workload == "join" else run_strings_workload(args)
 
     import torch
     import torch.distributed as dist
