@@ -550,6 +550,8 @@ struct ColArgs {
   unsigned int* special;
   int hot;
   int sh_vcount, sh_sum, sh_mn, sh_mx, smem_bytes;
+  unsigned int* vrange;  // != null: also record min/max of the (flipped) value bits of the rows (NUNIQUE range)
+  uint32_t vflip;
 };
 
 // Value of row r as raw bits, and its order-preserving encoding (64-bit form,
@@ -606,6 +608,7 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
   constexpr bool MM64 = W > 4;
   const int H         = a.hot;
   const int64_t step  = static_cast<int64_t>(gridDim.x) * blockDim.x * kRows;
+  uint32_t vlo = 0xffffffffu, vhi = 0;
   for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x) * kRows; base < a.n; base += step) {
     uint32_t g[kRows];
     uint64_t raw[kRows];
@@ -619,6 +622,15 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
       raw[j] = ok[j] ? load_raw<W, SGN, FLT>(a.col.data, r) : 0;
       if (ok[j] && a.nullable) ok[j] = __ldg(a.col.valid + r) != 0;
       ok[j] = ok[j] && g[j] != kUnsetId;
+    }
+    if (W <= 4 && a.vrange) {
+#pragma unroll
+      for (int j = 0; j < kRows; ++j)
+        if (ok[j]) {
+          const uint32_t x = static_cast<uint32_t>(raw[j]) ^ a.vflip;
+          vlo              = min(vlo, x);
+          vhi              = max(vhi, x);
+        }
     }
 #pragma unroll
     for (int j = 0; j < kRows; ++j) {
@@ -700,6 +712,16 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
           if (a.states & ST_MAX) red_max(rec + a.off_mx * L, o);
         }
       }
+    }
+  }
+  if (W <= 4 && a.vrange) {
+    for (int o = 16; o > 0; o >>= 1) {
+      vlo = min(vlo, __shfl_xor_sync(0xffffffffu, vlo, o));
+      vhi = max(vhi, __shfl_xor_sync(0xffffffffu, vhi, o));
+    }
+    if ((threadIdx.x & 31) == 0 && vlo <= vhi) {
+      atomicMin(a.vrange, vlo);
+      atomicMax(a.vrange + 1, vhi);
     }
   }
   __syncthreads();
@@ -1657,10 +1679,19 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
              newid.get(), rec.get());
 
       // pass 2: one kernel per value column that needs valid counts / sums / min / max
+      // (a NUNIQUE column of <= 4-byte values also gets its value range here)
+      std::vector<Buffer<unsigned int>> vranges(p.ncols);
       for (int ci = 0; ci < p.ncols; ++ci) {
         ColPlan& c = p.c[ci];
         if (!c.nullable && !(c.states & (ST_SUM | ST_MIN | ST_MAX))) continue;
         ColArgs a{};
+        if ((c.states & ST_NDIST) && c.pair_packed) {
+          vranges[ci]                  = Buffer<unsigned int>(al, 2);
+          const unsigned int init[2]   = {0xffffffffu, 0u};
+          LDF_CUDA(cudaMemcpyAsync(vranges[ci].get(), init, 8, cudaMemcpyHostToDevice, s));
+          a.vrange = vranges[ci].get();
+          a.vflip  = (c.col.width == 4 && is_signed_int(c.col.type)) ? 0x80000000u : 0u;
+        }
         a.gid        = gid.get();
         a.newid      = newid.get();
         a.n          = n;
@@ -1704,13 +1735,16 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
                     static_cast<int>(std::min<int64_t>(std::min(hot_cap, 12 * 1024), nid)), p.overflow};
           // value bitmaps for the most frequent ranks when the value range is small
           na.flip = (c.col.width == 4 && is_signed_int(c.col.type)) ? 0x80000000u : 0u;
-          Buffer<unsigned int> vr(al, 2);
-          const unsigned int vr_init[2] = {0xffffffffu, 0u};
-          LDF_CUDA(cudaMemcpyAsync(vr.get(), vr_init, 8, cudaMemcpyHostToDevice, s));
-          {
+          Buffer<unsigned int> vr_own;
+          unsigned int* vr = vranges[ci].get();  // set by the column pass when the column had one
+          if (vr == nullptr) {
+            vr_own                        = Buffer<unsigned int>(al, 2);
+            vr                            = vr_own.get();
+            const unsigned int vr_init[2] = {0xffffffffu, 0u};
+            LDF_CUDA(cudaMemcpyAsync(vr, vr_init, 8, cudaMemcpyHostToDevice, s));
             auto vk = c.col.width == 1 ? value_range_kernel<1> : c.col.width == 2 ? value_range_kernel<2>
                                                                                    : value_range_kernel<4>;
-            launch("value_range", vk, static_cast<unsigned>(4 * num_sms()), 256, 0, s, c.col, n, na.flip, vr.get());
+            launch("value_range", vk, static_cast<unsigned>(4 * num_sms()), 256, 0, s, c.col, n, na.flip, vr);
           }
           // size tiers of the ranks (row counts are field 0 of the records)
           Buffer<int64_t> tb(al, kSegTiers);
@@ -1722,7 +1756,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
           }
           unsigned int hv[2];
           int64_t tier[kSegTiers];
-          LDF_CUDA(cudaMemcpyAsync(hv, vr.get(), 8, cudaMemcpyDeviceToHost, s));
+          LDF_CUDA(cudaMemcpyAsync(hv, vr, 8, cudaMemcpyDeviceToHost, s));
           LDF_CUDA(cudaMemcpyAsync(tier, tb.get(), sizeof(tier), cudaMemcpyDeviceToHost, s));
           ctx.finish();
           Buffer<uint32_t> bits;
