@@ -62,7 +62,13 @@ struct ColPlan {
   int nullable;     // the record has a valid-count word
   int fixed;        // float sum: 3 words of fixed point, else 1 word
   int pair_packed;  // (id << 32 | value32) pair keys
-  int off_vcount, off_sum, off_mn, off_mx, off_nd;  // word offsets in the record
+  // valid count / sum / min / max live in the column's own rank-major block
+  // (word k of rank g at crec[g * cw + k], so one row's updates share a
+  // cache line); the distinct count lives in the shared field-major record
+  int off_vcount, off_sum, off_mn, off_mx;  // word offsets in the column block
+  int off_nd;                               // field of the shared record
+  int cw;                                   // words per rank in the column block
+  unsigned long long* crec;
   // shared-memory hot records (byte offsets of typed arrays, [hot] entries)
   int sh_vcount, sh_sum, sh_mn, sh_mx, sh_nd;
   int sum_chunks;  // 32-bit chunks of a sum magnitude: 6 (float, 2^-96 LSB) or 2 (integers)
@@ -543,8 +549,9 @@ struct ColArgs {
   uint32_t states;
   int sum_chunks;  // 6 (float, fixed point) or 2 (integer magnitude)
   int off_vcount, off_sum, off_mn, off_mx;
-  unsigned long long* rec;  // group records, field-major: word w of group g at rec[w * ld + g]
+  unsigned long long* rec;  // the column block: word k of rank g at rec[g * cw + k * ld]
   uint64_t ld;
+  int cw;
   const uint32_t* newid;    // assign-pass id -> frequency rank
   double* fb;
   unsigned int* special;
@@ -682,7 +689,7 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
           }
         }
       } else {
-        unsigned long long* rec = a.rec + gg;
+        unsigned long long* rec = a.rec + static_cast<uint64_t>(gg) * a.cw;
         const uint64_t L        = a.ld;
         if (a.nullable) red_add(rec + a.off_vcount * L, 1);
         if (a.states & ST_SUM) {
@@ -726,7 +733,7 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
   }
   __syncthreads();
   for (int gg = threadIdx.x; gg < H; gg += blockDim.x) {
-    unsigned long long* rec = a.rec + gg;
+    unsigned long long* rec = a.rec + static_cast<uint64_t>(gg) * a.cw;
     const uint64_t L        = a.ld;
     if (a.nullable) {
       const uint32_t vc = reinterpret_cast<const uint32_t*>(smem + a.sh_vcount)[gg];
@@ -1368,8 +1375,9 @@ __global__ void finalize_kernel(FinArgs f)
         if (d.valid) d.valid[i] = 1;
         continue;
       }
-      const ColPlan& c  = p.c[o.col];
-      const uint64_t vc = c.nullable ? rec[c.off_vcount * L] : call;
+      const ColPlan& c               = p.c[o.col];
+      const unsigned long long* crec = c.crec + static_cast<uint64_t>(id) * c.cw;
+      const uint64_t vc              = c.nullable ? crec[c.off_vcount] : call;
       bool ok           = vc > 0;
       switch (o.kind) {
         case LDF_AGG_COUNT: {
@@ -1395,12 +1403,12 @@ __global__ void finalize_kernel(FinArgs f)
           if (c.fixed) {
             bool special;
             double sval;
-            double sv = float_sum(c, rec, L, id, special, sval);
+            double sv = float_sum(c, crec, 1, id, special, sval);
             if (special) sv = sval;
             if (o.kind == LDF_AGG_MEAN) sv = sv / static_cast<double>(vc);
             store_double(d, i, sv);
           } else {
-            const uint64_t s = rec[c.off_sum * L];
+            const uint64_t s = crec[c.off_sum];
             const double sd  = is_signed_int_dev(o.in_type) ? static_cast<double>(static_cast<int64_t>(s))
                                                             : static_cast<double>(s);
             if (o.kind == LDF_AGG_MEAN) store_double(d, i, sd / static_cast<double>(vc));
@@ -1415,7 +1423,7 @@ __global__ void finalize_kernel(FinArgs f)
             store_int(d, i, 0);
             break;
           }
-          const uint64_t o64 = o.kind == LDF_AGG_MIN ? ~rec[c.off_mn * L] : rec[c.off_mx * L];
+          const uint64_t o64 = o.kind == LDF_AGG_MIN ? ~crec[c.off_mn] : crec[c.off_mx];
           const uint64_t b   = unordered_bits(o.in_type, o64);
           if (d.type == o.in_type) {
             store_int(OCol{d.data, nullptr, LDF_UINT64, d.width}, i, b);
@@ -1547,18 +1555,20 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
   uint64_t pair_cap = static_cast<uint64_t>(std::max<int64_t>(est_pairs + est_pairs / 2, 64));
 
   // ---- record layout and shared-memory hot set -------------------------------
-  int w = 1;  // count_all
+  int w = 1;  // shared record: count_all, then the distinct counts
   for (int ci = 0; ci < p.ncols; ++ci) {
     ColPlan& c   = p.c[ci];
     c.sum_chunks = c.fixed ? kSumChunks : 2;
     c.mm64       = type_width(c.col.type) > 4 ? 1 : 0;
-    c.off_vcount = c.nullable ? w++ : 0;
+    int cw       = 0;  // the column block
+    c.off_vcount = c.nullable ? cw++ : 0;
     if (c.states & ST_SUM) {
-      c.off_sum = w;
-      w += c.fixed ? kSumChunks : 1;
+      c.off_sum = cw;
+      cw += c.fixed ? kSumChunks : 1;
     }
-    if (c.states & ST_MIN) c.off_mn = w++;
-    if (c.states & ST_MAX) c.off_mx = w++;
+    if (c.states & ST_MIN) c.off_mn = cw++;
+    if (c.states & ST_MAX) c.off_mx = cw++;
+    c.cw = cw;
     if (c.states & ST_NDIST) c.off_nd = w++;
   }
   p.stride = w;
@@ -1624,6 +1634,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     Buffer<int32_t> perm;
     Buffer<uint32_t> newid;
     Buffer<unsigned long long> rec;
+    std::vector<Buffer<unsigned long long>> col_blocks(p.ncols);
     uint64_t L  = 1;
     int64_t nid = 0;
     if (n > 0) {
@@ -1674,6 +1685,13 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
       L     = static_cast<uint64_t>(nid);
       rec   = Buffer<unsigned long long>(al, L * p.stride);
       LDF_CUDA(cudaMemsetAsync(rec.get(), 0, L * p.stride * 8, s));
+      for (int ci = 0; ci < p.ncols; ++ci) {
+        ColPlan& c = p.c[ci];
+        if (c.cw == 0) continue;
+        col_blocks[ci] = Buffer<unsigned long long>(al, L * c.cw);
+        LDF_CUDA(cudaMemsetAsync(col_blocks[ci].get(), 0, L * c.cw * 8, s));
+        c.crec = col_blocks[ci].get();
+      }
       launch("rank_scatter", rank_scatter_kernel, gs_blocks(nid, 256), 256, 0, s,
              static_cast<const int32_t*>(perm.get()), nid, static_cast<const unsigned long long*>(counts.get()),
              newid.get(), rec.get());
@@ -1703,8 +1721,9 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
         a.off_sum    = c.off_sum;
         a.off_mn     = c.off_mn;
         a.off_mx     = c.off_mx;
-        a.rec        = rec.get();
-        a.ld         = L;
+        a.rec        = c.crec;
+        a.ld         = 1;
+        a.cw         = c.cw;
         a.fb         = c.fb;
         a.special    = c.special;
         const int mmw = c.mm64 ? 8 : 4;
