@@ -1576,8 +1576,9 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
   LDF_CUDA(cudaFuncSetAttribute(assign_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
   int hot_limit = 1 << 30;
   if (const char* e = std::getenv("LDF_B200_GB_HOT")) hot_limit = std::max(0, std::atoi(e));
-  // bytes of NUNIQUE value bitmaps (kept well inside the 126 MB L2)
-  uint64_t bitmap_budget = 48ull << 20;
+  // bytes of NUNIQUE value bitmaps (mostly L2-resident; more bitmap ranks
+  // beat sending ranks of more than seg_tier(0) rows to the pair set)
+  uint64_t bitmap_budget = 96ull << 20;
   if (const char* e = std::getenv("LDF_B200_ND_BITMAP_MB")) bitmap_budget = std::max(0ll, std::atoll(e)) << 20;
   // per-rank segments for the less frequent ranks (LDF_B200_ND_SEGMENTS=0 keeps them in the pair set)
   bool seg_enabled = true;

@@ -209,7 +209,7 @@ def test_groupby_nunique_size_tiers(segments, vtype, monkeypatch):
     # bitmaps), the all-ones bit pattern as a value, and null values
     monkeypatch.setenv("LDF_B200_ND_SEGMENTS", segments)
     rng = np.random.default_rng(77)
-    sizes = ([20000, 9000, 8193, 8192, 5000, 513, 512, 511, 300, 17, 16, 15, 10, 2, 1]
+    sizes = ([40000, 16385, 16384, 9000, 8193, 8192, 5000, 513, 512, 511, 300, 17, 16, 15, 10, 2, 1]
              + [1] * 2000 + [3] * 1000 + [40] * 500 + [700] * 40)
     keys = np.repeat(np.arange(len(sizes), dtype=np.int64) * 7 + 3, sizes)
     vals = np.empty(len(keys), dtype=np.int64)
