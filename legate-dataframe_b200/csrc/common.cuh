@@ -342,11 +342,14 @@ __device__ __forceinline__ uint64_t hash_words(const uint64_t w[4], int64_t n)
   return mix64(h);
 }
 
+// Hash of a null value.
+constexpr uint64_t kNullValueHash = 0x5bd1e9955bd1e995ull;
+
 // Hash of one column value of a row, null-aware.  A null hashes to a fixed
 // constant.
 __device__ __forceinline__ uint64_t hash_value(const DCol& c, int64_t r)
 {
-  if (!dvalid(c, r)) return 0x5bd1e9955bd1e995ull;
+  if (!dvalid(c, r)) return kNullValueHash;
   if (c.type == LDF_STRING) {
     const uint8_t* p = dstr_ptr(c, r);
     const int64_t n  = dstr_len(c, r);

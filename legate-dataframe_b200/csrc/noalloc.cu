@@ -28,7 +28,7 @@ void onesweep_gather_pass_raw(cudaStream_t s, const RadixPass& p, int64_t n, int
 namespace {
 
 constexpr int64_t kMaxRows = LDF_B200_NOALLOC_MAX_ROWS;
-constexpr int64_t kTileRows = 2048;  // rows per onesweep tile (radix.cu)
+constexpr int64_t kTileRows = ldf::kRadixTile;  // rows per onesweep tile
 
 // Scratch layout (bytes): row permutation, look-back status words, bucket
 // histogram, digit bases, error word.

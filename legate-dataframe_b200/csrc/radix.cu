@@ -10,9 +10,9 @@
 namespace ldf {
 namespace {
 
-constexpr int RT    = 256;
-constexpr int RI    = 8;
-constexpr int RTILE = RT * RI;
+constexpr int RT    = kRadixThreads;
+constexpr int RI    = kRadixItems;
+constexpr int RTILE = kRadixTile;
 constexpr int RW    = RT / 32;
 
 __device__ __forceinline__ uint64_t sort_word(const SortKeyDesc& k, int64_t row)
@@ -69,9 +69,7 @@ __device__ __forceinline__ uint32_t class_digit(const SortKeyDesc& k, int64_t ro
 
 __device__ __forceinline__ uint64_t bucket_word(const RadixPass& p, int64_t row)
 {
-  uint64_t h = 0x243f6a8885a308d3ull;
-  for (int j = 0; j < p.hash_keys.n; ++j) h = hash_combine64(h, hash_value(p.hash_keys.c[j], row));
-  return h % p.nparts;
+  return key_bits<KeyMode::GEN>(p.hash_keys, row) % p.nparts;
 }
 
 __device__ __forceinline__ uint64_t pass_word(const RadixPass& p, int64_t row)
@@ -129,11 +127,13 @@ __global__ void __launch_bounds__(RT) onesweep_kernel(PassArgs a)
   __shared__ uint32_t s_whist[RW][256];
   __shared__ uint32_t s_tile_start[256];
   __shared__ uint64_t s_gbase[256];
-  __shared__ uint64_t s_keys[WRITE_KEYS ? RTILE : 1];
-  __shared__ int32_t s_vals[RTILE];
-  __shared__ uint8_t s_dig[RTILE];
   __shared__ uint32_t s_scan[RW + 1];
   __shared__ int64_t s_tile;
+  // staged tile (dynamic): [keys u64 x RTILE when carried][rows i32 x RTILE][digits u8 x RTILE]
+  extern __shared__ __align__(16) unsigned char s_stage[];
+  uint64_t* s_keys = reinterpret_cast<uint64_t*>(s_stage);
+  int32_t* s_vals  = reinterpret_cast<int32_t*>(s_stage + (WRITE_KEYS ? RTILE * sizeof(uint64_t) : 0));
+  uint8_t* s_dig   = reinterpret_cast<uint8_t*>(s_vals + RTILE);
 
   const int64_t tile = next_tile_id(a.counter, &s_tile);
   for (int i = threadIdx.x; i < RW * 256; i += RT) (&s_whist[0][0])[i] = 0;
@@ -240,6 +240,20 @@ __global__ void __launch_bounds__(RT) onesweep_kernel(PassArgs a)
     if (WRITE_KEYS) a.keys_out[pos] = s_keys[j];
     a.vals_out[pos] = s_vals[j];
   }
+}
+
+constexpr size_t onesweep_smem(bool write_keys)
+{
+  return (write_keys ? RTILE * sizeof(uint64_t) : 0) + RTILE * (sizeof(int32_t) + 1);
+}
+
+template <bool GATHER, bool WRITE_KEYS>
+void launch_onesweep(cudaStream_t s, unsigned tiles, const PassArgs& a)
+{
+  constexpr size_t smem = onesweep_smem(WRITE_KEYS);
+  LDF_CUDA(cudaFuncSetAttribute(onesweep_kernel<GATHER, WRITE_KEYS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  launch("onesweep", onesweep_kernel<GATHER, WRITE_KEYS>, tiles, RT, smem, s, a);
 }
 
 __global__ void iota_kernel(int32_t* p, int64_t n)
@@ -350,10 +364,10 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
     a.counter    = reinterpret_cast<unsigned long long*>(status.get() + tiles * 256);
     a.err        = ctx.err();
     const unsigned g = static_cast<unsigned>(tiles);
-    if (gather && write_keys) launch("onesweep", onesweep_kernel<true, true>, g, RT, 0, s, a);
-    else if (gather) launch("onesweep", onesweep_kernel<true, false>, g, RT, 0, s, a);
-    else if (write_keys) launch("onesweep", onesweep_kernel<false, true>, g, RT, 0, s, a);
-    else launch("onesweep", onesweep_kernel<false, false>, g, RT, 0, s, a);
+    if (gather && write_keys) launch_onesweep<true, true>(s, g, a);
+    else if (gather) launch_onesweep<true, false>(s, g, a);
+    else if (write_keys) launch_onesweep<false, true>(s, g, a);
+    else launch_onesweep<false, false>(s, g, a);
     LDF_CHECK_LAUNCH();
     vin = vbuf[k % 2];
     kin = keys[k % 2].get();
@@ -395,7 +409,7 @@ void onesweep_gather_pass_raw(cudaStream_t s, const RadixPass& p, int64_t n, int
   a.status     = status;
   a.counter    = reinterpret_cast<unsigned long long*>(status + tiles * 256);
   a.err        = err;
-  launch("onesweep", onesweep_kernel<true, false>, static_cast<unsigned>(tiles), RT, 0, s, a);
+  launch_onesweep<true, false>(s, static_cast<unsigned>(tiles), a);
 }
 
 }  // namespace ldf

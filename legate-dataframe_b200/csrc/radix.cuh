@@ -6,6 +6,11 @@
 
 namespace ldf {
 
+// Rows per onesweep tile (threads x items per thread).
+constexpr int kRadixThreads = 256;
+constexpr int kRadixItems   = 12;
+constexpr int kRadixTile    = kRadixThreads * kRadixItems;
+
 // How a pass obtains the digit of a row.
 enum class DigitSrc : int {
   CARRIED = 0,  // byte `shift/8` of the carried key word

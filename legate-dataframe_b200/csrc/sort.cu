@@ -237,12 +237,19 @@ void string_ranks(const OpContext& ctx, const DCol& col, int64_t n, uint32_t* ou
 void gather_table(const OpContext& ctx, const ldf_column* table, int ncols, const int32_t* map, int64_t rows,
                   ldf_column* out)
 {
+  std::vector<DCol> fsrc;
+  std::vector<ldf_column*> fdst;
   for (int j = 0; j < ncols; ++j) {
     const ldf_column& c = table[j];
     out[j]              = alloc_out_column(ctx.alloc(), c.type, rows, c.valid != nullptr);
-    if (c.type == LDF_STRING) gather_strings(ctx, make_dcol(c), map, rows, out[j]);
-    else gather_fixed(ctx, make_dcol(c), map, rows, out[j]);
+    if (c.type == LDF_STRING) {
+      gather_strings(ctx, make_dcol(c), map, rows, out[j]);
+    } else {
+      fsrc.push_back(make_dcol(c));
+      fdst.push_back(&out[j]);
+    }
   }
+  gather_fixed_columns(ctx, fsrc.data(), map, rows, fdst.data(), static_cast<int>(fsrc.size()));
 }
 
 void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const uint8_t* ascending, int nkeys,
@@ -305,9 +312,7 @@ __global__ void bucket_count_kernel(KeyCols k, int64_t n, uint32_t nparts, unsig
     for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) sc[i] = 0;
   __syncthreads();
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t h = 0x243f6a8885a308d3ull;
-    for (int j = 0; j < k.n; ++j) h = hash_combine64(h, hash_value(k.c[j], r));
-    uint32_t b = static_cast<uint32_t>(h % nparts);
+    const uint32_t b = static_cast<uint32_t>(key_bits<KeyMode::GEN>(k, r) % nparts);
     if (use_smem) atomicAdd(&sc[b], 1u);
     else atomicAdd(&counts[b], 1ull);
   }

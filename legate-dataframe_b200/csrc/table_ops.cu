@@ -49,12 +49,39 @@ void free_out_column(const Allocator& a, ldf_column& c)
 
 namespace {
 
-__global__ void string_lengths_kernel(DCol src, const int32_t* map, int64_t rows, int64_t* lens)
+// Output length and source chars offset of each gathered string: srcoff[i] =
+// offset of the row's first char in src.chars (0 for an empty string), -1
+// for a null row.  The copy kernel then reads these sequentially instead of
+// gathering the ranges a second time.  Four rows per thread, loads in flight
+// together.
+constexpr int kLenRows = 4;
+__global__ void __launch_bounds__(256) string_lengths_kernel(DCol src, const int32_t* map, int64_t rows,
+                                                             int64_t* lens, int64_t* srcoff)
 {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = map ? map[i] : i;
-    lens[i]   = (r >= 0 && dvalid(src, r)) ? dstr_len(src, r) : 0;
+  const ldf_range* rg    = static_cast<const ldf_range*>(src.data);
+  const int64_t per_iter = static_cast<int64_t>(blockDim.x) * kLenRows;
+  for (int64_t base = blockIdx.x * per_iter; base < rows; base += static_cast<int64_t>(gridDim.x) * per_iter) {
+    int64_t r[kLenRows];
+#pragma unroll
+    for (int j = 0; j < kLenRows; ++j) {
+      const int64_t i = base + j * blockDim.x + threadIdx.x;
+      r[j]            = i < rows ? (map ? static_cast<int64_t>(__ldg(map + i)) : i) : -2;
+    }
+    ldf_range g[kLenRows];
+    bool ok[kLenRows];
+#pragma unroll
+    for (int j = 0; j < kLenRows; ++j) {
+      ok[j] = r[j] >= 0 && dvalid(src, r[j]);
+      g[j]  = r[j] >= 0 ? rg[r[j]] : ldf_range{0, -1};
+    }
+#pragma unroll
+    for (int j = 0; j < kLenRows; ++j) {
+      if (r[j] == -2) continue;
+      const int64_t i = base + j * blockDim.x + threadIdx.x;
+      const int64_t n = ok[j] ? g[j].hi - g[j].lo + 1 : 0;
+      lens[i]         = n;
+      srcoff[i]       = ok[j] ? (n > 0 ? g[j].lo - src.chars_base : 0) : -1;
+    }
   }
 }
 
@@ -72,42 +99,38 @@ constexpr int kStrRows  = 2;
 constexpr int kStrWords = 4;
 constexpr int kStrStage = 16 * 1024;
 
-__global__ void __launch_bounds__(kStrTile) string_copy_kernel(DCol src, const int32_t* map, int64_t rows,
+__global__ void __launch_bounds__(kStrTile) string_copy_kernel(DCol src, const int64_t* srcoff, int64_t rows,
                                                                const int64_t* offs, int64_t nchars,
                                                                ldf_range* dst_ranges, uint8_t* dst_valid,
                                                                uint8_t* dst_chars)
 {
   __shared__ __align__(16) uint8_t stage[kStrStage + 16];
-  const ldf_range* rg_src = static_cast<const ldf_range*>(src.data);
   const uintptr_t cbeg    = reinterpret_cast<uintptr_t>(src.chars);
   const uintptr_t cend    = cbeg + static_cast<uintptr_t>(src.num_chars);
   const int64_t per_tile  = static_cast<int64_t>(kStrTile) * kStrRows;
   for (int64_t tile = blockIdx.x; tile * per_tile < rows; tile += gridDim.x) {
     const int64_t i0 = tile * per_tile;
-    int64_t r[kStrRows], o[kStrRows], n[kStrRows];
+    int64_t so[kStrRows], o[kStrRows], n[kStrRows];
     const uint8_t* p[kStrRows];
 #pragma unroll
     for (int j = 0; j < kStrRows; ++j) {
       const int64_t i = i0 + j * kStrTile + threadIdx.x;
-      r[j]            = -2;
-      if (i < rows) r[j] = map ? __ldg(map + i) : i;
+      so[j] = -2;
+      n[j]  = 0;
+      o[j]  = 0;
+      if (i < rows) {
+        so[j] = __ldg(srcoff + i);
+        o[j]  = __ldg(offs + i);
+        n[j]  = (i + 1 < rows ? __ldg(offs + i + 1) : nchars) - o[j];
+      }
     }
 #pragma unroll
     for (int j = 0; j < kStrRows; ++j) {
       const int64_t i = i0 + j * kStrTile + threadIdx.x;
-      n[j] = 0;
-      o[j] = 0;
-      p[j] = nullptr;
-      if (r[j] == -2) continue;
-      o[j]          = offs[i];
-      const bool ok = r[j] >= 0 && dvalid(src, r[j]);
-      if (ok) {
-        const ldf_range rg = rg_src[r[j]];
-        n[j]               = rg.hi - rg.lo + 1;
-        p[j]               = reinterpret_cast<const uint8_t*>(src.chars) + (rg.lo - src.chars_base);
-      }
+      p[j]            = so[j] >= 0 ? reinterpret_cast<const uint8_t*>(src.chars) + so[j] : nullptr;
+      if (so[j] == -2) continue;
       dst_ranges[i] = ldf_range{o[j], o[j] + n[j] - 1};
-      if (dst_valid) dst_valid[i] = ok ? 1 : 0;
+      if (dst_valid) dst_valid[i] = so[j] >= 0 ? 1 : 0;
     }
     // the strings' words (all loads of the thread in flight together)
     unsigned long long w[kStrRows][kStrWords];
@@ -173,18 +196,72 @@ __global__ void __launch_bounds__(kStrTile) string_copy_kernel(DCol src, const i
   }
 }
 
-__global__ void gather_fixed_kernel(DCol src, const int32_t* map, int64_t rows, void* dst,
-                                    uint8_t* dst_valid)
+// Gather of up to kGatherCols fixed-width columns through one index map
+// (map[i] < 0 -> null).  Each thread owns kGatherRows rows (strided by the
+// block, so map reads and output writes stay coalesced) and keeps all their
+// source loads of one column in flight together.
+constexpr int kGatherCols = 8;
+constexpr int kGatherRows = 8;
+struct GatherSet {
+  int ncols;
+  int width[kGatherCols];
+  const void* src[kGatherCols];
+  const uint8_t* valid[kGatherCols];
+  void* dst[kGatherCols];
+  uint8_t* dst_valid[kGatherCols];
+};
+
+template <typename T>
+__device__ __forceinline__ void gather_one(const T* src, const uint8_t* valid, T* dst, uint8_t* dst_valid,
+                                           const int64_t (&i)[kGatherRows], const int32_t (&r)[kGatherRows],
+                                           int64_t rows)
 {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = map[i];
-    if (r >= 0) {
-      copy_fixed(dst, i, src.data, r, src.width);
-      if (dst_valid) dst_valid[i] = dvalid(src, r) ? 1 : 0;
-    } else {
-      zero_fixed(dst, i, src.width);
-      if (dst_valid) dst_valid[i] = 0;
+  T v[kGatherRows];
+  uint8_t ok[kGatherRows];
+#pragma unroll
+  for (int j = 0; j < kGatherRows; ++j) {
+    v[j]  = r[j] >= 0 ? __ldg(src + r[j]) : T(0);
+    ok[j] = r[j] >= 0 ? 1 : 0;
+    if (valid != nullptr && r[j] >= 0) ok[j] = __ldg(valid + r[j]) != 0 ? 1 : 0;
+  }
+#pragma unroll
+  for (int j = 0; j < kGatherRows; ++j) {
+    if (i[j] >= rows) continue;
+    dst[i[j]] = v[j];
+    if (dst_valid) dst_valid[i[j]] = ok[j];
+  }
+}
+
+__global__ void __launch_bounds__(256) gather_fixed_kernel(GatherSet g, const int32_t* map, int64_t rows)
+{
+  const int64_t per_iter = static_cast<int64_t>(blockDim.x) * kGatherRows;
+  for (int64_t base = blockIdx.x * per_iter; base < rows; base += static_cast<int64_t>(gridDim.x) * per_iter) {
+    int64_t i[kGatherRows];
+    int32_t r[kGatherRows];
+#pragma unroll
+    for (int j = 0; j < kGatherRows; ++j) {
+      i[j] = base + j * blockDim.x + threadIdx.x;
+      r[j] = i[j] < rows ? __ldg(map + i[j]) : -1;
+    }
+    for (int c = 0; c < g.ncols; ++c) {
+      switch (g.width[c]) {
+        case 1:
+          gather_one(static_cast<const uint8_t*>(g.src[c]), g.valid[c], static_cast<uint8_t*>(g.dst[c]),
+                     g.dst_valid[c], i, r, rows);
+          break;
+        case 2:
+          gather_one(static_cast<const uint16_t*>(g.src[c]), g.valid[c], static_cast<uint16_t*>(g.dst[c]),
+                     g.dst_valid[c], i, r, rows);
+          break;
+        case 4:
+          gather_one(static_cast<const uint32_t*>(g.src[c]), g.valid[c], static_cast<uint32_t*>(g.dst[c]),
+                     g.dst_valid[c], i, r, rows);
+          break;
+        default:
+          gather_one(static_cast<const unsigned long long*>(g.src[c]), g.valid[c],
+                     static_cast<unsigned long long*>(g.dst[c]), g.dst_valid[c], i, r, rows);
+          break;
+      }
     }
   }
 }
@@ -210,28 +287,50 @@ void gather_strings(const OpContext& ctx, const DCol& src, const int32_t* map, i
   }
   Buffer<int64_t> lens(a, rows);
   Buffer<int64_t> offs(a, rows);
+  Buffer<int64_t> srcoff(a, rows);
   Buffer<int64_t> total(a, 1);
-  launch("string_lengths", string_lengths_kernel, grid_for(rows, 256), 256, 0, s, src, map, rows, lens.get());
+  launch("string_lengths", string_lengths_kernel, grid_for(ceil_div(rows, kLenRows), 256), 256, 0, s, src, map, rows,
+         lens.get(), srcoff.get());
   LDF_CHECK_LAUNCH();
   exclusive_scan_i64(lens.get(), offs.get(), rows, total.get(), ctx);
   int64_t nchars = ctx.read_i64(total.get());
   dst.chars      = static_cast<char*>(a.allocate(static_cast<size_t>(nchars)));
   dst.num_chars  = nchars;
   dst.chars_base = 0;
-  launch("string_copy", string_copy_kernel, grid_for(ceil_div(rows, kStrRows), kStrTile), kStrTile, 0, s, src, map,
-         rows,
+  launch("string_copy", string_copy_kernel, grid_for(ceil_div(rows, kStrRows), kStrTile), kStrTile, 0, s, src,
+         static_cast<const int64_t*>(srcoff.get()), rows,
          static_cast<const int64_t*>(offs.get()), nchars, static_cast<ldf_range*>(dst.data), dst.valid,
          reinterpret_cast<uint8_t*>(dst.chars));
   LDF_CHECK_LAUNCH();
 }
 
+void gather_fixed_columns(const OpContext& ctx, const DCol* src, const int32_t* map, int64_t rows,
+                          ldf_column* const* dst, int ncols)
+{
+  if (rows == 0) return;
+  for (int c0 = 0; c0 < ncols; c0 += kGatherCols) {
+    GatherSet g{};
+    g.ncols = ncols - c0 < kGatherCols ? ncols - c0 : kGatherCols;
+    for (int k = 0; k < g.ncols; ++k) {
+      const DCol& sc = src[c0 + k];
+      LDF_REQUIRE(sc.width == 1 || sc.width == 2 || sc.width == 4 || sc.width == 8,
+                  "gather: unsupported fixed width");
+      g.width[k]     = sc.width;
+      g.src[k]       = sc.data;
+      g.valid[k]     = sc.valid;
+      g.dst[k]       = dst[c0 + k]->data;
+      g.dst_valid[k] = dst[c0 + k]->valid;
+    }
+    launch("gather_fixed", gather_fixed_kernel, grid_for(ceil_div(rows, kGatherRows), 256), 256, 0, ctx.stream(), g,
+           map, rows);
+  }
+}
+
 void gather_fixed(const OpContext& ctx, const DCol& src, const int32_t* map, int64_t rows,
                   ldf_column& dst)
 {
-  if (rows == 0) return;
-  launch("gather_fixed", gather_fixed_kernel, grid_for(rows, 256), 256, 0, ctx.stream(), src, map, rows, dst.data,
-                                                                      dst.valid);
-  LDF_CHECK_LAUNCH();
+  ldf_column* d = &dst;
+  gather_fixed_columns(ctx, &src, map, rows, &d, 1);
 }
 
 }  // namespace ldf

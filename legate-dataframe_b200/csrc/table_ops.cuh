@@ -32,12 +32,15 @@ KeyCols make_keys(const ldf_column* cols, int ncols, const int32_t* idx, int nke
 // -> GEN (64-bit row hash + column-wise equality).
 KeyMode key_mode(const KeyCols& k);
 
+// Seed of the row hash of a key set.
+constexpr uint64_t kKeyHashSeed = 0x243f6a8885a308d3ull;
+
 // Key bits / row hash for each mode.
 template <KeyMode M>
 __device__ __forceinline__ uint64_t key_bits(const KeyCols& k, int64_t r)
 {
   if constexpr (M == KeyMode::GEN) {
-    uint64_t h = 0x243f6a8885a308d3ull;
+    uint64_t h = kKeyHashSeed;
     for (int j = 0; j < k.n; ++j) h = hash_combine64(h, hash_value(k.c[j], r));
     return h;
   } else {
@@ -89,5 +92,10 @@ void gather_strings(const OpContext& ctx, const DCol& src, const int32_t* map, i
 // Gather a fixed-width column by index map (map[i] < 0 -> null).
 void gather_fixed(const OpContext& ctx, const DCol& src, const int32_t* map, int64_t rows,
                   ldf_column& dst);
+
+// The same for several fixed-width columns through one map (one launch per
+// eight columns).
+void gather_fixed_columns(const OpContext& ctx, const DCol* src, const int32_t* map, int64_t rows,
+                          ldf_column* const* dst, int ncols);
 
 }  // namespace ldf
