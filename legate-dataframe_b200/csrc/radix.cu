@@ -15,19 +15,20 @@ constexpr int RI    = kRadixItems;
 constexpr int RTILE = kRadixTile;
 constexpr int RW    = RT / 32;
 
-__device__ __forceinline__ uint64_t sort_word(const SortKeyDesc& k, int64_t row)
+// Order-preserving word of a sort key from the value's raw bits (zero for a
+// null or a NaN: those rows are placed by the CLASS pass).
+__device__ __forceinline__ uint64_t sort_word_of(const SortKeyDesc& k, uint64_t raw, bool valid)
 {
-  const DCol& c = k.col;
-  if (!dvalid(c, row)) return 0;
+  if (!valid) return 0;
   uint64_t o;
-  switch (c.type) {
-    case LDF_INT8: o = static_cast<uint8_t>(static_cast<const int8_t*>(c.data)[row]) ^ 0x80u; break;
-    case LDF_INT16: o = static_cast<uint16_t>(static_cast<const int16_t*>(c.data)[row]) ^ 0x8000u; break;
-    case LDF_INT32: o = static_cast<uint32_t>(static_cast<const int32_t*>(c.data)[row]) ^ 0x80000000u; break;
+  switch (k.col.type) {
+    case LDF_INT8: o = (raw & 0xffu) ^ 0x80u; break;
+    case LDF_INT16: o = (raw & 0xffffu) ^ 0x8000u; break;
+    case LDF_INT32: o = (raw & 0xffffffffu) ^ 0x80000000u; break;
     case LDF_INT64:
-    case LDF_TIMESTAMP_US: o = static_cast<uint64_t>(static_cast<const int64_t*>(c.data)[row]) ^ (1ull << 63); break;
+    case LDF_TIMESTAMP_US: o = raw ^ (1ull << 63); break;
     case LDF_FLOAT32: {
-      uint32_t b = static_cast<const uint32_t*>(c.data)[row];
+      uint32_t b = static_cast<uint32_t>(raw);
       if ((b & 0x7f800000u) == 0x7f800000u && (b & 0x007fffffu)) return 0;  // NaN: CLASS pass
       if ((b & 0x7fffffffu) == 0) b = 0;                                    // -0.0 == 0.0
       o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
@@ -35,19 +36,24 @@ __device__ __forceinline__ uint64_t sort_word(const SortKeyDesc& k, int64_t row)
       break;
     }
     case LDF_FLOAT64: {
-      uint64_t b = static_cast<const uint64_t*>(c.data)[row];
+      uint64_t b = raw;
       if ((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull && (b & 0x000fffffffffffffull)) return 0;
       if ((b & 0x7fffffffffffffffull) == 0) b = 0;
       o = (b & (1ull << 63)) ? ~b : (b | (1ull << 63));
       break;
     }
-    default: o = dbits(c, row); break;  // unsigned, bool, string ranks (uint32)
+    default: o = raw; break;  // unsigned, bool, string ranks (uint32)
   }
   if (k.descending) {
     const uint64_t mask = k.key_bytes >= 8 ? ~0ull : ((1ull << (8 * k.key_bytes)) - 1);
     o                   = ~o & mask;
   }
   return o;
+}
+
+__device__ __forceinline__ uint64_t sort_word(const SortKeyDesc& k, int64_t row)
+{
+  return sort_word_of(k, dbits(k.col, row), dvalid(k.col, row));
 }
 
 // 0 = value, 1 = NaN, 2 = null when nulls_at_end; reversed otherwise
@@ -87,18 +93,78 @@ __device__ __forceinline__ uint32_t pass_digit_of_row(const RadixPass& p, int64_
 constexpr int kHistPassesPerLaunch = 16;
 struct HistArgs {
   int npasses;
+  uint32_t reuse;  // bit q: pass q reads the same key word as pass q - 1
   RadixPass p[kHistPassesPerLaunch];
   int64_t n;
   uint32_t* hist;  // [npasses][256]
 };
 
+// Raw bits of kHR rows of a column of width W, all loads in flight together.
+constexpr int kHR = 4;
+template <int W>
+__device__ __forceinline__ void load_raw_rows(const DCol& c, const int64_t (&r)[kHR], int64_t n, uint64_t (&raw)[kHR],
+                                              bool (&ok)[kHR])
+{
+#pragma unroll
+  for (int j = 0; j < kHR; ++j) {
+    raw[j] = 0;
+    ok[j]  = false;
+    if (r[j] >= n) continue;
+    if (W == 1) raw[j] = __ldg(static_cast<const uint8_t*>(c.data) + r[j]);
+    else if (W == 2) raw[j] = __ldg(static_cast<const uint16_t*>(c.data) + r[j]);
+    else if (W == 4) raw[j] = __ldg(static_cast<const uint32_t*>(c.data) + r[j]);
+    else raw[j] = __ldg(static_cast<const unsigned long long*>(c.data) + r[j]);
+    ok[j] = c.valid == nullptr || __ldg(c.valid + r[j]) != 0;
+  }
+}
+
+// All digit histograms of up to kHistPassesPerLaunch passes in one read of the
+// columns: kHR rows per thread, each key word loaded once for all the passes
+// over it (their loads in flight together), shared-memory counts.
 __global__ void __launch_bounds__(RT) histogram_kernel(HistArgs a)
 {
   __shared__ uint32_t sh[kHistPassesPerLaunch * 256];
   for (int i = threadIdx.x; i < a.npasses * 256; i += RT) sh[i] = 0;
   __syncthreads();
-  for (int64_t r = blockIdx.x * (int64_t)RT + threadIdx.x; r < a.n; r += (int64_t)gridDim.x * RT) {
-    for (int q = 0; q < a.npasses; ++q) atomicAdd(&sh[q * 256 + pass_digit_of_row(a.p[q], r)], 1u);
+  const int64_t per_iter = static_cast<int64_t>(RT) * kHR;
+  for (int64_t base = blockIdx.x * per_iter; base < a.n; base += static_cast<int64_t>(gridDim.x) * per_iter) {
+    int64_t r[kHR];
+#pragma unroll
+    for (int j = 0; j < kHR; ++j) r[j] = base + j * RT + threadIdx.x;
+    uint64_t w[kHR];
+#pragma unroll
+    for (int j = 0; j < kHR; ++j) w[j] = 0;
+    for (int q = 0; q < a.npasses; ++q) {
+      const RadixPass& p = a.p[q];
+      uint32_t d[kHR];
+      if (p.src == DigitSrc::CLASS) {
+#pragma unroll
+        for (int j = 0; j < kHR; ++j) d[j] = r[j] < a.n ? class_digit(p.key, r[j]) : 256u;
+      } else {
+        if (!((a.reuse >> q) & 1u)) {
+          if (p.src == DigitSrc::BUCKET) {
+#pragma unroll
+            for (int j = 0; j < kHR; ++j) w[j] = r[j] < a.n ? bucket_word(p, r[j]) : 0;
+          } else {
+            uint64_t raw[kHR];
+            bool ok[kHR];
+            switch (p.key.col.width) {
+              case 1: load_raw_rows<1>(p.key.col, r, a.n, raw, ok); break;
+              case 2: load_raw_rows<2>(p.key.col, r, a.n, raw, ok); break;
+              case 4: load_raw_rows<4>(p.key.col, r, a.n, raw, ok); break;
+              default: load_raw_rows<8>(p.key.col, r, a.n, raw, ok); break;
+            }
+#pragma unroll
+            for (int j = 0; j < kHR; ++j) w[j] = sort_word_of(p.key, raw[j], ok[j]);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < kHR; ++j) d[j] = r[j] < a.n ? static_cast<uint32_t>(w[j] >> p.shift) & 0xffu : 256u;
+      }
+#pragma unroll
+      for (int j = 0; j < kHR; ++j)
+        if (d[j] < 256) atomicAdd(&sh[q * 256 + d[j]], 1u);
+    }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < a.npasses * 256; i += RT)
@@ -122,7 +188,7 @@ struct PassArgs {
 // word); otherwise it is the carried key.  WRITE_KEYS: later passes of the same
 // word follow, so carry the word along.
 template <bool GATHER, bool WRITE_KEYS>
-__global__ void __launch_bounds__(RT) onesweep_kernel(PassArgs a)
+__global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs a)
 {
   __shared__ uint32_t s_whist[RW][256];
   __shared__ uint32_t s_tile_start[256];
@@ -144,29 +210,28 @@ __global__ void __launch_bounds__(RT) onesweep_kernel(PassArgs a)
   const int64_t tbase    = tile * RTILE;
   uint64_t key[RI];
   int32_t val[RI];
-  uint32_t dig[RI];
-  uint32_t lrank[RI];
+  uint32_t dr[RI];  // digit (bits 0-8, 256 = no row), then rank among the tile's rows of that digit << 9
 #pragma unroll
   for (int i = 0; i < RI; ++i) {
     const int64_t idx = tbase + warp * (32 * RI) + i * 32 + lane;
     key[i]            = 0;
     val[i]            = 0;
-    dig[i]            = 256;
+    dr[i]             = 256;
     if (idx < a.n) {
       const int64_t row = a.vals_in ? a.vals_in[idx] : idx;
       val[i]            = static_cast<int32_t>(row);
       if (a.p.src == DigitSrc::CLASS) {
-        dig[i] = class_digit(a.p.key, row);
+        dr[i] = class_digit(a.p.key, row);
       } else {
         key[i] = GATHER ? pass_word(a.p, row) : a.keys_in[idx];
-        dig[i] = static_cast<uint32_t>(key[i] >> a.p.shift) & 0xffu;
+        dr[i]  = static_cast<uint32_t>(key[i] >> a.p.shift) & 0xffu;
       }
     }
   }
   // stable warp-level ranking, items in (i, lane) order
 #pragma unroll
   for (int i = 0; i < RI; ++i) {
-    const uint32_t d     = dig[i];
+    const uint32_t d     = dr[i];
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const uint32_t rank  = __popc(peers & lt_mask);
     uint32_t base        = 0;
@@ -174,7 +239,7 @@ __global__ void __launch_bounds__(RT) onesweep_kernel(PassArgs a)
     __syncwarp();
     if (d < 256 && rank == 0) s_whist[warp][d] = base + __popc(peers);
     __syncwarp();
-    lrank[i] = base + rank;
+    dr[i] = d | ((base + rank) << 9);
   }
   __syncthreads();
   // per-digit warp prefixes and tile counts (thread t owns digit t)
@@ -189,17 +254,28 @@ __global__ void __launch_bounds__(RT) onesweep_kernel(PassArgs a)
   uint32_t tile_total;
   const uint32_t start = block_exclusive_scan<uint32_t, RT>(run, s_scan, &tile_total);
   s_tile_start[t]      = start;
+  // publish this tile's digit counts before anything else, so the tiles
+  // after it can finish their look-back while this one stages its rows
+  uint64_t* st = a.status;
+  if (tile == 0) st_release_u64(&st[t], kFlagPrefix | run);
+  else st_release_u64(&st[tile * 256 + t], kFlagAgg | run);
+  __syncthreads();
+  // stage the tile in digit order (tile-local positions need no look-back)
+#pragma unroll
+  for (int i = 0; i < RI; ++i) {
+    const uint32_t d = dr[i] & 0x1ffu;
+    if (d < 256) {
+      const uint32_t lp = s_tile_start[d] + s_whist[warp][d] + (dr[i] >> 9);
+      if (WRITE_KEYS) s_keys[lp] = key[i];
+      s_vals[lp] = val[i];
+      s_dig[lp]  = static_cast<uint8_t>(d);
+    }
+  }
   // per-digit decoupled look-back
   {
-    uint64_t* st = a.status;
-    uint64_t excl;
-    if (tile == 0) {
-      st_release_u64(&st[t], kFlagPrefix | run);
-      excl = 0;
-    } else {
-      st_release_u64(&st[tile * 256 + t], kFlagAgg | run);
-      excl          = 0;
-      int64_t j     = tile - 1;
+    uint64_t excl = 0;
+    if (tile > 0) {
+      int64_t j      = tile - 1;
       uint32_t spins = 0;
       while (j >= 0) {
         uint64_t s = ld_volatile_u64(&st[j * 256 + t]);
@@ -219,18 +295,6 @@ __global__ void __launch_bounds__(RT) onesweep_kernel(PassArgs a)
       st_release_u64(&st[tile * 256 + t], kFlagPrefix | (excl + run));
     }
     s_gbase[t] = a.digit_base[t] + excl;
-  }
-  __syncthreads();
-  // stage the tile in digit order
-#pragma unroll
-  for (int i = 0; i < RI; ++i) {
-    const uint32_t d = dig[i];
-    if (d < 256) {
-      const uint32_t lp = s_tile_start[d] + s_whist[warp][d] + lrank[i];
-      if (WRITE_KEYS) s_keys[lp] = key[i];
-      s_vals[lp] = val[i];
-      s_dig[lp]  = static_cast<uint8_t>(d);
-    }
   }
   __syncthreads();
   const int64_t cnt = a.n - tbase < RTILE ? a.n - tbase : RTILE;
@@ -271,6 +335,14 @@ unsigned hblocks(int64_t n)
 
 // Two passes belong to the same carried word when they read the same column
 // transform (or bucket) and differ only in shift.
+// Histogram grid: one block per RT * kHR rows, at most five resident per SM.
+unsigned hist_blocks(int64_t n)
+{
+  int64_t b   = ceil_div(n, static_cast<int64_t>(RT) * kHR);
+  int64_t cap = static_cast<int64_t>(num_sms()) * 5;
+  return static_cast<unsigned>(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
 bool same_word(const RadixPass& a, const RadixPass& b)
 {
   if (a.src != b.src || a.src == DigitSrc::CLASS) return false;
@@ -288,10 +360,13 @@ void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes
   for (size_t b = 0; b < passes.size(); b += kHistPassesPerLaunch) {
     HistArgs h{};
     h.npasses = static_cast<int>(std::min<size_t>(kHistPassesPerLaunch, passes.size() - b));
-    for (int q = 0; q < h.npasses; ++q) h.p[q] = passes[b + q];
+    for (int q = 0; q < h.npasses; ++q) {
+      h.p[q] = passes[b + q];
+      if (q > 0 && same_word(passes[b + q - 1], passes[b + q])) h.reuse |= 1u << q;
+    }
     h.n    = n;
     h.hist = d_hist + b * 256;
-    if (n > 0) launch("histogram", histogram_kernel, hblocks(n), RT, 0, s, h);
+    if (n > 0) launch("histogram", histogram_kernel, hist_blocks(n), RT, 0, s, h);
     LDF_CHECK_LAUNCH();
   }
 }
@@ -388,7 +463,7 @@ void radix_histogram_raw(cudaStream_t s, const RadixPass& p, int64_t n, uint32_t
   h.p[0]    = p;
   h.n       = n;
   h.hist    = d_hist;
-  launch("histogram", histogram_kernel, hblocks(n), RT, 0, s, h);
+  launch("histogram", histogram_kernel, hist_blocks(n), RT, 0, s, h);
 }
 
 int64_t radix_status_words(int64_t n) { return ceil_div(n, RTILE) * 256 + 2; }

@@ -10,6 +10,8 @@ namespace ldf {
 constexpr int kRadixThreads = 256;
 constexpr int kRadixItems   = 12;
 constexpr int kRadixTile    = kRadixThreads * kRadixItems;
+// Resident onesweep CTAs per SM the register budget is sized for.
+constexpr int kRadixMinBlocks = 4;
 
 // How a pass obtains the digit of a row.
 enum class DigitSrc : int {
