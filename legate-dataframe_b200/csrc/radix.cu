@@ -84,11 +84,6 @@ __device__ __forceinline__ uint64_t pass_word(const RadixPass& p, int64_t row)
   return sort_word(p.key, row);
 }
 
-__device__ __forceinline__ uint32_t pass_digit_of_row(const RadixPass& p, int64_t row)
-{
-  if (p.src == DigitSrc::CLASS) return class_digit(p.key, row);
-  return static_cast<uint32_t>(pass_word(p, row) >> p.shift) & 0xffu;
-}
 
 constexpr int kHistPassesPerLaunch = 16;
 struct HistArgs {
@@ -184,33 +179,133 @@ struct PassArgs {
   int* err;
 };
 
-// GATHER: the word is loaded from the columns at the row (first pass of a
-// word); otherwise it is the carried key.  WRITE_KEYS: later passes of the same
-// word follow, so carry the word along.
-template <bool GATHER, bool WRITE_KEYS>
-__global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs a)
+// Predecessor tiles whose status words one look-back round trip loads.
+constexpr int kLookback = 8;
+
+// Shared state of one onesweep tile.
+struct OsShared {
+  uint32_t whist[RW][256];  // per-warp digit counts, then per-warp digit prefixes
+  uint32_t tile_start[256];  // tile-local start of each digit
+  uint64_t gbase[256];       // global position of each digit's first row of the tile
+  uint32_t scan[RW + 1];
+  int64_t tile[2];
+};
+
+// Everything of one pass over one tile after its rows are in registers:
+// key[i] / val[i] / dr[i] (digit, 256 = no row) of item i of this thread,
+// item order (warp, i, lane).  Stable warp-level ranking, tile-local scan, the
+// tile's digit counts published at once, rows staged in digit order into
+// s_keys / s_vals / s_dig (tile-local positions need no look-back), per-digit
+// decoupled look-back, then coalesced runs written out.  sh.whist must be zero
+// on entry.  Ends with every thread past its reads of the staging arrays.
+template <bool WRITE_KEYS>
+__device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile, uint64_t (&key)[RI],
+                                                 int32_t (&val)[RI], uint32_t (&dr)[RI], OsShared& sh,
+                                                 uint64_t* s_keys, int32_t* s_vals, uint8_t* s_dig)
 {
-  __shared__ uint32_t s_whist[RW][256];
-  __shared__ uint32_t s_tile_start[256];
-  __shared__ uint64_t s_gbase[256];
-  __shared__ uint32_t s_scan[RW + 1];
-  __shared__ int64_t s_tile;
-  // staged tile (dynamic): [keys u64 x RTILE when carried][rows i32 x RTILE][digits u8 x RTILE]
-  extern __shared__ __align__(16) unsigned char s_stage[];
-  uint64_t* s_keys = reinterpret_cast<uint64_t*>(s_stage);
-  int32_t* s_vals  = reinterpret_cast<int32_t*>(s_stage + (WRITE_KEYS ? RTILE * sizeof(uint64_t) : 0));
-  uint8_t* s_dig   = reinterpret_cast<uint8_t*>(s_vals + RTILE);
-
-  const int64_t tile = next_tile_id(a.counter, &s_tile);
-  for (int i = threadIdx.x; i < RW * 256; i += RT) (&s_whist[0][0])[i] = 0;
-  __syncthreads();
-
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t lt_mask = (1u << lane) - 1u;
-  const int64_t tbase    = tile * RTILE;
-  uint64_t key[RI];
-  int32_t val[RI];
-  uint32_t dr[RI];  // digit (bits 0-8, 256 = no row), then rank among the tile's rows of that digit << 9
+  // stable warp-level ranking, items in (i, lane) order
+#pragma unroll
+  for (int i = 0; i < RI; ++i) {
+    const uint32_t d     = dr[i];
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank  = __popc(peers & lt_mask);
+    uint32_t base        = 0;
+    if (d < 256) base = sh.whist[warp][d];
+    __syncwarp();
+    if (d < 256 && rank == 0) sh.whist[warp][d] = base + __popc(peers);
+    __syncwarp();
+    dr[i] = d | ((base + rank) << 9);
+  }
+  __syncthreads();
+  // per-digit warp prefixes and tile counts (thread t owns digit t)
+  const int t = threadIdx.x;
+  uint32_t run = 0;
+#pragma unroll
+  for (int w = 0; w < RW; ++w) {
+    uint32_t c       = sh.whist[w][t];
+    sh.whist[w][t]   = run;
+    run += c;
+  }
+  uint32_t tile_total;
+  const uint32_t start = block_exclusive_scan<uint32_t, RT>(run, sh.scan, &tile_total);
+  sh.tile_start[t]     = start;
+  // publish this tile's digit counts before anything else, so the tiles
+  // after it can finish their look-back while this one stages its rows
+  uint64_t* st = a.status;
+  if (tile == 0) st_release_u64(&st[t], kFlagPrefix | run);
+  else st_release_u64(&st[tile * 256 + t], kFlagAgg | run);
+  __syncthreads();
+  // stage the tile in digit order
+#pragma unroll
+  for (int i = 0; i < RI; ++i) {
+    const uint32_t d = dr[i] & 0x1ffu;
+    if (d < 256) {
+      const uint32_t lp = sh.tile_start[d] + sh.whist[warp][d] + (dr[i] >> 9);
+      if (WRITE_KEYS) s_keys[lp] = key[i];
+      s_vals[lp] = val[i];
+      s_dig[lp]  = static_cast<uint8_t>(d);
+    }
+  }
+  // per-digit decoupled look-back, kLookback predecessors' status words
+  // loaded together per round trip
+  {
+    uint64_t excl = 0;
+    if (tile > 0) {
+      int64_t j      = tile - 1;  // next predecessor to fold in
+      uint32_t spins = 0;
+      while (j >= 0) {
+        uint64_t sv[kLookback];
+#pragma unroll
+        for (int w = 0; w < kLookback; ++w) sv[w] = j - w >= 0 ? ld_volatile_u64(&st[(j - w) * 256 + t]) : kFlagPrefix;
+        int used  = 0;
+        bool done = false, stall = false;
+#pragma unroll
+        for (int w = 0; w < kLookback; ++w) {
+          if (done || stall) continue;
+          const uint64_t f = sv[w] & ~kValueMask;
+          if (f == 0) {
+            stall = true;
+            continue;
+          }
+          excl += sv[w] & kValueMask;
+          ++used;
+          if (f == kFlagPrefix) done = true;
+        }
+        if (done) break;
+        j -= used;
+        if (stall) {
+          if (++spins > kSpinLimit) {
+            atomicExch(a.err, LDF_ERR_TIMEOUT);
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      st_release_u64(&st[tile * 256 + t], kFlagPrefix | (excl + run));
+    }
+    sh.gbase[t] = a.digit_base[t] + excl;
+  }
+  __syncthreads();
+  const int64_t tbase = tile * RTILE;
+  const int64_t cnt   = a.n - tbase < RTILE ? a.n - tbase : RTILE;
+  for (int j = threadIdx.x; j < cnt; j += RT) {
+    const uint32_t d  = s_dig[j];
+    const int64_t pos = static_cast<int64_t>(sh.gbase[d]) + (j - static_cast<int64_t>(sh.tile_start[d]));
+    if (WRITE_KEYS) a.keys_out[pos] = s_keys[j];
+    a.vals_out[pos] = s_vals[j];
+  }
+}
+
+// Rows of a tile straight from global memory (GATHER: the word is loaded from
+// the columns at the row, the first pass of a word; otherwise the carried key).
+template <bool GATHER>
+__device__ __forceinline__ void load_tile_rows(const PassArgs& a, int64_t tile, uint64_t (&key)[RI],
+                                               int32_t (&val)[RI], uint32_t (&dr)[RI])
+{
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t tbase = tile * RTILE;
 #pragma unroll
   for (int i = 0; i < RI; ++i) {
     const int64_t idx = tbase + warp * (32 * RI) + i * 32 + lane;
@@ -228,82 +323,28 @@ __global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs 
       }
     }
   }
-  // stable warp-level ranking, items in (i, lane) order
-#pragma unroll
-  for (int i = 0; i < RI; ++i) {
-    const uint32_t d     = dr[i];
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    const uint32_t rank  = __popc(peers & lt_mask);
-    uint32_t base        = 0;
-    if (d < 256) base = s_whist[warp][d];
-    __syncwarp();
-    if (d < 256 && rank == 0) s_whist[warp][d] = base + __popc(peers);
-    __syncwarp();
-    dr[i] = d | ((base + rank) << 9);
-  }
+}
+
+// One tile per CTA.  WRITE_KEYS: later passes of the same word follow, so
+// carry the word along.
+template <bool GATHER, bool WRITE_KEYS>
+__global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs a)
+{
+  __shared__ OsShared sh;
+  // staged tile (dynamic): [keys u64 x RTILE when carried][rows i32 x RTILE][digits u8 x RTILE]
+  extern __shared__ __align__(16) unsigned char s_stage[];
+  uint64_t* s_keys = reinterpret_cast<uint64_t*>(s_stage);
+  int32_t* s_vals  = reinterpret_cast<int32_t*>(s_stage + (WRITE_KEYS ? RTILE * sizeof(uint64_t) : 0));
+  uint8_t* s_dig   = reinterpret_cast<uint8_t*>(s_vals + RTILE);
+
+  const int64_t tile = next_tile_id(a.counter, &sh.tile[0]);
+  for (int i = threadIdx.x; i < RW * 256; i += RT) (&sh.whist[0][0])[i] = 0;
   __syncthreads();
-  // per-digit warp prefixes and tile counts (thread t owns digit t)
-  const int t = threadIdx.x;
-  uint32_t run = 0;
-#pragma unroll
-  for (int w = 0; w < RW; ++w) {
-    uint32_t c    = s_whist[w][t];
-    s_whist[w][t] = run;
-    run += c;
-  }
-  uint32_t tile_total;
-  const uint32_t start = block_exclusive_scan<uint32_t, RT>(run, s_scan, &tile_total);
-  s_tile_start[t]      = start;
-  // publish this tile's digit counts before anything else, so the tiles
-  // after it can finish their look-back while this one stages its rows
-  uint64_t* st = a.status;
-  if (tile == 0) st_release_u64(&st[t], kFlagPrefix | run);
-  else st_release_u64(&st[tile * 256 + t], kFlagAgg | run);
-  __syncthreads();
-  // stage the tile in digit order (tile-local positions need no look-back)
-#pragma unroll
-  for (int i = 0; i < RI; ++i) {
-    const uint32_t d = dr[i] & 0x1ffu;
-    if (d < 256) {
-      const uint32_t lp = s_tile_start[d] + s_whist[warp][d] + (dr[i] >> 9);
-      if (WRITE_KEYS) s_keys[lp] = key[i];
-      s_vals[lp] = val[i];
-      s_dig[lp]  = static_cast<uint8_t>(d);
-    }
-  }
-  // per-digit decoupled look-back
-  {
-    uint64_t excl = 0;
-    if (tile > 0) {
-      int64_t j      = tile - 1;
-      uint32_t spins = 0;
-      while (j >= 0) {
-        uint64_t s = ld_volatile_u64(&st[j * 256 + t]);
-        uint64_t f = s & ~kValueMask;
-        if (f == 0) {
-          if (++spins > kSpinLimit) {
-            atomicExch(a.err, LDF_ERR_TIMEOUT);
-            break;
-          }
-          __nanosleep(32);
-          continue;
-        }
-        excl += s & kValueMask;
-        if (f == kFlagPrefix) break;
-        --j;
-      }
-      st_release_u64(&st[tile * 256 + t], kFlagPrefix | (excl + run));
-    }
-    s_gbase[t] = a.digit_base[t] + excl;
-  }
-  __syncthreads();
-  const int64_t cnt = a.n - tbase < RTILE ? a.n - tbase : RTILE;
-  for (int j = threadIdx.x; j < cnt; j += RT) {
-    const uint32_t d  = s_dig[j];
-    const int64_t pos = static_cast<int64_t>(s_gbase[d]) + (j - static_cast<int64_t>(s_tile_start[d]));
-    if (WRITE_KEYS) a.keys_out[pos] = s_keys[j];
-    a.vals_out[pos] = s_vals[j];
-  }
+  uint64_t key[RI];
+  int32_t val[RI];
+  uint32_t dr[RI];
+  load_tile_rows<GATHER>(a, tile, key, val, dr);
+  rank_and_scatter<WRITE_KEYS>(a, tile, key, val, dr, sh, s_keys, s_vals, s_dig);
 }
 
 constexpr size_t onesweep_smem(bool write_keys)
@@ -333,8 +374,6 @@ unsigned hblocks(int64_t n)
   return static_cast<unsigned>(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
-// Two passes belong to the same carried word when they read the same column
-// transform (or bucket) and differ only in shift.
 // Histogram grid: one block per RT * kHR rows, at most five resident per SM.
 unsigned hist_blocks(int64_t n)
 {
@@ -343,6 +382,8 @@ unsigned hist_blocks(int64_t n)
   return static_cast<unsigned>(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
+// Two passes belong to the same carried word when they read the same column
+// transform (or bucket) and differ only in shift.
 bool same_word(const RadixPass& a, const RadixPass& b)
 {
   if (a.src != b.src || a.src == DigitSrc::CLASS) return false;

@@ -95,3 +95,19 @@ def test_sort_all_equal_skips_passes():
     t = pa.table({"a": np.full(10000, 7, dtype=np.int64), "row": np.arange(10000)})
     res = run_sort(t, ["a"])
     assert res.column("row").to_pylist() == list(range(10000))
+
+
+@pytest.mark.parametrize("n", [3_000_000, 3072 * 1000])
+def test_sort_many_tiles_per_block(n):
+    """Thousands of onesweep tiles per pass (long look-back chains, the
+    look-back loading several predecessors per round trip), with and without a
+    partial last tile; two keys so the second key's first pass gathers
+    through the permutation."""
+    rng = np.random.default_rng(11)
+    t = pa.table({"k": rng.integers(-(2**63), 2**63 - 1, n, dtype=np.int64),
+                  "u": pa.array(rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)),
+                  "row": np.arange(n)})
+    res = run_sort(t, ["k"])
+    assert_tables_equal(res, R.sort(t, ["k"]), sort_by=None)
+    res = run_sort(t, ["u", "k"], [False, True])
+    assert_tables_equal(res, R.sort(t, ["u", "k"], [False, True]), sort_by=None)
