@@ -135,7 +135,12 @@ typedef struct {
  * request order; null keys form a group (null_policy::INCLUDE).  Output row
  * order is unspecified.  Replaces the cudf::groupby call in
  * GroupByAggregationTask::gpu_variant (groupby_aggregation.cu:90-167);
- * semantics of the Acero hash_* aggregations (groupby_aggregation.cpp:41-94). */
+ * semantics of the Acero hash_* aggregations (groupby_aggregation.cpp:41-94).
+ * Input buffers may also be host memory (pinned, or pageable at lower copy
+ * speed): such columns are copied to the device inside the call on a side
+ * stream, keys first, and each pass starts as soon as the columns it reads
+ * have arrived; the host buffers must stay valid until `stream` has passed
+ * the end of the call. */
 int ldf_b200_groupby_aggregation(const ldf_column* table, int32_t ncols,
                                  const int32_t* keys, int32_t nkeys,
                                  const ldf_aggregation* aggs, int32_t naggs,

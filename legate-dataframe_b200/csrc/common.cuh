@@ -46,6 +46,10 @@ struct LdfError : std::runtime_error {
 // multiples of it.
 int num_sms();
 
+// Non-blocking stream of the current device for host -> device staging copies
+// (created on first use, one per device, kept until the process exits).
+cudaStream_t staging_stream();
+
 // ---------------------------------------------------------------------------
 // Kernel launches.  Every kernel of the library goes through `launch`, which
 // counts launches and, when profiling is on, brackets the launch with CUDA

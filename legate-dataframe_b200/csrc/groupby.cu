@@ -1484,8 +1484,14 @@ void launch_column(ColArgs& a, int type)
 
 template <KeyMode M>
 void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const int32_t* keys, int nkeys,
-                 const ldf_aggregation* aggs, int naggs, const std::vector<int>& agg_col, ldf_column* out)
+                 const ldf_aggregation* aggs, int naggs, const std::vector<int>& agg_col, ldf_column* out,
+                 const HostStaging& hs, const std::vector<int>& col_of_plan)
 {
+  // host-resident inputs: wait for a column's copy right before its first reader
+  auto wait_keys = [&]() {
+    for (int j = 0; j < nkeys; ++j) hs.wait(keys[j]);
+  };
+  auto wait_plan_col = [&](int ci) { hs.wait(col_of_plan[ci]); };
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
   g_column_stream     = s;
@@ -1525,6 +1531,8 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
       LDF_CUDA(cudaMemsetAsync(spcounts.get(), 0, pc.pair_cap * 4, s));
       pc.pairs = spairs.get();
     }
+    wait_keys();
+    if (ndist_col >= 0) wait_plan_col(ndist_col);
     launch("sample", sample_kernel<M>, gs_blocks(ns, 256), 256, 0, s, p.k, ns, stride, sslots.get(), scap,
            scounts.get(), pc, ndist_col >= 0 ? 1 : 0, spcounts.get());
     Buffer<unsigned long long> stats(al, 4);
@@ -1649,6 +1657,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
       LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, assign_kernel<M>, kGbThreads, a_smem));
       const int64_t ablocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(occ, 1),
                                                 ceil_div(n, int64_t(kGbThreads) * kRows));
+      wait_keys();
       launch("assign", assign_kernel<M>, static_cast<unsigned>(ablocks), kGbThreads, a_smem, s, pa, gid.get());
       unsigned long long hm[2];
       LDF_CUDA(cudaMemcpyAsync(hm, misc.get(), 16, cudaMemcpyDeviceToHost, s));
@@ -1698,11 +1707,17 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
              newid.get(), rec.get());
 
       // pass 2: one kernel per value column that needs valid counts / sums / min / max
-      // (a NUNIQUE column of <= 4-byte values also gets its value range here)
+      // (a NUNIQUE column of <= 4-byte values also gets its value range here).
+      // NUNIQUE columns first: host-resident inputs are copied in that order.
       std::vector<Buffer<unsigned int>> vranges(p.ncols);
-      for (int ci = 0; ci < p.ncols; ++ci) {
+      std::vector<int> pass_order;
+      for (int ci = 0; ci < p.ncols; ++ci)
+        if (p.c[ci].states & ST_NDIST) pass_order.push_back(ci);
+      for (int ci = 0; ci < p.ncols; ++ci)
+        if (!(p.c[ci].states & ST_NDIST)) pass_order.push_back(ci);
+      auto column_pass = [&](int ci) {
         ColPlan& c = p.c[ci];
-        if (!c.nullable && !(c.states & (ST_SUM | ST_MIN | ST_MAX))) continue;
+        if (!c.nullable && !(c.states & (ST_SUM | ST_MIN | ST_MAX))) return;
         ColArgs a{};
         if ((c.states & ST_NDIST) && c.pair_packed) {
           vranges[ci]                  = Buffer<unsigned int>(al, 2);
@@ -1744,12 +1759,16 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
         if ((a.states & ST_MIN) && !c.mm64) a.sh_mn = take(4);
         if ((a.states & ST_MAX) && !c.mm64) a.sh_mx = take(4);
         a.smem_bytes = off;
+        wait_plan_col(ci);
         launch_column(a, c.col.type);
-      }
-      // pass 3: NUNIQUE
-      for (int ci = 0; ci < p.ncols; ++ci) {
+      };
+      // pass 3: NUNIQUE of one column (after its column pass, which records
+      // the value range).  With host-resident inputs it runs right after that
+      // pass, before the other columns' passes, so a column still being
+      // copied holds back as little work as possible.
+      auto nunique_pass = [&](int ci) {
         ColPlan& c = p.c[ci];
-        if (!(c.states & ST_NDIST)) continue;
+        wait_plan_col(ci);
         if (c.pair_packed) {
           NdArgs na{gid.get(), newid.get(), c.col, n, c.pairs, c.pair_cap, rec.get() + c.off_nd * L,
                     static_cast<int>(std::min<int64_t>(std::min(hot_cap, 12 * 1024), nid)), p.overflow};
@@ -1869,6 +1888,16 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
                  static_cast<const uint32_t*>(gid.get()), static_cast<const uint32_t*>(newid.get()),
                  rec.get() + c.off_nd * L);
         }
+      };
+      if (hs.staged_bytes() > 0) {
+        for (int ci : pass_order) {
+          column_pass(ci);
+          if (p.c[ci].states & ST_NDIST) nunique_pass(ci);
+        }
+      } else {  // all inputs on the device: every column pass, then the NUNIQUE passes
+        for (int ci : pass_order) column_pass(ci);
+        for (int ci : pass_order)
+          if (p.c[ci].states & ST_NDIST) nunique_pass(ci);
       }
       LDF_CUDA(cudaMemcpyAsync(hm, misc.get(), 16, cudaMemcpyDeviceToHost, s));
       ctx.finish();
@@ -1937,6 +1966,16 @@ void groupby_aggregation(const ldf_column* table, int ncols, const int32_t* keys
 {
   if (nkeys < 1) fail(LDF_ERR_INVALID_ARGUMENT, "must pass at least one key column");
   LDF_REQUIRE(naggs <= kMaxAggs, "too many aggregations");
+  // Host-resident inputs are copied in the order the passes read them: the
+  // keys, then NUNIQUE inputs, then the other aggregated columns.
+  std::vector<int> order(keys, keys + nkeys);
+  for (int pass = 0; pass < 2; ++pass)
+    for (int a = 0; a < naggs; ++a)
+      if (aggs[a].kind != LDF_AGG_COUNT_ALL && (aggs[a].kind == LDF_AGG_COUNT_DISTINCT) == (pass == 0))
+        order.push_back(aggs[a].in_col);
+  for (int j = 0; j < nkeys; ++j) LDF_REQUIRE(keys[j] >= 0 && keys[j] < ncols, "key column index out of range");
+  HostStaging hs(ctx, table, ncols, order);
+  table = hs.table();
   KeyCols k       = make_keys(table, ncols, keys, nkeys);
   const int64_t n = ncols > 0 ? table[0].size : 0;
   LDF_REQUIRE(n < (int64_t(1) << 31), "tables of 2^31 rows or more per task are not supported");
@@ -1981,9 +2020,13 @@ void groupby_aggregation(const ldf_column* table, int ncols, const int32_t* keys
       fail(LDF_ERR_UNSUPPORTED, "min/max of a string column is not supported");
   }
   switch (key_mode(k)) {
-    case KeyMode::K32: run_groupby<KeyMode::K32>(ctx, p, table, keys, nkeys, aggs, naggs, agg_col, out); break;
-    case KeyMode::K64: run_groupby<KeyMode::K64>(ctx, p, table, keys, nkeys, aggs, naggs, agg_col, out); break;
-    default: run_groupby<KeyMode::GEN>(ctx, p, table, keys, nkeys, aggs, naggs, agg_col, out); break;
+    case KeyMode::K32:
+      run_groupby<KeyMode::K32>(ctx, p, table, keys, nkeys, aggs, naggs, agg_col, out, hs, col_of_plan);
+      break;
+    case KeyMode::K64:
+      run_groupby<KeyMode::K64>(ctx, p, table, keys, nkeys, aggs, naggs, agg_col, out, hs, col_of_plan);
+      break;
+    default: run_groupby<KeyMode::GEN>(ctx, p, table, keys, nkeys, aggs, naggs, agg_col, out, hs, col_of_plan); break;
   }
 }
 

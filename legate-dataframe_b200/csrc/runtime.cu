@@ -79,6 +79,19 @@ int num_sms()
   return sms;
 }
 
+cudaStream_t staging_stream()
+{
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static cudaStream_t streams[kMaxDevices] = {};
+  int dev = 0;
+  LDF_CUDA(cudaGetDevice(&dev));
+  LDF_REQUIRE(dev >= 0 && dev < kMaxDevices, "device ordinal out of range");
+  std::lock_guard<std::mutex> g(mu);
+  if (streams[dev] == nullptr) LDF_CUDA(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
+  return streams[dev];
+}
+
 void* Allocator::allocate(size_t nbytes) const
 {
   if (nbytes == 0) nbytes = 16;

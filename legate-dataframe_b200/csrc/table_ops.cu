@@ -47,6 +47,75 @@ void free_out_column(const Allocator& a, ldf_column& c)
   c.chars = nullptr;
 }
 
+// ---- host-resident inputs -----------------------------------------------------
+namespace {
+bool host_resident(const void* p)
+{
+  if (p == nullptr) return false;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return true;  // unknown to CUDA: plain host memory
+  }
+  return at.type == cudaMemoryTypeHost || at.type == cudaMemoryTypeUnregistered;
+}
+}  // namespace
+
+HostStaging::HostStaging(const OpContext& ctx, const ldf_column* table, int ncols, const std::vector<int>& order)
+  : s_(ctx.stream()), table_(table, table + ncols), ready_(static_cast<size_t>(ncols), nullptr)
+{
+  const Allocator& al = ctx.alloc();
+  cudaStream_t cs     = nullptr;
+  for (int c : order) {
+    if (c < 0 || c >= ncols || ready_[c] != nullptr) continue;
+    ldf_column& col  = table_[c];
+    const bool str   = col.type == LDF_STRING;
+    const bool h_dat = host_resident(col.data), h_val = host_resident(col.valid);
+    const bool h_chr = str && host_resident(col.chars);
+    if (!h_dat && !h_val && !h_chr) continue;
+    if (cs == nullptr) {
+      // the staging buffers may reuse memory that earlier work on the op's
+      // stream still touches: the copies start after that work
+      cs = staging_stream();
+      cudaEvent_t e0;
+      LDF_CUDA(cudaEventCreateWithFlags(&e0, cudaEventDisableTiming));
+      LDF_CUDA(cudaEventRecord(e0, s_));
+      LDF_CUDA(cudaStreamWaitEvent(cs, e0, 0));
+      LDF_CUDA(cudaEventDestroy(e0));
+    }
+    auto stage = [&](void* src, size_t nbytes) -> void* {
+      bufs_.emplace_back(al, std::max<size_t>(nbytes, 1));
+      void* dst = bufs_.back().get();
+      if (nbytes) LDF_CUDA(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyHostToDevice, cs));
+      bytes_ += static_cast<int64_t>(nbytes);
+      return dst;
+    };
+    const size_t rows = static_cast<size_t>(col.size);
+    if (h_dat) col.data = stage(col.data, rows * (str ? sizeof(ldf_range) : static_cast<size_t>(type_width(col.type))));
+    if (h_val) col.valid = static_cast<uint8_t*>(stage(col.valid, rows));
+    if (h_chr) col.chars = static_cast<char*>(stage(col.chars, static_cast<size_t>(col.num_chars)));
+    LDF_CUDA(cudaEventCreateWithFlags(&ready_[c], cudaEventDisableTiming));
+    LDF_CUDA(cudaEventRecord(ready_[c], cs));
+  }
+}
+
+HostStaging::~HostStaging()
+{
+  // the op's stream passes every copy before the staging buffers go back to
+  // the allocator (also when the op failed part way)
+  for (cudaEvent_t e : ready_)
+    if (e != nullptr) {
+      cudaStreamWaitEvent(s_, e, 0);
+      cudaEventDestroy(e);
+    }
+}
+
+void HostStaging::wait(int col) const
+{
+  if (col >= 0 && col < static_cast<int>(ready_.size()) && ready_[col] != nullptr)
+    LDF_CUDA(cudaStreamWaitEvent(s_, ready_[col], 0));
+}
+
 namespace {
 
 // Output length and source chars offset of each gathered string: srcoff[i] =

@@ -80,6 +80,32 @@ __device__ __forceinline__ void write_out_row(const OutSpec& o, int64_t pos, int
   }
 }
 
+// Input columns that live in host memory (pinned or pageable), copied to the
+// device inside the op so that the copies overlap its kernels.  The columns
+// named in `order` are copied in that order on the staging stream, one event
+// after each; the op's stream waits on a column's event (`wait`) right before
+// the first kernel that reads it.  `table` is the op's view of the input with
+// device pointers.  Columns already on the device are used in place.  The
+// host memory must stay valid until the op's stream has passed the end of
+// the op.
+class HostStaging {
+ public:
+  HostStaging(const OpContext& ctx, const ldf_column* table, int ncols, const std::vector<int>& order);
+  ~HostStaging();
+  HostStaging(const HostStaging&)            = delete;
+  HostStaging& operator=(const HostStaging&) = delete;
+  const ldf_column* table() const { return table_.data(); }
+  void wait(int col) const;
+  int64_t staged_bytes() const { return bytes_; }
+
+ private:
+  cudaStream_t s_;
+  std::vector<ldf_column> table_;
+  std::vector<cudaEvent_t> ready_;
+  std::vector<Buffer<uint8_t>> bufs_;
+  int64_t bytes_ = 0;
+};
+
 // Allocate an output column of `rows` rows (fixed width or string ranges).
 ldf_column alloc_out_column(const Allocator& a, int type, int64_t rows, bool nullable);
 void free_out_column(const Allocator& a, ldf_column& c);

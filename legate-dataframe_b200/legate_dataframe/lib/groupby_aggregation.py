@@ -62,7 +62,9 @@ def groupby_aggregation(
     "count_distinct", or ``(kind, pyarrow.compute.CountOptions)`` for the
     count kinds.  The output holds the key columns then one column per
     aggregation in request order; row order is unspecified.  Null keys form a
-    group.
+    group.  The table's columns may be device tensors or host tensors (pinned
+    for full copy speed): host columns are copied to the device inside the
+    call, overlapped with the passes that do not need them yet.
     """
     keys = list(keys)
     if len(keys) == 0:

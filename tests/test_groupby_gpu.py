@@ -227,3 +227,36 @@ def test_groupby_nunique_size_tiers(segments, vtype, monkeypatch):
     res = run_groupby(t, ["k"], aggs)
     exp = R.groupby(t, ["k"], aggs)
     assert_tables_equal(res, exp, sort_by=["k"])
+
+
+def _on_host(col, pinned):
+    """The same column with every buffer in host memory (pinned or pageable)."""
+    from legate_dataframe import LogicalColumn
+
+    def h(t):
+        if t is None:
+            return None
+        t = t.cpu()
+        return t.pin_memory() if pinned else t
+
+    return LogicalColumn(col.arrow_type, col.ldf_type, col.size, h(col.data), h(col.valid), h(col.chars),
+                         col.chars_base, col.num_chars)
+
+
+@pytest.mark.parametrize("key_kind", ["int64", "string", "int32"])
+@pytest.mark.parametrize("pinned", [True, False])
+def test_groupby_host_resident_inputs(key_kind, pinned):
+    """Input columns in host memory are copied to the device inside the op
+    (overlapped with its passes); the result is bit-identical to the one of
+    the same columns resident on the device, on two calls in a row."""
+    from legate_dataframe import LogicalTable
+    from legate_dataframe.lib.groupby_aggregation import groupby_aggregation
+
+    rng = np.random.default_rng(23)
+    t = _table(rng, 200_000, key_kind, 3000, zipf=1.2)
+    dev = LogicalTable.from_arrow(t)
+    host = LogicalTable([_on_host(c, pinned) for c in dev.get_columns()], dev.get_column_names())
+    exp = groupby_aggregation(dev, ["k"], ALL_AGGS).to_arrow()
+    for _ in range(2):
+        res = groupby_aggregation(host, ["k"], ALL_AGGS).to_arrow()
+        assert_tables_equal(res, exp, sort_by=["k"])
