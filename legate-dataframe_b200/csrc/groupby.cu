@@ -331,18 +331,27 @@ __device__ __forceinline__ uint64_t pool_take(const GbPlan& p, IdPool& pool, boo
 }
 
 constexpr int kRows = 4;  // rows per lane per step (memory-level parallelism)
-
-// Group ids of the kRows rows of this lane (kUnsetId for rows past the end).
+// Rows per lane per step of the assign pass.  Multi-column and string keys
+// (GEN) take one: their key hashing and comparison code is large, and four
+// unrolled copies of it outgrow the instruction cache.
+constexpr int kGenRows = 1;
 template <KeyMode M>
-__device__ void group_ids(const GbPlan& p, IdPool& pool, const int64_t (&r)[kRows], uint32_t (&id)[kRows])
+__host__ __device__ constexpr int assign_rows()
+{
+  return M == KeyMode::GEN ? kGenRows : kRows;
+}
+
+// Group ids of the R rows of this lane (kUnsetId for rows past the end).
+template <KeyMode M, int R>
+__device__ void group_ids(const GbPlan& p, IdPool& pool, const int64_t (&r)[R], uint32_t (&id)[R])
 {
   const uint64_t empty = empty_word<M>();
-  uint64_t word[kRows], h[kRows], idx[kRows], hi[kRows];
-  bool pending[kRows];
+  uint64_t word[R], h[R], idx[R], hi[R];
+  bool pending[R];
   unsigned long long* s = p.slots;
   const int sw          = M == KeyMode::K32 ? 1 : 2;  // words per slot
 #pragma unroll
-  for (int j = 0; j < kRows; ++j) {
+  for (int j = 0; j < R; ++j) {
     id[j]      = kUnsetId;
     pending[j] = false;
     word[j] = h[j] = idx[j] = hi[j] = 0;
@@ -367,9 +376,9 @@ __device__ void group_ids(const GbPlan& p, IdPool& pool, const int64_t (&r)[kRow
     pending[j] = true;
   }
   // first probes of all rows in flight together
-  uint64_t v[kRows];
+  uint64_t v[R];
 #pragma unroll
-  for (int j = 0; j < kRows; ++j) {
+  for (int j = 0; j < R; ++j) {
     v[j] = 0;
     if (!pending[j]) continue;
     if (M == KeyMode::K32) {
@@ -380,9 +389,9 @@ __device__ void group_ids(const GbPlan& p, IdPool& pool, const int64_t (&r)[kRow
       hi[j]              = t.y;
     }
   }
-  bool need[kRows];
+  bool need[R];
 #pragma unroll
-  for (int j = 0; j < kRows; ++j) {
+  for (int j = 0; j < R; ++j) {
     need[j] = false;
     if (!pending[j]) continue;
     for (int probe = 0; probe < kMaxProbe; ++probe) {
@@ -408,7 +417,7 @@ __device__ void group_ids(const GbPlan& p, IdPool& pool, const int64_t (&r)[kRow
   }
   // inserts: ids from the warp pool, then publish
 #pragma unroll
-  for (int j = 0; j < kRows; ++j) {
+  for (int j = 0; j < R; ++j) {
     const uint64_t mine = pool_take(p, pool, need[j]);
     if (!need[j] || mine == kEmpty) continue;
     p.id_key[mine]      = M == KeyMode::GEN ? static_cast<uint64_t>(r[j]) : word[j];
@@ -508,7 +517,8 @@ __global__ void __launch_bounds__(kGbThreads) assign_kernel(GbPlan p, uint32_t* 
   for (int i = threadIdx.x; i < H; i += blockDim.x) cnt[i] = 0;
   __syncthreads();
   IdPool pool{0, 0};
-  constexpr int64_t kChunk = 32 * kRows * 32;  // rows per dynamically scheduled chunk
+  constexpr int R          = assign_rows<M>();
+  constexpr int64_t kChunk = 32 * R * 32;  // rows per dynamically scheduled chunk
   for (;;) {
     unsigned long long chunk = 0;
     if (lane_id() == 0) chunk = atomicAdd(p.chunk_counter, 1ull);
@@ -516,17 +526,17 @@ __global__ void __launch_bounds__(kGbThreads) assign_kernel(GbPlan p, uint32_t* 
     const int64_t c0 = static_cast<int64_t>(chunk) * kChunk;
     if (c0 >= p.n) break;
     const int64_t c1 = c0 + kChunk < p.n ? c0 + kChunk : p.n;
-    for (int64_t base = c0; base < c1; base += 32 * kRows) {
-      int64_t r[kRows];
-      uint32_t id[kRows];
+    for (int64_t base = c0; base < c1; base += 32 * R) {
+      int64_t r[R];
+      uint32_t id[R];
 #pragma unroll
-      for (int j = 0; j < kRows; ++j) {
+      for (int j = 0; j < R; ++j) {
         r[j] = base + j * 32 + lane_id();
         if (r[j] >= c1) r[j] = p.n;  // past the chunk: no row
       }
-      group_ids<M>(p, pool, r, id);
+      group_ids<M, R>(p, pool, r, id);
 #pragma unroll
-      for (int j = 0; j < kRows; ++j) {
+      for (int j = 0; j < R; ++j) {
         if (r[j] >= p.n) continue;
         gid[r[j]] = id[j];
         if (id[j] == kUnsetId) continue;
@@ -1656,7 +1666,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
       int occ               = 1;
       LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, assign_kernel<M>, kGbThreads, a_smem));
       const int64_t ablocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(occ, 1),
-                                                ceil_div(n, int64_t(kGbThreads) * kRows));
+                                                ceil_div(n, int64_t(kGbThreads) * assign_rows<M>()));
       wait_keys();
       launch("assign", assign_kernel<M>, static_cast<unsigned>(ablocks), kGbThreads, a_smem, s, pa, gid.get());
       unsigned long long hm[2];
