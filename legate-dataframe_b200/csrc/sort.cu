@@ -15,8 +15,10 @@
 //
 // hash_partition: reference task::repartition_by_hash local step
 // (cpp/src/core/repartition_by_hash.cu:296-310): bucket = hash(keys) % nparts,
-// rows grouped by bucket, start offsets returned; here one stable radix pass
-// on the bucket id (two for more than 256 buckets) then one gather.
+// rows grouped by bucket, start offsets returned; here one pass hashes the
+// keys into a bucket id per row (and counts the buckets), then one stable
+// radix pass on the bucket ids (two for more than 256 buckets), then one
+// gather.
 #include "radix.cuh"
 
 namespace ldf {
@@ -304,7 +306,10 @@ void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const u
 }
 
 namespace {
-__global__ void bucket_count_kernel(KeyCols k, int64_t n, uint32_t nparts, unsigned long long* counts)
+// Bucket id of every row (hash of the key columns % nparts), written once so
+// that the radix passes read 4 bytes per row instead of hashing the keys
+// again, and the bucket sizes.
+__global__ void bucket_ids_kernel(KeyCols k, int64_t n, uint32_t nparts, uint32_t* ids, unsigned long long* counts)
 {
   extern __shared__ unsigned int sc[];
   const bool use_smem = nparts <= 8192;
@@ -313,6 +318,7 @@ __global__ void bucket_count_kernel(KeyCols k, int64_t n, uint32_t nparts, unsig
   __syncthreads();
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t b = static_cast<uint32_t>(key_bits<KeyMode::GEN>(k, r) % nparts);
+    ids[r]           = b;
     if (use_smem) atomicAdd(&sc[b], 1u);
     else atomicAdd(&counts[b], 1ull);
   }
@@ -332,25 +338,34 @@ void hash_partition(const ldf_column* table, int ncols, const int32_t* keys, int
   LDF_REQUIRE(n < (int64_t(1) << 31), "tables of 2^31 rows or more per task are not supported");
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
-  std::vector<RadixPass> passes;
-  for (uint64_t span = 1, shift = 0; span < static_cast<uint64_t>(nparts); span <<= 8, shift += 8) {
-    RadixPass p{};
-    p.src       = DigitSrc::BUCKET;
-    p.shift     = static_cast<int>(shift);
-    p.hash_keys = k;
-    p.nparts    = static_cast<uint32_t>(nparts);
-    passes.push_back(p);
-  }
-  Buffer<int32_t> perm(al, std::max<int64_t>(n, 1));
-  radix_sort_rows(ctx, passes, n, perm.get());
-  // bucket sizes
+  // bucket id of every row, and the bucket sizes
+  Buffer<uint32_t> ids(al, std::max<int64_t>(n, 1));
   Buffer<unsigned long long> counts(al, nparts);
   LDF_CUDA(cudaMemsetAsync(counts.get(), 0, static_cast<size_t>(nparts) * 8, s));
   if (n > 0) {
     size_t smem = nparts <= 8192 ? static_cast<size_t>(nparts) * 4 : 0;
-    launch("bucket_count", bucket_count_kernel, blocks_for(n), 256, smem, s, k, n, static_cast<uint32_t>(nparts), counts.get());
+    launch("bucket_ids", bucket_ids_kernel, blocks_for(n), 256, smem, s, k, n, static_cast<uint32_t>(nparts), ids.get(),
+           counts.get());
     LDF_CHECK_LAUNCH();
   }
+  // stable radix passes over the bucket ids (a uint32 column, no nulls)
+  ldf_column idc{};
+  idc.type = LDF_UINT32;
+  idc.size = n;
+  idc.data = ids.get();
+  std::vector<RadixPass> passes;
+  for (uint64_t span = 1, shift = 0; span < static_cast<uint64_t>(nparts); span <<= 8, shift += 8) {
+    RadixPass p{};
+    p.src              = DigitSrc::COLUMN;
+    p.shift            = static_cast<int>(shift);
+    p.key.col          = make_dcol(idc);
+    p.key.descending   = 0;
+    p.key.nulls_at_end = 1;
+    p.key.key_bytes    = 4;
+    passes.push_back(p);
+  }
+  Buffer<int32_t> perm(al, std::max<int64_t>(n, 1));
+  radix_sort_rows(ctx, passes, n, perm.get());
   std::vector<unsigned long long> h(nparts);
   LDF_CUDA(cudaMemcpyAsync(h.data(), counts.get(), static_cast<size_t>(nparts) * 8, cudaMemcpyDeviceToHost, s));
   gather_table(ctx, table, ncols, perm.get(), n, out);
