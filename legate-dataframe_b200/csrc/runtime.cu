@@ -186,45 +186,102 @@ void OpContext::finish() const
 }
 
 // ---------------------------------------------------------------------------
-// Single-pass exclusive scan with decoupled look-back.  256 threads x 8 items
-// per tile; the input is read once and the output written once.
+// Single-pass exclusive scan with decoupled look-back.  256 threads x 16 items
+// per tile; the input is read once and the output written once, both
+// coalesced: item i of a thread is element i * 32 + lane of its warp's
+// 512-element segment, so each warp scans its segment as 16 warp-wide scans
+// with a running carry.  Warp 0 does the look-back over a window of 32
+// predecessor tiles per round trip.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int kScanThreads = 256;
-constexpr int kScanItems   = 8;
+constexpr int kScanItems   = 16;
+constexpr int kScanWarps   = kScanThreads / 32;
 constexpr int kScanTile    = kScanThreads * kScanItems;
+
+// Exclusive prefix of `tile` over the tile aggregates before it; every lane
+// of one warp calls it.  Publishes the tile's aggregate first and its
+// inclusive prefix at the end.
+__device__ __forceinline__ uint64_t warp_lookback(uint64_t* status, int64_t tile, uint64_t aggregate, int* err)
+{
+  const int lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) st_release_u64(&status[0], kFlagPrefix | aggregate);
+    return 0;
+  }
+  if (lane == 0) st_release_u64(&status[tile], kFlagAgg | aggregate);
+  uint64_t excl  = 0;
+  int64_t j      = tile - 1;  // the window covers tiles j, j - 1, ..., j - 31 (lane order)
+  uint32_t spins = 0;
+  for (;;) {
+    const int64_t t  = j - lane;
+    const uint64_t v = t >= 0 ? ld_volatile_u64(&status[t]) : kFlagPrefix;
+    const uint64_t f = v & ~kValueMask;
+    const uint32_t not_ready = __ballot_sync(0xffffffffu, f == 0);
+    const uint32_t prefix    = __ballot_sync(0xffffffffu, f == kFlagPrefix);
+    const int first_prefix   = prefix ? __ffs(prefix) - 1 : 32;
+    const int first_waiting  = not_ready ? __ffs(not_ready) - 1 : 32;
+    if (first_waiting < first_prefix) {  // a tile before the nearest prefix has not published yet
+      if (++spins > kSpinLimit) {
+        if (lane == 0) atomicExch(err, LDF_ERR_TIMEOUT);
+        break;
+      }
+      __nanosleep(32);
+      continue;
+    }
+    excl += warp_reduce_sum<uint64_t>(lane <= first_prefix ? (v & kValueMask) : 0);
+    if (first_prefix < 32) break;
+    j -= 32;
+  }
+  if (lane == 0) st_release_u64(&status[tile], kFlagPrefix | (excl + aggregate));
+  return excl;
+}
 
 template <typename TIn>
 __global__ void __launch_bounds__(kScanThreads)
   scan_kernel(const TIn* in, int64_t* out, int64_t n, uint64_t* status,
               unsigned long long* counter, int64_t* total, int* err)
 {
-  __shared__ int64_t s_scan[kScanThreads / 32 + 1];
+  __shared__ int64_t s_warp[kScanWarps + 1];
   __shared__ int64_t s_tile;
   __shared__ uint64_t s_prefix;
-  const int64_t tile = next_tile_id(counter, &s_tile);
-  const int64_t base = tile * kScanTile + static_cast<int64_t>(threadIdx.x) * kScanItems;
+  const int64_t tile  = next_tile_id(counter, &s_tile);
+  const int warp      = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t wbase = tile * kScanTile + static_cast<int64_t>(warp) * (32 * kScanItems);
   int64_t v[kScanItems];
-  int64_t sum = 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    int64_t r = base + i;
-    v[i]      = r < n ? static_cast<int64_t>(in[r]) : 0;
-    sum += v[i];
+    const int64_t r = wbase + i * 32 + lane;
+    v[i]            = r < n ? static_cast<int64_t>(in[r]) : 0;
   }
-  int64_t tile_total;
-  int64_t excl = block_exclusive_scan<int64_t, kScanThreads>(sum, s_scan, &tile_total);
-  if (threadIdx.x == 0) {
-    s_prefix = lookback_exclusive(status, tile, static_cast<uint64_t>(tile_total), err);
-    if (tile == static_cast<int64_t>(gridDim.x) - 1) *total = static_cast<int64_t>(s_prefix) + tile_total;
+  // exclusive scan of the warp's segment, (i, lane) order
+  int64_t carry = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t x   = v[i];
+    const int64_t inc = warp_inclusive_scan(x);
+    v[i]              = carry + inc - x;
+    carry += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  if (lane == 0) s_warp[warp] = carry;
+  __syncthreads();
+  if (warp == 0) {
+    const int64_t w   = lane < kScanWarps ? s_warp[lane] : 0;
+    const int64_t inc = warp_inclusive_scan(w);
+    if (lane < kScanWarps) s_warp[lane] = inc - w;
+    const int64_t tile_total = __shfl_sync(0xffffffffu, inc, kScanWarps - 1);
+    const uint64_t excl = warp_lookback(status, tile, static_cast<uint64_t>(tile_total), err);
+    if (lane == 0) {
+      s_prefix = excl;
+      if (tile == static_cast<int64_t>(gridDim.x) - 1) *total = static_cast<int64_t>(excl) + tile_total;
+    }
   }
   __syncthreads();
-  int64_t run = static_cast<int64_t>(s_prefix) + excl;
+  const int64_t off = static_cast<int64_t>(s_prefix) + s_warp[warp];
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    int64_t r = base + i;
-    if (r < n) out[r] = run;
-    run += v[i];
+    const int64_t r = wbase + i * 32 + lane;
+    if (r < n) out[r] = off + v[i];
   }
 }
 
