@@ -64,8 +64,19 @@ bool host_resident(const void* p)
 HostStaging::HostStaging(const OpContext& ctx, const ldf_column* table, int ncols, const std::vector<int>& order)
   : s_(ctx.stream()), table_(table, table + ncols), ready_(static_cast<size_t>(ncols), nullptr)
 {
+  try {
+    stage_columns(ctx, order);
+  } catch (...) {
+    release();  // a copy already issued must finish before its buffer is freed
+    throw;
+  }
+}
+
+void HostStaging::stage_columns(const OpContext& ctx, const std::vector<int>& order)
+{
+  const int ncols     = static_cast<int>(table_.size());
   const Allocator& al = ctx.alloc();
-  cudaStream_t cs     = nullptr;
+  cudaStream_t& cs    = cs_;
   for (int c : order) {
     if (c < 0 || c >= ncols || ready_[c] != nullptr) continue;
     ldf_column& col  = table_[c];
@@ -99,14 +110,25 @@ HostStaging::HostStaging(const OpContext& ctx, const ldf_column* table, int ncol
   }
 }
 
-HostStaging::~HostStaging()
+HostStaging::~HostStaging() { release(); }
+
+// The op's stream passes every copy before the staging buffers go back to the
+// allocator (stream-ordered), also when the op failed part way.
+void HostStaging::release() noexcept
 {
-  // the op's stream passes every copy before the staging buffers go back to
-  // the allocator (also when the op failed part way)
-  for (cudaEvent_t e : ready_)
+  if (cs_ != nullptr) {  // every copy issued so far
+    cudaEvent_t done;
+    if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(done, cs_);
+      cudaStreamWaitEvent(s_, done, 0);
+      cudaEventDestroy(done);
+    }
+    cs_ = nullptr;
+  }
+  for (cudaEvent_t& e : ready_)
     if (e != nullptr) {
-      cudaStreamWaitEvent(s_, e, 0);
       cudaEventDestroy(e);
+      e = nullptr;
     }
 }
 

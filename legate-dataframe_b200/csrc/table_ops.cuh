@@ -99,7 +99,11 @@ class HostStaging {
   int64_t staged_bytes() const { return bytes_; }
 
  private:
+  void stage_columns(const OpContext& ctx, const std::vector<int>& order);
+  void release() noexcept;
+
   cudaStream_t s_;
+  cudaStream_t cs_ = nullptr;  // staging stream, once a copy was issued
   std::vector<ldf_column> table_;
   std::vector<cudaEvent_t> ready_;
   std::vector<Buffer<uint8_t>> bufs_;
