@@ -99,52 +99,8 @@ struct GbPlan {
   int* err;
 };
 
-// ---- ordered encodings (min/max) ----------------------------------------
-__device__ __forceinline__ uint64_t ordered_bits(const DCol& c, int64_t r)
-{
-  switch (c.type) {
-    case LDF_INT8: return static_cast<uint64_t>(static_cast<int64_t>(static_cast<const int8_t*>(c.data)[r])) ^ (1ull << 63);
-    case LDF_INT16: return static_cast<uint64_t>(static_cast<int64_t>(static_cast<const int16_t*>(c.data)[r])) ^ (1ull << 63);
-    case LDF_INT32: return static_cast<uint64_t>(static_cast<int64_t>(static_cast<const int32_t*>(c.data)[r])) ^ (1ull << 63);
-    case LDF_INT64:
-    case LDF_TIMESTAMP_US: return static_cast<uint64_t>(static_cast<const int64_t*>(c.data)[r]) ^ (1ull << 63);
-    case LDF_FLOAT32: {
-      uint32_t b = static_cast<const uint32_t*>(c.data)[r];
-      b          = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-      return b;
-    }
-    case LDF_FLOAT64: {
-      uint64_t b = static_cast<const uint64_t*>(c.data)[r];
-      return (b & (1ull << 63)) ? ~b : (b | (1ull << 63));
-    }
-    default: return dbits(c, r);  // unsigned, bool
-  }
-}
-
-// 64-bit ordered value of a <= 4-byte type <-> its 32-bit ordered form (both
-// keep the order; the 64-bit one flips bit 63 for signed integers).
-__device__ __forceinline__ uint64_t narrow_ordered(int type, uint64_t o)
-{
-  switch (type) {
-    case LDF_INT8:
-    case LDF_INT16:
-    case LDF_INT32: return static_cast<uint32_t>(o) ^ 0x80000000u;  // low 32 bits of the sign-extended value
-    default: return o;  // unsigned, bool, float32 are already 32-bit ordered
-  }
-}
-__device__ __forceinline__ uint64_t widen_ordered(int type, uint32_t o32)
-{
-  switch (type) {
-    case LDF_INT8:
-    case LDF_INT16:
-    case LDF_INT32: {
-      const int32_t v = static_cast<int32_t>(o32 ^ 0x80000000u);
-      return static_cast<uint64_t>(static_cast<int64_t>(v)) ^ (1ull << 63);
-    }
-    default: return o32;
-  }
-}
-
+// 32-bit ordered form of a <= 4-byte value -> its 64-bit ordered form (the
+// one the global min/max words hold).
 template <int W, bool SGN, bool FLT>
 __device__ __forceinline__ uint64_t widen32(uint32_t o32)
 {
@@ -1453,8 +1409,6 @@ __global__ void finalize_kernel(FinArgs f)
   }
 }
 
-thread_local cudaStream_t g_column_stream = nullptr;
-
 unsigned gs_blocks(int64_t n, int threads)
 {
   int64_t b   = ceil_div(n, threads);
@@ -1462,18 +1416,15 @@ unsigned gs_blocks(int64_t n, int threads)
   return static_cast<unsigned>(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
-void launch_column(ColArgs& a, int type)
+void launch_column(ColArgs& a, int type, cudaStream_t s)
 {
-  cudaStream_t s = 0;
-  (void)s;
   auto go = [&](auto kernel) {
     LDF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     int occ = 1;
     LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kGbThreads, a.smem_bytes));
     const int64_t blocks = std::min<int64_t>(static_cast<int64_t>(num_sms()) * std::max(occ, 1),
                                              ceil_div(a.n, int64_t(kGbThreads) * kRows));
-    launch("column", kernel, static_cast<unsigned>(blocks), kGbThreads, static_cast<size_t>(a.smem_bytes),
-           g_column_stream, a);
+    launch("column", kernel, static_cast<unsigned>(blocks), kGbThreads, static_cast<size_t>(a.smem_bytes), s, a);
   };
   switch (type) {
     case LDF_BOOL8:
@@ -1504,7 +1455,6 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
   auto wait_plan_col = [&](int ci) { hs.wait(col_of_plan[ci]); };
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
-  g_column_stream     = s;
   const int64_t n     = p.n;
 
   int ndist_col = -1;
@@ -1770,7 +1720,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
         if ((a.states & ST_MAX) && !c.mm64) a.sh_mx = take(4);
         a.smem_bytes = off;
         wait_plan_col(ci);
-        launch_column(a, c.col.type);
+        launch_column(a, c.col.type, s);
       };
       // pass 3: NUNIQUE of one column (after its column pass, which records
       // the value range).  With host-resident inputs it runs right after that
