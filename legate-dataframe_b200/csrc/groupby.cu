@@ -1111,7 +1111,14 @@ __global__ void sample_kernel(KeyCols k, int64_t n_sample, int64_t stride, unsig
       }
     }
     if (g < 0) continue;
-    atomicAdd(&counts[g], 1u);
+    {
+      // lanes of the warp that sampled the same key add once (the most
+      // frequent keys would otherwise serialize on one counter)
+      const uint32_t active = __activemask();
+      const uint32_t peers  = __match_any_sync(active, static_cast<unsigned long long>(g));
+      if ((threadIdx.x & 31) == static_cast<unsigned>(__ffs(peers) - 1))
+        atomicAdd(&counts[g], static_cast<unsigned>(__popc(peers)));
+    }
     if (with_pairs && dvalid(pc.col, r)) {
       uint64_t entry, h;
       if (pc.pair_packed) {
@@ -1166,12 +1173,12 @@ __global__ void freq_stats_kernel(const unsigned int* counts, int64_t n, unsigne
   }
 }
 
-// p[i * stride] = v for i < n
-__global__ void fill_stride_kernel(unsigned long long* p, int64_t n, int stride, unsigned long long v)
+// p[i] = {a, b} for i < n (16-byte stores)
+__global__ void fill_pairs_kernel(ulonglong2* p, int64_t n, unsigned long long a, unsigned long long b)
 {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    p[i * stride] = v;
+    p[i] = make_ulonglong2(a, b);
 }
 
 template <typename T>
@@ -1333,6 +1340,11 @@ __global__ void finalize_kernel(FinArgs f)
       if (d.valid) d.valid[i] = is_null ? 0 : 1;
     }
     const uint64_t call = rec[0];
+    // the exact float sum of a column, rounded once, is shared by its SUM and MEAN
+    int sum_col      = -1;
+    double sum_val   = 0.0;
+    bool sum_special = false;
+    double sum_sval  = 0.0;
     for (int a = 0; a < f.nagg; ++a) {
       const AggOut& o = f.a[a];
       const OCol& d   = o.dst;
@@ -1367,10 +1379,11 @@ __global__ void finalize_kernel(FinArgs f)
             break;
           }
           if (c.fixed) {
-            bool special;
-            double sval;
-            double sv = float_sum(c, crec, 1, id, special, sval);
-            if (special) sv = sval;
+            if (sum_col != o.col) {
+              sum_val = float_sum(c, crec, 1, id, sum_special, sum_sval);
+              sum_col = o.col;
+            }
+            double sv = sum_special ? sum_sval : sum_val;
             if (o.kind == LDF_AGG_MEAN) sv = sv / static_cast<double>(vc);
             store_double(d, i, sv);
           } else {
@@ -1560,10 +1573,11 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     Buffer<unsigned long long> id_key(al, id_cap);
     Buffer<unsigned long long> misc(al, 4);  // id counter, overflow, chunk counter
     Buffer<uint32_t> gid(al, std::max<int64_t>(n, 1));
-    LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, cap * sw * 8, s));
-    if (M == KeyMode::K64)
-      launch("fill_key_words", fill_stride_kernel, gs_blocks(cap, 256), 256, 0, s, slots.get(),
-             static_cast<int64_t>(cap), 2, kSentinel64);
+    if (M == KeyMode::K64)  // empty slot: {sentinel key word, no id}
+      launch("fill_slots", fill_pairs_kernel, gs_blocks(cap, 256), 256, 0, s,
+             reinterpret_cast<ulonglong2*>(slots.get()), static_cast<int64_t>(cap), kSentinel64, kEmpty);
+    else
+      LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, cap * sw * 8, s));
     LDF_CUDA(cudaMemsetAsync(counts.get(), 0, static_cast<size_t>(kIdFirst) * 8, s));  // reserved ids
     const unsigned long long first = kIdFirst;
     LDF_CUDA(cudaMemsetAsync(misc.get(), 0, 32, s));
