@@ -443,6 +443,76 @@ def run_strings_workload(args):
     return 0
 
 
+def run_ingest_workload(args):
+    """--rows (default 20M) rows as a host Arrow table shaped like the string
+    workload (string key from a 2M-entry dictionary, 10% null int64 ts,
+    float32 value) into the device layout: `LogicalTable.from_arrow` (Arrow
+    buffers copied as they are, bitmaps and offsets expanded on the device)
+    against the same conversion done on the host with numpy and then copied;
+    and `parquet_read` of the table written to a local Parquet file against
+    Arrow's Parquet read alone."""
+    import numpy as np
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+    import torch
+
+    from legate_dataframe import LogicalColumn, LogicalTable
+    from legate_dataframe.lib.parquet import parquet_read
+
+    dev = torch.device("cuda", 0)
+    n, nd = args.rows, 2_000_000
+    rng = np.random.default_rng(9)
+    lens = rng.integers(8, 25, nd)
+    alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz0123456789", dtype=np.uint8)
+    chars = alphabet[rng.integers(0, 36, int(lens.sum()))]
+    doff = np.zeros(nd + 1, np.int32)
+    np.cumsum(lens, out=doff[1:])
+    dictionary = pa.StringArray.from_buffers(nd, pa.py_buffer(doff), pa.py_buffer(chars.tobytes()))
+    ranks = np.minimum(rng.zipf(1.5, n), nd) - 1
+    key = pa.DictionaryArray.from_arrays(pa.array(ranks.astype(np.int32)), dictionary).cast(pa.string())
+    ts = pa.array(rng.integers(0, 365 * 86400 * 10**6, n), mask=rng.random(n) < 0.10)
+    val = pa.array(rng.lognormal(size=n).astype(np.float32))
+    t = pa.table({"k": key, "ts": ts, "v": val})
+    arrow_bytes = sum(b.size for c in t.columns for ch in c.chunks for b in ch.buffers() if b is not None)
+
+    def host_then_copy():
+        cols = []
+        for c in t.columns:
+            h = LogicalColumn.from_arrow(c, device=torch.device("cpu"))
+            cols.append(LogicalColumn(h.arrow_type, h.ldf_type, h.size, h.data.to(dev),
+                                      None if h.valid is None else h.valid.to(dev),
+                                      None if h.chars is None else h.chars.to(dev), h.chars_base, h.num_chars))
+        return LogicalTable(cols, t.column_names)
+
+    def timed(fn, steps):
+        fn()
+        torch.cuda.synchronize()
+        best = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            best.append(time.perf_counter() - t0)
+            del r
+        return 1e3 * statistics.median(best)
+
+    steps = max(args.steps, 3)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "t.parquet")
+        pq.write_table(t, path)
+        results = {
+            "from_arrow (device expansion)": timed(lambda: LogicalTable.from_arrow(t), steps),
+            "host numpy conversion + copy": timed(host_then_copy, steps),
+            "parquet_read": timed(lambda: parquet_read(path), steps),
+            "Arrow Parquet read alone (host)": timed(lambda: pq.read_table(path), steps),
+        }
+    for name, ms in results.items():
+        print(json.dumps({"workload": f"ingest {name}: {n} rows", "ms": round(ms, 3), "rows_per_s": n / (ms / 1e3),
+                          "arrow_GBps": arrow_bytes / (ms / 1e3) / 1e9, "arrow_bytes": arrow_bytes,
+                          "timing": "host wall clock, median, device synchronized"}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -456,14 +526,16 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-requests", type=int, default=8192)
     ap.add_argument("--ref-rows", type=int, default=8_000_000, help="rows per step of the reference arm")
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "join", "strings"],
-                    help="groupby = the benchmark line; join / strings print per-op lines")
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "join", "strings", "ingest"],
+                    help="groupby = the benchmark line; join / strings / ingest print per-op lines")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload != "groupby":
-        if args.rows == N_ROWS and args.workload == "strings":
-            args.rows = 100_000_000
+        if args.rows == N_ROWS and args.workload in ("strings", "ingest"):
+            args.rows = 100_000_000 if args.workload == "strings" else 20_000_000
+        if args.workload == "ingest":
+            return run_ingest_workload(args)
         return run_join_workload(args) if args.workload == "join" else run_strings_workload(args)
 
     import torch

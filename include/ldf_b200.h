@@ -179,6 +179,23 @@ int ldf_b200_distinct(const ldf_column* table, int32_t ncols,
                       const int32_t* keys, int32_t nkeys,
                       ldf_column* out, const ldf_allocator* alloc, void* stream);
 
+/* ---- Arrow buffers -> legate layout (on the device) ------------------------ */
+/* An Arrow bitmap (validity, or boolean values) -> one byte per row (1 = bit
+ * set), the legate null-mask / bool layout: out[i] = bit (bit_offset + i) of
+ * `bits` (LSB first).  Device pointers; `bits` holds at least
+ * (bit_offset + n + 7) / 8 bytes.  The converse of bitmask_to_bools
+ * (null_mask.cu:98-113), used on the column copy of
+ * PhysicalColumn::from_arrow (column.cpp:86-122). */
+int ldf_b200_arrow_bits_to_bytes(const uint8_t* bits, int64_t bit_offset, int64_t n,
+                                 uint8_t* out, void* stream);
+/* Arrow string offsets (offset_bytes 4 or 8; n + 1 entries) -> n legate
+ * ranges: ranges[i] = {offsets[i], offsets[i + 1] - 1}, inclusive global
+ * char positions; the chars copied from position offsets[0] on get
+ * chars_base = offsets[0].  Device pointers.  As offsets_to_ranges
+ * (ranges.cu:109-138). */
+int ldf_b200_arrow_offsets_to_ranges(const void* offsets, int32_t offset_bytes, int64_t n,
+                                     ldf_range* ranges, void* stream);
+
 /* ---- hash partition without device allocation ----------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory themselves -- a task body running concurrently with other tasks on the

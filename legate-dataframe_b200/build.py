@@ -32,6 +32,7 @@ SOURCES = [
     "noalloc.cu",
     "batch.cu",
     "distinct.cu",
+    "ingest.cu",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -15,6 +15,8 @@ void hash_partition(const ldf_column* table, int ncols, const int32_t* keys, int
                     ldf_column* out, int64_t* offsets, const OpContext& ctx);
 void distinct(const ldf_column* table, int ncols, const int32_t* keys, int nkeys, ldf_column* out,
               const OpContext& ctx);
+void arrow_bits_to_bytes(const uint8_t* bits, int64_t bit_offset, int64_t n, uint8_t* out, cudaStream_t s);
+void arrow_offsets_to_ranges(const void* offsets, int offset_bytes, int64_t n, ldf_range* out, cudaStream_t s);
 }  // namespace ldf
 
 namespace {
@@ -122,6 +124,19 @@ int ldf_b200_distinct(const ldf_column* table, int32_t ncols, const int32_t* key
     LDF_REQUIRE(out != nullptr || ncols == 0, "null output array");
     ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
     ldf::distinct(table, ncols, keys, nkeys, out, ctx);
+  });
+}
+
+int ldf_b200_arrow_bits_to_bytes(const uint8_t* bits, int64_t bit_offset, int64_t n, uint8_t* out, void* stream)
+{
+  return guarded([&] { ldf::arrow_bits_to_bytes(bits, bit_offset, n, out, static_cast<cudaStream_t>(stream)); });
+}
+
+int ldf_b200_arrow_offsets_to_ranges(const void* offsets, int32_t offset_bytes, int64_t n, ldf_range* ranges,
+                                     void* stream)
+{
+  return guarded([&] {
+    ldf::arrow_offsets_to_ranges(offsets, offset_bytes, n, ranges, static_cast<cudaStream_t>(stream));
   });
 }
 

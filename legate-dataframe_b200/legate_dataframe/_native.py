@@ -141,6 +141,14 @@ def lib():
                 P(ldf_column), P(ctypes.c_int64), ctypes.c_void_p,
             ]
             L.ldf_b200_hash_partition_noalloc.restype = ctypes.c_int
+            L.ldf_b200_arrow_bits_to_bytes.argtypes = [
+                ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+            ]
+            L.ldf_b200_arrow_offsets_to_ranges.argtypes = [
+                ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+            ]
+            L.ldf_b200_arrow_bits_to_bytes.restype = ctypes.c_int
+            L.ldf_b200_arrow_offsets_to_ranges.restype = ctypes.c_int
             L.ldf_b200_launch_count.restype = ctypes.c_ulonglong
             L.ldf_b200_profile_enable.argtypes = [ctypes.c_int]
             L.ldf_b200_profile_report.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int]

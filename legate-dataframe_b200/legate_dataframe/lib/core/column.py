@@ -14,6 +14,7 @@ A column is nullable iff its Arrow source had nulls (core/column.cpp:128).
 from __future__ import annotations
 
 import ctypes
+import warnings
 
 import numpy as np
 import pyarrow as pa
@@ -54,14 +55,25 @@ def ldf_type_of(arrow_type: pa.DataType) -> int:
     raise ValueError(f"unsupported Arrow type for the B200 path: {arrow_type}")
 
 
-def _to_device(arr: np.ndarray, device) -> torch.Tensor:
-    arr = np.ascontiguousarray(arr)
-    if not arr.flags.writeable:
-        arr = arr.copy()
-    t = torch.from_numpy(arr.view(np.uint8).reshape(-1))
-    if t.numel() == 0:
+def _buffer_to_device(buf, start: int, nbytes: int, device) -> torch.Tensor:
+    """Bytes [start, start + nbytes) of an Arrow buffer, copied to the device."""
+    if buf is None or nbytes <= 0:
         return torch.empty(16, dtype=torch.uint8, device=device)
-    return t.to(device, non_blocking=False)
+    host = np.frombuffer(buf, dtype=np.uint8, count=nbytes, offset=start)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")  # read-only view: torch only reads it
+        return torch.from_numpy(host).to(device)
+
+
+def _expand_bits(L, buf, bit_offset: int, n: int, device, stream) -> torch.Tensor:
+    """One byte per row from an Arrow bitmap, expanded on the device."""
+    out = torch.empty(max(n, 1), dtype=torch.uint8, device=device)
+    if n:
+        first = bit_offset >> 3
+        nbytes = ((bit_offset & 7) + n + 7) >> 3
+        bits = _buffer_to_device(buf, first, nbytes, device)
+        N.check(L.ldf_b200_arrow_bits_to_bytes(bits.data_ptr(), bit_offset & 7, n, out.data_ptr(), stream))
+    return out
 
 
 class LogicalColumn:
@@ -80,36 +92,69 @@ class LogicalColumn:
     # ---- construction -------------------------------------------------------
     @staticmethod
     def from_arrow(array, device=None) -> "LogicalColumn":
+        """Copy an Arrow array to the device in the legate layout.  The Arrow
+        buffers are copied as they are (values, the validity bitmap, string
+        offsets and characters) and expanded on the device: the bitmap into
+        one byte per row, the offsets into inclusive ranges (the library's
+        ldf_b200_arrow_bits_to_bytes / ldf_b200_arrow_offsets_to_ranges)."""
         if isinstance(array, pa.ChunkedArray):
             array = array.combine_chunks()
         if device is None:
             device = N.require_cuda()
         t = ldf_type_of(array.type)
         n = len(array)
+        if torch.device(device).type == "cpu":
+            return LogicalColumn._from_arrow_host(array, t, n)
+        off = array.offset
+        bufs = array.buffers()
+        L = N.lib()
+        stream = torch.cuda.current_stream(device).cuda_stream
         valid = None
         if array.null_count > 0:
-            valid = _to_device(np.asarray(array.is_valid(), dtype=np.uint8), device)
+            valid = _expand_bits(L, bufs[0], off, n, device, stream)
+        if t == N.LDF_STRING:
+            ow = 8 if pa.types.is_large_string(array.type) else 4
+            odt = np.int64 if ow == 8 else np.int32
+            host_off = np.frombuffer(bufs[1], dtype=odt, count=n + 1, offset=off * ow) if n else np.zeros(1, odt)
+            base, end = int(host_off[0]), int(host_off[-1])
+            chars = _buffer_to_device(bufs[2], base, end - base, device)
+            ranges = torch.empty(max(n, 1) * 16, dtype=torch.uint8, device=device)
+            if n:
+                d_off = _buffer_to_device(bufs[1], off * ow, (n + 1) * ow, device)
+                N.check(L.ldf_b200_arrow_offsets_to_ranges(d_off.data_ptr(), ow, n, ranges.data_ptr(), stream))
+            return LogicalColumn(array.type, t, n, ranges, valid, chars, base, end - base)
+        if t == N.LDF_BOOL8:
+            data = _expand_bits(L, bufs[1], off, n, device, stream)
+        else:
+            w = N.TYPE_WIDTH[t]
+            data = _buffer_to_device(bufs[1], off * w, n * w, device)
+        return LogicalColumn(array.type, t, n, data, valid)
+
+    @staticmethod
+    def _from_arrow_host(array, t: int, n: int) -> "LogicalColumn":
+        """The same layout in host memory (numpy conversion on the host)."""
+        def host(a: np.ndarray) -> torch.Tensor:
+            a = np.ascontiguousarray(a)
+            return torch.from_numpy(a.view(np.uint8).reshape(-1).copy())
+
+        valid = host(np.asarray(array.is_valid(), dtype=np.uint8)) if array.null_count > 0 else None
         if t == N.LDF_STRING:
             large = pa.types.is_large_string(array.type)
             bufs = array.buffers()
             off = np.frombuffer(bufs[1], dtype=np.int64 if large else np.int32)[array.offset : array.offset + n + 1]
-            off = off.astype(np.int64)
-            chars_np = np.frombuffer(bufs[2], dtype=np.uint8) if bufs[2] is not None else np.zeros(0, np.uint8)
-            base = int(off[0]) if n else 0
-            chars_np = chars_np[base : int(off[-1]) if n else base]
+            off = off.astype(np.int64) if n else np.zeros(1, np.int64)
+            base, end = int(off[0]), int(off[-1])
+            chars = np.frombuffer(bufs[2], dtype=np.uint8)[base:end] if bufs[2] is not None else np.zeros(0, np.uint8)
             ranges = np.empty((n, 2), dtype=np.int64)
             ranges[:, 0] = off[:-1]
             ranges[:, 1] = off[1:] - 1
-            return LogicalColumn(array.type, t, n, _to_device(ranges, device), valid,
-                                 _to_device(chars_np, device), base, len(chars_np))
+            return LogicalColumn(array.type, t, n, host(ranges), valid, host(chars), base, end - base)
         if t == N.LDF_BOOL8:
             vals = np.asarray(array.fill_null(False).to_numpy(zero_copy_only=False), dtype=np.uint8)
         else:
-            storage = array
-            if not (array.type in _FIXED):
-                storage = array.view(pa.int32() if t == N.LDF_INT32 else pa.int64())
+            storage = array if array.type in _FIXED else array.view(pa.int32() if t == N.LDF_INT32 else pa.int64())
             vals = np.asarray(storage.fill_null(0).to_numpy(zero_copy_only=False)).astype(_NP_OF_LDF[t], copy=False)
-        return LogicalColumn(array.type, t, n, _to_device(vals, device), valid)
+        return LogicalColumn(array.type, t, n, host(vals), valid)
 
     @staticmethod
     def from_torch(data: torch.Tensor, arrow_type, valid: torch.Tensor | None = None) -> "LogicalColumn":

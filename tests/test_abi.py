@@ -132,3 +132,11 @@ def test_python_distinct_argument_errors():
         distinct(tbl, [])
     with pytest.raises(IndexError):
         distinct(tbl, ["nope"])
+
+
+def test_arrow_conversion_argument_errors_without_gpu():
+    L = N.lib()
+    assert L.ldf_b200_arrow_offsets_to_ranges(None, 3, 4, None, None) == N.LDF_ERR_INVALID_ARGUMENT
+    assert b"4 or 8 bytes" in L.ldf_b200_last_error()
+    assert L.ldf_b200_arrow_bits_to_bytes(None, 0, -1, None, None) == N.LDF_ERR_INVALID_ARGUMENT
+    assert L.ldf_b200_arrow_bits_to_bytes(None, 0, 0, None, None) == N.LDF_OK  # nothing to do
