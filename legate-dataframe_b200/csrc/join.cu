@@ -82,7 +82,32 @@ struct BuildTable {
   const uint64_t* part_base;
   const uint64_t* part_cap;
   int* dup;  // K32: set by the build when a key occurs twice
+  // Dense integer keys (K32/K64): direct[key - dmin] = the build row with
+  // that key (-1 none) for the drange values from dmin on, instead of slots.
+  const int32_t* direct;
+  int64_t dmin, dmax;
+  uint64_t drange;
 };
+
+// Slot of key value k in a direct-address table, or drange when k is outside
+// [dmin, dmax] (compared as values, so no wrap-around can alias a slot).
+__device__ __forceinline__ uint64_t direct_slot(const BuildTable& t, int64_t k)
+{
+  return (k >= t.dmin && k <= t.dmax) ? static_cast<uint64_t>(k - t.dmin) : t.drange;
+}
+
+// Integer value of a single fixed-width key (sign-extended for signed types).
+__device__ __forceinline__ int64_t key_value(const DCol& c, int64_t r)
+{
+  switch (c.type) {
+    case LDF_INT8: return static_cast<const int8_t*>(c.data)[r];
+    case LDF_INT16: return static_cast<const int16_t*>(c.data)[r];
+    case LDF_INT32: return static_cast<const int32_t*>(c.data)[r];
+    case LDF_INT64:
+    case LDF_TIMESTAMP_US: return static_cast<const int64_t*>(c.data)[r];
+    default: return static_cast<int64_t>(dbits(c, r));  // unsigned, bool
+  }
+}
 
 // First slot and slot range [lo, hi) of hash h.
 __device__ __forceinline__ uint64_t first_slot(const BuildTable& t, uint64_t h, uint64_t& lo, uint64_t& hi)
@@ -142,6 +167,44 @@ __global__ void build_kernel(BuildTable t, int64_t n)
   }
 }
 
+// Range of the valid build keys' values: mm[0] = min, mm[1] = max (as
+// order-preserving unsigned words), mm[2] = 1 when an unsigned 64-bit key
+// does not fit int64.
+__global__ void key_range_kernel(DCol key, int64_t n, unsigned long long* mm)
+{
+  unsigned long long lo = ~0ull, hi = 0;
+  int wide              = 0;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    if (!dvalid(key, r)) continue;
+    const int64_t v = key_value(key, r);
+    if (key.type == LDF_UINT64 && v < 0) wide = 1;
+    const unsigned long long o = static_cast<unsigned long long>(v) ^ (1ull << 63);
+    lo                         = o < lo ? o : lo;
+    hi                         = o > hi ? o : hi;
+  }
+  for (int d = 16; d > 0; d >>= 1) {
+    const unsigned long long l2 = __shfl_xor_sync(0xffffffffu, lo, d), h2 = __shfl_xor_sync(0xffffffffu, hi, d);
+    lo                          = l2 < lo ? l2 : lo;
+    hi                          = h2 > hi ? h2 : hi;
+  }
+  wide = __any_sync(0xffffffffu, wide);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(mm, lo);
+    atomicMax(mm + 1, hi);
+    if (wide) atomicExch(mm + 2, 1ull);
+  }
+}
+
+// Direct-address build: a second row with the same key sets *dup.
+__global__ void direct_build_kernel(DCol key, int64_t n, int64_t dmin, int32_t* direct, int* dup)
+{
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    if (!dvalid(key, r)) continue;  // null rows: null list or excluded
+    const uint64_t u = static_cast<uint64_t>(key_value(key, r) - dmin);  // every valid key lies in [dmin, dmax]
+    if (atomicCAS(direct + u, -1, static_cast<int32_t>(r)) != -1) *dup = 1;
+  }
+}
+
 // Enumerate the build rows matching probe row r of `pk`; f(build_row) returns
 // false to stop early.
 template <KeyMode M, typename F>
@@ -154,6 +217,14 @@ __device__ __forceinline__ void for_each_match(const BuildTable& t, const KeyCol
       int64_t nn = *t.null_count;
       for (int64_t i = 0; i < nn; ++i)
         if (!f(static_cast<int64_t>(t.null_list[i]))) return;
+    }
+    return;
+  }
+  if (M != KeyMode::GEN && t.direct) {
+    const uint64_t u = direct_slot(t, key_value(pk.c[0], r));
+    if (u < t.drange) {
+      const int32_t br = __ldg(t.direct + u);
+      if (br >= 0) f(static_cast<int64_t>(br));
     }
     return;
   }
@@ -332,11 +403,17 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a)
     for (int i = 0; i < kProbeItems; ++i) {
       const int64_t r = base + i * kProbeThreads + threadIdx.x;
       if (r < a.n_probe && dvalid(a.pk.c[0], r)) {
-        uint64_t lo, hi;
-        const uint64_t idx = first_slot(a.t, mix64(key_bits<M>(a.pk, r)), lo, hi);
-        const unsigned long long* p =
-          M == KeyMode::K64 ? reinterpret_cast<const unsigned long long*>(static_cast<const Slot16*>(a.t.slots) + idx)
-                            : reinterpret_cast<const unsigned long long*>(a.t.slots) + idx;
+        const void* p;
+        if (a.t.direct) {
+          const uint64_t u = direct_slot(a.t, key_value(a.pk.c[0], r));
+          if (u >= a.t.drange) continue;
+          p = a.t.direct + u;
+        } else {
+          uint64_t lo, hi;
+          const uint64_t idx = first_slot(a.t, mix64(key_bits<M>(a.pk, r)), lo, hi);
+          p = M == KeyMode::K64 ? static_cast<const void*>(static_cast<const Slot16*>(a.t.slots) + idx)
+                                : static_cast<const void*>(static_cast<const uint64_t*>(a.t.slots) + idx);
+        }
         asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
       }
     }
@@ -764,10 +841,49 @@ void run_join(const OpContext& ctx, const KeyCols& pk, int64_t n_probe, const Ke
     t.part_cap  = plan->cap;
     t.cap       = plan->total;
   }
+  // Dense integer keys: when the build keys' value range is at most twice the
+  // build rows (and 2^31), a direct-address table of build rows replaces the
+  // hash table if no key repeats (a repeat falls back to the hash table).
+  // The table is 4 bytes per key value, so the probe's lookups mostly stay in
+  // L2, and probe keys outside the range need no lookup at all.
+  Buffer<int32_t> direct;
+  if (M != KeyMode::GEN && !plan && n_build > 0 && !is_float(bk.c[0].type)) {
+    Buffer<unsigned long long> mm(al, 4);
+    const unsigned long long init[4] = {~0ull, 0ull, 0ull, 0ull};
+    LDF_CUDA(cudaMemcpyAsync(mm.get(), init, sizeof(init), cudaMemcpyHostToDevice, s));
+    launch("key_range", key_range_kernel, grid_stride_blocks(n_build, 256), 256, 0, s, bk.c[0], n_build, mm.get());
+    unsigned long long h[3];
+    LDF_CUDA(cudaMemcpyAsync(h, mm.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    ctx.finish();
+    const uint64_t span  = h[0] <= h[1] ? (h[1] - h[0]) : ~0ull;  // max - min (order-preserving words)
+    const uint64_t limit = static_cast<uint64_t>(std::max<int64_t>(2 * n_build, int64_t(1) << 16));
+    if (h[2] == 0 && span < limit && span < (uint64_t(1) << 31)) {
+      const int64_t dmin = static_cast<int64_t>(h[0] ^ (1ull << 63));
+      direct             = Buffer<int32_t>(al, span + 1);
+      LDF_CUDA(cudaMemsetAsync(direct.get(), 0xff, (span + 1) * sizeof(int32_t), s));
+      LDF_CUDA(cudaMemsetAsync(mm.get() + 3, 0, sizeof(unsigned long long), s));
+      launch("direct_build", direct_build_kernel, grid_stride_blocks(n_build, 256), 256, 0, s, bk.c[0], n_build,
+             dmin, direct.get(), reinterpret_cast<int*>(mm.get() + 3));
+      unsigned long long dup = 0;
+      LDF_CUDA(cudaMemcpyAsync(&dup, mm.get() + 3, sizeof(dup), cudaMemcpyDeviceToHost, s));
+      ctx.finish();
+      if (dup == 0) {
+        t.direct = direct.get();
+        t.dmin   = dmin;
+        t.dmax   = static_cast<int64_t>(h[1] ^ (1ull << 63));
+        t.drange = span + 1;
+      } else {
+        direct.reset();
+      }
+    }
+  }
   const size_t slot_bytes = M == KeyMode::K64 ? sizeof(Slot16) : sizeof(uint64_t);
-  Buffer<uint8_t> slots(al, t.cap * slot_bytes);
-  LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, t.cap * slot_bytes, s));
-  t.slots = slots.get();
+  Buffer<uint8_t> slots;
+  if (t.direct == nullptr) {
+    slots = Buffer<uint8_t>(al, t.cap * slot_bytes);
+    LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, t.cap * slot_bytes, s));
+    t.slots = slots.get();
+  }
 
   Buffer<int32_t> null_list;
   Buffer<int64_t> null_count;
@@ -784,19 +900,21 @@ void run_join(const OpContext& ctx, const KeyCols& pk, int64_t n_probe, const Ke
   }
   // K32 builds flag duplicate keys themselves (the slot word holds the key)
   Buffer<int64_t> dupflag;
-  if (M == KeyMode::K32) {
+  if (M == KeyMode::K32 && t.direct == nullptr) {
     dupflag = Buffer<int64_t>(al, 1);
     LDF_CUDA(cudaMemsetAsync(dupflag.get(), 0, sizeof(int64_t), s));
     t.dup = reinterpret_cast<int*>(dupflag.get());
   }
-  if (n_build > 0) {
+  if (n_build > 0 && t.direct == nullptr) {
     launch("build", build_kernel<M>, grid_stride_blocks(n_build, 256), 256, 0, s, t, n_build);
     LDF_CHECK_LAUNCH();
   }
 
   // ---- uniqueness ----------------------------------------------------------
   bool unique = true;
-  if (M == KeyMode::K32 && n_build > 1) {
+  if (t.direct != nullptr) {  // no key repeats; null keys match each other with nulls_equal
+    if (t.null_count) unique = ctx.read_i64(t.null_count) <= 1;
+  } else if (M == KeyMode::K32 && n_build > 1) {
     int64_t h[2] = {0, 0};  // duplicate flag, null-key rows (all equal with nulls_equal)
     LDF_CUDA(cudaMemcpyAsync(&h[0], dupflag.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     if (t.null_count) LDF_CUDA(cudaMemcpyAsync(&h[1], t.null_count, sizeof(int64_t), cudaMemcpyDeviceToHost, s));

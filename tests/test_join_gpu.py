@@ -232,3 +232,47 @@ def test_join_radix_partitioned_edges(how, monkeypatch):
     rhs = pa.table({"kr": pa.array([None, 1, None], pa.int32()), "w": np.arange(3)})
     for ne in (True, False):
         assert_tables_equal(run_join(lhs, rhs, ["k"], ["kr"], how, ne), R.join(lhs, rhs, ["k"], ["kr"], how, ne))
+
+
+@pytest.mark.parametrize("how", ["inner", "left", "full", "semi", "anti"])
+@pytest.mark.parametrize("case", ["dense_perm", "dense_gaps", "dense_dup", "dense_nulls", "dense_two_nulls",
+                                  "int64_edges", "uint64_high", "int8_negative"])
+def test_join_dense_integer_keys(how, case):
+    """Build keys whose value range is at most twice the build rows take a
+    direct-address table (a repeated key falls back to the hash table).  Probe
+    keys outside the range, at the int64 extremes (where a subtraction would
+    wrap around), nulls on either side, and unsigned keys above 2^63."""
+    rng = np.random.default_rng(zlib.crc32(f"{how}{case}".encode()))
+    nb, nl = 5000, 12000
+    i64 = np.iinfo(np.int64)
+    if case == "dense_perm":
+        bk = pa.array(rng.permutation(nb) - 1000)
+        lk = pa.array(rng.integers(-3000, 6000, nl))
+    elif case == "dense_gaps":
+        bk = pa.array(rng.choice(2 * nb - 10, nb, replace=False) + 7)
+        lk = pa.array(rng.integers(0, 2 * nb + 20, nl))
+    elif case == "dense_dup":
+        bk = pa.array(np.concatenate([np.arange(nb - 1), [17]]))
+        lk = pa.array(rng.integers(-5, nb + 5, nl))
+    elif case in ("dense_nulls", "dense_two_nulls"):
+        m = np.zeros(nb, bool)
+        m[[3] if case == "dense_nulls" else [3, 4000]] = True
+        bk = pa.array(rng.permutation(nb), mask=m)
+        lk = pa.array(rng.integers(0, nb + 100, nl), mask=rng.random(nl) < 0.1)
+    elif case == "int64_edges":
+        bk = pa.array(i64.max - rng.permutation(nb))
+        lk = pa.array(np.concatenate([i64.min + rng.integers(0, 3 * nb, nl // 2),
+                                      i64.max - rng.integers(0, 2 * nb, nl - nl // 2)]))
+    elif case == "uint64_high":
+        bk = pa.array((np.uint64(2**63) + rng.permutation(nb).astype(np.uint64)))
+        lk = pa.array((np.uint64(2**63) + rng.integers(0, 2 * nb, nl).astype(np.uint64)))
+    else:  # int8_negative: every value of int8, twice (a repeat: hash table)
+        bk = pa.array(np.tile(np.arange(-128, 128, dtype=np.int8), 2))
+        lk = pa.array(rng.integers(-128, 128, nl).astype(np.int8))
+    rhs = pa.table({"rk": bk, "rv": np.arange(len(bk), dtype=np.int64), "rw": rng.normal(size=len(bk))})
+    lhs = pa.table({"lk": lk, "lv": np.arange(len(lk), dtype=np.int32)})
+    ro = None if how in ("semi", "anti") else ["rk", "rv", "rw"]
+    for nulls_equal in (True, False):
+        res = run_join(lhs, rhs, ["lk"], ["rk"], how, nulls_equal, ro=ro)
+        exp = R.join(lhs, rhs, ["lk"], ["rk"], how, nulls_equal, rhs_out=ro)
+        assert_tables_equal(res, exp)
