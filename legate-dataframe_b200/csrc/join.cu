@@ -321,6 +321,13 @@ struct ProbeArgs {
   uint32_t* tile_counts;        // count pass output
   const int64_t* tile_offsets;  // write pass with known offsets (null -> claim with an atomic)
   int64_t* total;  // device: number of rows written by the probe
+  // Build-side outputs.  rkey: the column of `ro` that is the build key
+  // (-1 none): a matched row takes it from its own probe key, which is equal.
+  // rpack: two other columns (ro indices pcol[0], pcol[1]) packed per build
+  // row as two 8-byte words, read with one 16-byte load (null: none packed).
+  int rkey;
+  const ulonglong2* rpack;
+  int pcol[2];
   int* err;
 };
 
@@ -364,6 +371,59 @@ __device__ __forceinline__ void emit_column_batch(const DCol& src, const OCol& d
     if (pos[i] < 0) continue;
     store_w<W>(d.data, pos[i], v[i]);
     if (d.valid) d.valid[pos[i]] = ok[i] ? 1 : 0;
+  }
+}
+
+// One output column of `o` from source rows row[i] (see emit_column_batch).
+__device__ __forceinline__ void emit_one(const DCol& src, const OCol& d, const int64_t* pos, const int64_t* row)
+{
+  switch (d.width) {
+    case 1: emit_column_batch<1>(src, d, pos, row); break;
+    case 2: emit_column_batch<2>(src, d, pos, row); break;
+    case 4: emit_column_batch<4>(src, d, pos, row); break;
+    default: emit_column_batch<8>(src, d, pos, row); break;
+  }
+}
+
+// Build-side output columns of the thread's items (brow[i] < 0: no match).
+__device__ __forceinline__ void emit_build_batch(const ProbeArgs& a, const int64_t* pos, const int64_t* lrow,
+                                                 const int64_t* brow)
+{
+  const OutSpec& o = a.ro;
+  if (a.rpack) {
+    ulonglong2 w[kProbeItems];
+#pragma unroll
+    for (int i = 0; i < kProbeItems; ++i)
+      w[i] = (pos[i] >= 0 && brow[i] >= 0) ? __ldg(a.rpack + brow[i]) : make_ulonglong2(0, 0);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const OCol& d = o.dst[a.pcol[q]];
+#pragma unroll
+      for (int i = 0; i < kProbeItems; ++i) {
+        if (pos[i] < 0) continue;
+        const uint64_t v = q == 0 ? w[i].x : w[i].y;
+        switch (d.width) {
+          case 1: store_w<1>(d.data, pos[i], v); break;
+          case 2: store_w<2>(d.data, pos[i], v); break;
+          case 4: store_w<4>(d.data, pos[i], v); break;
+          default: store_w<8>(d.data, pos[i], v); break;
+        }
+        if (d.valid) d.valid[pos[i]] = brow[i] >= 0 ? 1 : 0;
+      }
+    }
+  }
+  for (int j = 0; j < o.n; ++j) {
+    if (a.rpack && (j == a.pcol[0] || j == a.pcol[1])) continue;
+    if (j == a.rkey) {
+      // the probe key of a matched row (its validity too: null keys match
+      // only null keys)
+      int64_t krow[kProbeItems];
+#pragma unroll
+      for (int i = 0; i < kProbeItems; ++i) krow[i] = brow[i] >= 0 ? lrow[i] : -1;
+      emit_one(a.pk.c[0], o.dst[j], pos, krow);
+    } else {
+      emit_one(o.src[j], o.dst[j], pos, brow);
+    }
   }
 }
 
@@ -476,7 +536,7 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a)
       if (out) opos[i] = pos++;
     }
     emit_batch(a.lo, opos, lrow);
-    emit_batch(a.ro, opos, brow);
+    emit_build_batch(a, opos, lrow, brow);
     return;
   }
 #pragma unroll
@@ -505,6 +565,25 @@ __global__ void __launch_bounds__(kProbeThreads) probe_kernel(ProbeArgs a)
         return true;
       });
     }
+  }
+}
+
+// Two build-side output columns packed per row (see ProbeArgs::rpack).
+template <int W0, int W1>
+__global__ void pack_rows_kernel(DCol c0, DCol c1, int64_t n, ulonglong2* out)
+{
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x)
+    out[b] = make_ulonglong2(load_w<W0>(c0.data, b), load_w<W1>(c1.data, b));
+}
+
+template <int W0>
+void launch_pack(const DCol& c0, const DCol& c1, int64_t n, ulonglong2* out, cudaStream_t s, unsigned grid)
+{
+  switch (c1.width) {
+    case 1: launch("pack_rows", pack_rows_kernel<W0, 1>, grid, 256, 0, s, c0, c1, n, out); break;
+    case 2: launch("pack_rows", pack_rows_kernel<W0, 2>, grid, 256, 0, s, c0, c1, n, out); break;
+    case 4: launch("pack_rows", pack_rows_kernel<W0, 4>, grid, 256, 0, s, c0, c1, n, out); break;
+    default: launch("pack_rows", pack_rows_kernel<W0, 8>, grid, 256, 0, s, c0, c1, n, out); break;
   }
 }
 
@@ -990,6 +1069,37 @@ void run_join(const OpContext& ctx, const KeyCols& pk, int64_t n_probe, const Ke
     matched = Buffer<uint8_t>(al, n_build);
     LDF_CUDA(cudaMemsetAsync(matched.get(), 0, n_build, s));
     a.matched = matched.get();
+  }
+
+  // Build-side outputs of the one-pass probe: the build key column comes from
+  // the probe key, and two other non-nullable fixed-width columns are packed
+  // into one 16-byte record per build row, so a matched probe row reads them
+  // with one random access.
+  a.rkey = -1;
+  Buffer<ulonglong2> rpack;
+  if (unique && M != KeyMode::GEN && !need_maps && tiles > 0 && n_build > 0) {
+    std::vector<int> rest;
+    for (int j = 0; j < ro.n; ++j) {
+      if (a.rkey < 0 && ro.src[j].data == bk.c[0].data && ro.src[j].type == bk.c[0].type) a.rkey = j;
+      else rest.push_back(j);
+    }
+    bool packable = rest.size() == 2;
+    for (int j : rest) packable = packable && ro.src[j].valid == nullptr && ro.src[j].type != LDF_STRING;
+    if (packable) {
+      const DCol& c0 = ro.src[rest[0]];
+      const DCol& c1 = ro.src[rest[1]];
+      rpack          = Buffer<ulonglong2>(al, n_build);
+      const unsigned g = grid_stride_blocks(n_build, 256);
+      switch (c0.width) {
+        case 1: launch_pack<1>(c0, c1, n_build, rpack.get(), s, g); break;
+        case 2: launch_pack<2>(c0, c1, n_build, rpack.get(), s, g); break;
+        case 4: launch_pack<4>(c0, c1, n_build, rpack.get(), s, g); break;
+        default: launch_pack<8>(c0, c1, n_build, rpack.get(), s, g); break;
+      }
+      a.rpack   = rpack.get();
+      a.pcol[0] = rest[0];
+      a.pcol[1] = rest[1];
+    }
   }
 
   if (tiles > 0) {
