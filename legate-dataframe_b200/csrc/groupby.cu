@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(kGbThreads) assign_kernel(GbPlan p, uint32_t* 
   __syncthreads();
   IdPool pool{0, 0};
   constexpr int R          = assign_rows<M>();
-  constexpr int64_t kChunk = 32 * R * 32;  // rows per dynamically scheduled chunk
+  constexpr int64_t kChunk = 32 * R * 8;  // rows per dynamically scheduled chunk
   for (;;) {
     unsigned long long chunk = 0;
     if (lane_id() == 0) chunk = atomicAdd(p.chunk_counter, 1ull);
