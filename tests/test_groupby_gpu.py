@@ -5,6 +5,8 @@ the shared-memory pre-aggregation, the sampled-estimate path and overflow
 retry.  Integer aggregates and NUNIQUE bit-exact; float SUM/MEAN within 1e-12
 relative of the Neumaier oracle."""
 
+import zlib
+
 import numpy as np
 import pyarrow as pa
 import pyarrow.compute as pc
@@ -260,3 +262,36 @@ def test_groupby_host_resident_inputs(key_kind, pinned):
     for _ in range(2):
         res = groupby_aggregation(host, ["k"], ALL_AGGS).to_arrow()
         assert_tables_equal(res, exp, sort_by=["k"])
+
+
+@pytest.mark.parametrize("vkind", ["int32_neg", "int8", "int16", "uint8", "uint32", "bool"])
+@pytest.mark.parametrize("other", [False, True])
+def test_groupby_nunique_with_min_max(vkind, other):
+    """MIN / MAX / COUNT beside NUNIQUE on one column, with and without
+    another aggregated column; ranks below and above the shared-memory hot
+    limits of the column and NUNIQUE kernels are both present."""
+    rng = np.random.default_rng(zlib.crc32(f"{vkind}{other}".encode()))
+    n = 400_000
+    ranks = np.minimum(rng.zipf(1.1, n), 30000) - 1
+    k = rng.permutation(30000)[ranks].astype(np.int64)
+    mask = rng.random(n) < 0.1
+    if vkind == "int32_neg":
+        v = pa.array(rng.integers(-3000, 2000, n).astype(np.int32), mask=mask)
+    elif vkind == "int8":
+        v = pa.array(rng.integers(-128, 128, n).astype(np.int8), mask=mask)
+    elif vkind == "int16":
+        v = pa.array(rng.integers(-30000, 30000, n).astype(np.int16))
+    elif vkind == "uint8":
+        v = pa.array(rng.integers(0, 256, n).astype(np.uint8), mask=mask)
+    elif vkind == "uint32":
+        v = pa.array(rng.integers(4_000_000_000, 4_000_100_000, n).astype(np.uint32))
+    else:
+        v = pa.array(rng.random(n) < 0.3, mask=mask)
+    t = pa.table({"k": k, "v": v, "w": rng.normal(size=n)})
+    aggs = [("v", "count_distinct", "nd"), ("v", "min", "mn"), ("v", "max", "mx"), ("v", "count", "c"),
+            ("v", ("count_distinct", pc.CountOptions(mode="all")), "nda")]
+    if other:
+        aggs.append(("w", "sum", "ws"))
+    res = run_groupby(t, ["k"], aggs)
+    exp = R.groupby(t, ["k"], aggs)
+    assert_tables_equal(res, exp, sort_by=["k"], rtol=RTOL)
