@@ -27,13 +27,16 @@ namespace {
 constexpr uint64_t kEmpty = ~0ull;
 
 // ---- string ranking --------------------------------------------------------
-__global__ void str_find_insert_kernel(DCol col, int64_t n, unsigned long long* slots, uint64_t cap,
+// Slot of each string (rows r = i * stride, i < n) in the dedupe table;
+// row_slot[i] = -1 for a null row.
+__global__ void str_find_insert_kernel(DCol col, int64_t n, int64_t stride, unsigned long long* slots, uint64_t cap,
                                        int32_t* row_slot, int* overflow)
 {
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
-       r += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i * stride;
     if (!dvalid(col, r)) {
-      row_slot[r] = -1;
+      row_slot[i] = -1;
       continue;
     }
     const uint64_t h     = hash_value(col, r);  // valid row: hash_bytes of the string
@@ -57,21 +60,64 @@ __global__ void str_find_insert_kernel(DCol col, int64_t n, unsigned long long* 
       idx = idx + 1 == cap ? 0 : idx + 1;
     }
     if (found < 0) atomicExch(overflow, 1);
-    row_slot[r] = static_cast<int32_t>(found);
+    row_slot[i] = static_cast<int32_t>(found);
   }
 }
 
-// slot -> dense distinct id; distinct id -> representative row
+// Occurrences per slot of a sample (lanes of a warp on the same slot add once:
+// frequent strings would serialize on one counter).
+__global__ void slot_count_kernel(const int32_t* row_slot, int64_t n, unsigned int* count)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sl = row_slot[i];
+    if (sl < 0) continue;
+    const uint32_t peers = __match_any_sync(__activemask(), sl);
+    if ((threadIdx.x & 31) == static_cast<unsigned>(__ffs(peers) - 1))
+      atomicAdd(count + sl, static_cast<unsigned>(__popc(peers)));
+  }
+}
+
+// out[0] += slots seen, out[1] += slots seen once.
+__global__ void distinct_stats_kernel(const unsigned int* count, int64_t cap, unsigned long long* out)
+{
+  unsigned long long d = 0, f1 = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cap; i += (int64_t)gridDim.x * blockDim.x) {
+    d += count[i] != 0;
+    f1 += count[i] == 1;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    d += __shfl_xor_sync(0xffffffffu, d, o);
+    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, d);
+    atomicAdd(out + 1, f1);
+  }
+}
+
+// slot -> dense distinct id; distinct id -> representative row.  The
+// occupied slots of a warp take their ids with one atomic (order is
+// irrelevant: the ids get sorted).
 __global__ void str_compact_kernel(const unsigned long long* slots, uint64_t cap, int32_t* slot_id,
                                    int32_t* repr, unsigned long long* count)
 {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < static_cast<int64_t>(cap);
-       i += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t v = slots[i];
-    if (v == kEmpty) continue;
-    unsigned long long d = atomicAdd(count, 1ull);  // order is irrelevant: ids get sorted
-    slot_id[i]           = static_cast<int32_t>(d);
-    repr[d]              = static_cast<int32_t>(v >> 32);
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  // every lane of a warp runs the same number of iterations (ballots below)
+  for (int64_t base = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); base < static_cast<int64_t>(cap);
+       base += stride) {
+    const int64_t i       = base + lane;
+    const uint64_t v      = i < static_cast<int64_t>(cap) ? slots[i] : kEmpty;
+    const bool used       = v != kEmpty;
+    const uint32_t ballot = __ballot_sync(0xffffffffu, used);
+    if (ballot == 0) continue;
+    unsigned long long first = 0;
+    if (lane == 0) first = atomicAdd(count, static_cast<unsigned long long>(__popc(ballot)));
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (!used) continue;
+    const unsigned long long d = first + __popc(ballot & ((1u << lane) - 1u));
+    slot_id[i]                 = static_cast<int32_t>(d);
+    repr[d]                    = static_cast<int32_t>(v >> 32);
   }
 }
 
@@ -173,26 +219,63 @@ void string_ranks(const OpContext& ctx, const DCol& col, int64_t n, uint32_t* ou
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
   if (n == 0) return;
-  uint64_t cap = static_cast<uint64_t>(2 * n + 64);
-  Buffer<unsigned long long> slots(al, cap);
+  // Dedupe table size from a strided sample of 2^20 rows: distinct strings
+  // estimated by GEE (Charikar et al. 2000), taken x8 because it
+  // underestimates heavy tails; a table too small for the real count
+  // overflows and the pass is redone with room for every row.
+  uint64_t cap          = static_cast<uint64_t>(2 * n + 64);
+  const int64_t kSample = int64_t(1) << 20;
+  if (n > 4 * kSample) {
+    const int64_t stride = n / kSample;
+    const uint64_t scap  = static_cast<uint64_t>(2 * kSample + 64);
+    Buffer<unsigned long long> sslots(al, scap);
+    Buffer<int32_t> sslot(al, kSample);
+    Buffer<unsigned int> scount(al, scap);
+    Buffer<unsigned long long> sm(al, 4);
+    LDF_CUDA(cudaMemsetAsync(sslots.get(), 0xff, scap * 8, s));
+    LDF_CUDA(cudaMemsetAsync(scount.get(), 0, scap * 4, s));
+    LDF_CUDA(cudaMemsetAsync(sm.get(), 0, 32, s));
+    launch("str_find_insert", str_find_insert_kernel, blocks_for(kSample), 256, 0, s, col, kSample, stride,
+           sslots.get(), scap, sslot.get(), reinterpret_cast<int*>(sm.get() + 2));
+    launch("slot_count", slot_count_kernel, blocks_for(kSample), 256, 0, s, static_cast<const int32_t*>(sslot.get()),
+           kSample, scount.get());
+    launch("distinct_stats", distinct_stats_kernel, blocks_for(static_cast<int64_t>(scap)), 256, 0, s,
+           static_cast<const unsigned int*>(scount.get()), static_cast<int64_t>(scap), sm.get());
+    unsigned long long h[3];
+    LDF_CUDA(cudaMemcpyAsync(h, sm.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    ctx.finish();
+    if (h[2] == 0) {
+      const double est = std::sqrt(static_cast<double>(n) / kSample) * static_cast<double>(h[1]) +
+                         static_cast<double>(h[0] - h[1]);
+      const int64_t groups = std::min<int64_t>(n, static_cast<int64_t>(8 * est) + 1024);
+      cap                  = static_cast<uint64_t>(2 * groups + 64);
+    }
+  }
   Buffer<int32_t> row_slot(al, n);
   Buffer<int64_t> misc(al, 4);
-  LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, cap * 8, s));
-  LDF_CUDA(cudaMemsetAsync(misc.get(), 0, 32, s));
+  Buffer<unsigned long long> slots;
   int* overflow              = reinterpret_cast<int*>(misc.get());
   unsigned long long* dcount = reinterpret_cast<unsigned long long*>(misc.get() + 1);
   unsigned long long* maxlen = reinterpret_cast<unsigned long long*>(misc.get() + 2);
-  launch("str_find_insert", str_find_insert_kernel, blocks_for(n), 256, 0, s, col, n, slots.get(), cap, row_slot.get(), overflow);
-  LDF_CHECK_LAUNCH();
+  for (int attempt = 0;; ++attempt) {
+    slots = Buffer<unsigned long long>(al, cap);
+    LDF_CUDA(cudaMemsetAsync(slots.get(), 0xff, cap * 8, s));
+    LDF_CUDA(cudaMemsetAsync(misc.get(), 0, 32, s));
+    launch("str_find_insert", str_find_insert_kernel, blocks_for(n), 256, 0, s, col, n, int64_t(1), slots.get(), cap,
+           row_slot.get(), overflow);
+    int ov = 0;
+    LDF_CUDA(cudaMemcpyAsync(&ov, overflow, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ctx.finish();
+    if (ov == 0) break;
+    const uint64_t full = static_cast<uint64_t>(2 * n + 64);
+    if (attempt > 0 || cap >= full) fail(LDF_ERR_INTERNAL, "string dictionary overflow");
+    cap = full;  // the estimate was too low: room for every row
+  }
   Buffer<int32_t> slot_id(al, cap);
   Buffer<int32_t> repr(al, n);
   launch("str_compact", str_compact_kernel, blocks_for(cap), 256, 0, s, slots.get(), cap, slot_id.get(), repr.get(), dcount);
   LDF_CHECK_LAUNCH();
-  int64_t h[3];
-  LDF_CUDA(cudaMemcpyAsync(h, misc.get(), 24, cudaMemcpyDeviceToHost, s));
-  ctx.finish();
-  if (h[0] != 0) fail(LDF_ERR_INTERNAL, "string dictionary overflow");
-  const int64_t D = h[1];
+  const int64_t D = ctx.read_i64(misc.get() + 1);
   Buffer<uint32_t> rank(al, std::max<int64_t>(D, 1));
   if (D > 0) {
     launch("max_len", max_len_kernel, blocks_for(D), 256, 0, s, col, repr.get(), D, maxlen);

@@ -111,3 +111,24 @@ def test_sort_many_tiles_per_block(n):
     assert_tables_equal(res, R.sort(t, ["k"]), sort_by=None)
     res = run_sort(t, ["u", "k"], [False, True])
     assert_tables_equal(res, R.sort(t, ["u", "k"], [False, True]), sort_by=None)
+
+
+def test_sort_strings_sampled_dictionary():
+    """More than 4M string rows: the dedupe table of distinct strings is
+    sized from a sampled estimate.  Checked by properties at this size:
+    the keys come out in bytewise order, equal keys keep their input order,
+    and the rows are a permutation of the input."""
+    rng = np.random.default_rng(12)
+    n, nd = 5_000_000, 300_000
+    words = np.array([f"{i:x}{'z' * (i % 11)}" for i in range(nd)], dtype=object)
+    ranks = np.minimum(rng.zipf(1.05, n), nd) - 1
+    t = pa.table({"k": pa.array(words[ranks], pa.string()), "row": np.arange(n)})
+    res = run_sort(t, ["k"])
+    keys = np.array(res.column("k").to_pylist(), dtype=object)
+    rows = res.column("row").to_numpy()
+    assert np.array_equal(np.sort(rows), np.arange(n))
+    assert np.array_equal(keys, words[ranks][rows])
+    enc = np.array([k.encode() for k in keys], dtype=object)
+    assert all(enc[i] <= enc[i + 1] for i in range(n - 1))
+    same = enc[1:] == enc[:-1]
+    assert np.all(rows[1:][same] > rows[:-1][same])
