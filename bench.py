@@ -434,6 +434,9 @@ def run_strings_workload(args):
         "hash_partition(key, 256)": (lambda: hash_partition(t, ["k"], 256), 2 * n * row_bytes),
     }
     peak, kind = measured_peak_gbs()
+    wanted = {"groupby": "groupby", "sort": "stable sort", "partition": "hash_partition"}
+    if args.ops:
+        ops = {k: v for k, v in ops.items() if any(k.startswith(wanted[o]) for o in args.ops.split(","))}
     for name, (fn, algo) in ops.items():
         ms, rows, kern = _profiled(N, fn, args.steps)
         print(json.dumps({"workload": f"{name}: {n} rows", "ms": round(ms, 3), "rows_per_s": n / (ms / 1e3),
@@ -526,6 +529,7 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-requests", type=int, default=8192)
     ap.add_argument("--ref-rows", type=int, default=8_000_000, help="rows per step of the reference arm")
+    ap.add_argument("--ops", default="", help="--workload strings: comma list of groupby,sort,partition (default all)")
     ap.add_argument("--workload", default="groupby", choices=["groupby", "join", "strings", "ingest"],
                     help="groupby = the benchmark line; join / strings / ingest print per-op lines")
     args = ap.parse_args()
