@@ -11,7 +11,10 @@
 //    join.cu:79-101).  SEMI/ANTI emit lhs rows with / without a match.
 //
 // Device plan (one GPU, stream ordered):
-//  1. build   open-addressing table over the rhs keys, linear probing, load
+//  1. build   a single integer key whose build values span at most twice the
+//             build rows gets a direct-address table (row of key - min; a
+//             repeated key falls back to hashing).  Otherwise an
+//             open-addressing table over the rhs keys, linear probing, load
 //             factor 0.5, 8-byte slots {row, key32 | hash tag} (16-byte
 //             {key64, row} for 8-byte keys).  Nullable single keys with
 //             nulls_equal keep their null rows in a separate "null list".
@@ -21,20 +24,23 @@
 //             total (no tile waits on another; output rows come in tile
 //             completion order); otherwise a count pass sizes every tile's
 //             output exactly first.
-//  3. probe   tiles of 256 threads x 4 rows: the items' first slots are
+//  3. probe   tiles of 256 threads x 4 rows: the items' first lookups are
 //             prefetched together, matches resolved, the block scan counts
 //             output rows, then the fixed-width output columns are written
 //             directly from the probe kernel, column by column with the
 //             items' loads issued together (the gather is fused: no gather
-//             maps for fixed-width columns).  String output columns go
-//             through int32 gather maps and a string gather.
+//             maps for fixed-width columns).  The build key column is
+//             written from the equal probe key, and two other build columns
+//             can come packed in one 16-byte record per build row.  String
+//             output columns go through int32 gather maps and a string
+//             gather.
 //  4. FULL    unmatched rhs rows (never touched by a probe) are compacted and
 //             appended after the probe output.
 // Optional (LDF_B200_JOIN_PARTITION=1): both sides are first scattered into
 // 256 hash partitions so that the build partitions being probed stay in L2.
-// On the 200M x 20M int32-key workload on B200 it probes faster (5.6 vs
-// 7.9 ms) but the partitioning costs more than it saves, so it is off by
-// default.
+// On the 200M x 20M int32-key workload on B200 it probed faster than the
+// hash table (5.6 vs 7.9 ms) but the partitioning cost more than it saved,
+// so it is off by default (and dense keys take the direct table instead).
 #include "table_ops.cuh"
 
 namespace ldf {
