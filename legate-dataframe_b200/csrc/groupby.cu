@@ -11,26 +11,37 @@
 //    distinct valid values, plus one for null under mode "all".
 //  * output types are the Arrow hash_<kind> result types (.cpp:100-132).
 //
-// Device plan (one fused pass over the rows):
-//  * key table: open addressing over 8-byte key words (the key itself for
-//    1-8 byte keys, {representative row, hash tag} otherwise), sized from a
-//    strided sample (GEE estimate x8); a probe sequence longer than kMaxProbe
-//    flags overflow and the call re-runs with a larger table.
-//  * dense group ids: a row that inserts a key takes the next id (one atomic
-//    per warp for all inserting lanes), zero-initialises that group's state
-//    record, then publishes key and id.  Only touched records are written, so
-//    no table-sized memset of the state arena is needed.
-//  * hot groups in shared memory: ids are handed out in first-seen order, so
-//    under skew the heaviest keys get the smallest ids; ids below `hot` keep
-//    their record in shared memory (one flush per CTA at the end).  Hot and cold
-//    rows run the same code through one generic pointer (shared or global), so
-//    a warp never diverges on where its groups live.
-//  * one 8-word record per group (count, per-column valid count, sum, min,
-//    max, distinct count): a cold row's atomics touch a single 64-byte line.
-//  * float sums: exact 192-bit two's-complement fixed point (LSB 2^-96):
-//    integer adds are associative, so the result is independent of thread
-//    order and bit-identical alone or in a batch.
-//  * NUNIQUE: (group id, value) pairs in a pair set; first insertions count.
+// Device plan (stream ordered; the host reads back sizes between passes):
+//  1. sample  2^20 strided rows into scratch tables: GEE estimates (Charikar et
+//             al. 2000) of the groups (x8, heavy tails are underestimated) and
+//             of the (group, value) pairs of the first NUNIQUE column.
+//  2. assign  key -> dense id through an open-addressing key table (one word
+//             {id, key32} for <= 4-byte keys, {key word, id} otherwise, the
+//             word of multi-column / string keys being {representative row,
+//             hash tag}); ids come from per-warp pools of 32; row counts per
+//             id (the hottest ids in shared memory).  Warps take 1,024-row
+//             chunks; multi-column and string keys go one row per lane (their
+//             code is large).  A probe longer than kMaxProbe or too many ids
+//             flags overflow and the call re-runs with a 4x table.
+//  3. ranks   ids renumbered by descending row count (radix sort), so the
+//             most frequent groups get the smallest ranks; the row count and
+//             distinct counts live in field-major arrays by rank, each value
+//             column's valid count / sum / min / max in its own rank-major
+//             block (one row's updates share a cache line).
+//  4. columns one pass per value column: the most frequent ranks accumulate
+//             in shared memory (flushed once per CTA), the others with
+//             red.add / red.max.  Float sums are exact fixed point (six 32-bit
+//             chunks, LSB 2^-96): integer adds are associative, so a sum is
+//             independent of thread order and bit-identical alone or in a
+//             batch, and is rounded once at the end.
+//  5. NUNIQUE <= 4-byte values: one bit per value of the column's range for
+//             the most frequent ranks (96 MB of bitmaps), a pair set for the
+//             next ranks, and per-rank segments deduplicated in shared memory
+//             for the rest; wider values and strings: a generic pair set.
+//  6. output  used ranks compacted; keys, aggregates and their Arrow result
+//             types written in one finalize pass.
+// Input columns in host memory are copied in by HostStaging (keys first) and
+// each pass waits only for the columns it reads.
 #include "radix.cuh"
 
 #include <cmath>
