@@ -176,8 +176,30 @@ struct PassArgs {
   const uint64_t* digit_base;  // [256]
   uint64_t* status;            // [tiles * 256]
   unsigned long long* counter;
+  int32_t* inv_out;  // != null: inv_out[row] = the row's output position
+  RadixPayload pay;  // columns moved by this pass (pay.n = 0: none)
   int* err;
 };
+
+// dst[pos] = src[row] for every payload column.
+__device__ __forceinline__ void move_payload(const RadixPayload& p, int64_t pos, int64_t row)
+{
+  for (int c = 0; c < p.n; ++c) {
+    const DCol& sc = p.src[c];
+    switch (sc.width) {
+      case 1: static_cast<uint8_t*>(p.dst[c])[pos] = __ldg(static_cast<const uint8_t*>(sc.data) + row); break;
+      case 2: static_cast<uint16_t*>(p.dst[c])[pos] = __ldg(static_cast<const uint16_t*>(sc.data) + row); break;
+      case 4: static_cast<uint32_t*>(p.dst[c])[pos] = __ldg(static_cast<const uint32_t*>(sc.data) + row); break;
+      case 8:
+        static_cast<unsigned long long*>(p.dst[c])[pos] = __ldg(static_cast<const unsigned long long*>(sc.data) + row);
+        break;
+      default:  // 16: string ranges
+        static_cast<ulonglong2*>(p.dst[c])[pos] = __ldg(static_cast<const ulonglong2*>(sc.data) + row);
+        break;
+    }
+    if (p.dst_valid[c]) p.dst_valid[c][pos] = dvalid(sc, row) ? 1 : 0;
+  }
+}
 
 // Predecessor tiles whose status words one look-back round trip loads.
 constexpr int kLookback = 8;
@@ -295,6 +317,8 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
     const int64_t pos = static_cast<int64_t>(sh.gbase[d]) + (j - static_cast<int64_t>(sh.tile_start[d]));
     if (WRITE_KEYS) a.keys_out[pos] = s_keys[j];
     a.vals_out[pos] = s_vals[j];
+    if (a.inv_out) a.inv_out[s_vals[j]] = static_cast<int32_t>(pos);
+    if (a.pay.n) move_payload(a.pay, pos, s_vals[j]);
   }
 }
 
@@ -361,6 +385,13 @@ void launch_onesweep(cudaStream_t s, unsigned tiles, const PassArgs& a)
   launch("onesweep", onesweep_kernel<GATHER, WRITE_KEYS>, tiles, RT, smem, s, a);
 }
 
+// Identity order: the payload columns copied as they are.
+__global__ void copy_payload_kernel(RadixPayload p, int64_t n)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    move_payload(p, i, i);
+}
+
 __global__ void iota_kernel(int32_t* p, int64_t n)
 {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -413,7 +444,7 @@ void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes
 }
 
 void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
-                     int32_t* perm, std::vector<uint32_t>* hist_out)
+                     int32_t* perm, std::vector<uint32_t>* hist_out, int32_t* inv, const RadixPayload* payload)
 {
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
@@ -438,6 +469,8 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
   }
   if (run.empty()) {
     if (n > 0) launch("iota", iota_kernel, hblocks(n), RT, 0, s, perm, n);
+    if (n > 0 && inv) launch("iota", iota_kernel, hblocks(n), RT, 0, s, inv, n);
+    if (n > 0 && payload && payload->n) launch("copy_payload", copy_payload_kernel, hblocks(n), RT, 0, s, *payload, n);
     LDF_CHECK_LAUNCH();
     return;
   }
@@ -478,6 +511,8 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
     a.digit_base = d_bases.get() + k * 256;
     a.status     = status.get();
     a.counter    = reinterpret_cast<unsigned long long*>(status.get() + tiles * 256);
+    a.inv_out    = k + 1 == run.size() ? inv : nullptr;
+    if (k + 1 == run.size() && payload) a.pay = *payload;
     a.err        = ctx.err();
     const unsigned g = static_cast<unsigned>(tiles);
     if (gather && write_keys) launch_onesweep<true, true>(s, g, a);

@@ -52,7 +52,23 @@ void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes
 
 // Run the passes; `perm` receives the row order.  Passes whose histogram has a
 // single bucket holding every row are skipped.
+// Columns the last radix pass moves into sorted order itself: dst[j][pos] =
+// src[j][row] (and the null masks), written as the pass's coalesced runs
+// while the tile's source rows are still in cache.  Widths 1, 2, 4, 8, and 16
+// (the ranges of a string column; its characters stay where they are).
+constexpr int kPassPayload = 4;
+struct RadixPayload {
+  int n;
+  DCol src[kPassPayload];
+  void* dst[kPassPayload];
+  uint8_t* dst_valid[kPassPayload];
+};
+
+// `inv` (optional, n entries): inv[row] = the row's position in the sorted
+// order, written by the last pass.  `payload` (optional): columns the last
+// pass writes in sorted order.
 void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
-                     int32_t* perm, std::vector<uint32_t>* hist_out = nullptr);
+                     int32_t* perm, std::vector<uint32_t>* hist_out = nullptr, int32_t* inv = nullptr,
+                     const RadixPayload* payload = nullptr);
 
 }  // namespace ldf

@@ -447,11 +447,60 @@ void hash_partition(const ldf_column* table, int ncols, const int32_t* keys, int
     p.key.key_bytes    = 4;
     passes.push_back(p);
   }
+  // The radix pass itself moves up to kPassPayload columns into bucket order
+  // (written with its runs, read while the tile's rows are in cache): fixed
+  // widths straight into the outputs, a string column's ranges (and mask)
+  // into scratch, from which its characters are then copied in order.  Any
+  // further fixed-width columns are scattered through the inverse
+  // permutation, further string columns gathered.
+  RadixPayload pay{};
+  std::vector<DCol> fsrc;
+  std::vector<ldf_column*> fdst;
+  int pay_col[kPassPayload];                   // table column of each payload entry
+  std::vector<char> in_pass(ncols, 0);
+  std::vector<Buffer<uint8_t>> str_scratch;    // moved string ranges and masks, in bucket order
+  for (int j = 0; j < ncols; ++j) {
+    const ldf_column& c = table[j];
+    out[j]              = alloc_out_column(al, c.type, n, c.valid != nullptr);
+    if (pay.n < kPassPayload) {
+      pay_col[pay.n] = j;
+      in_pass[j]     = 1;
+      pay.src[pay.n] = make_dcol(c);
+      if (c.type == LDF_STRING) {
+        str_scratch.emplace_back(al, std::max<int64_t>(n, 1) * sizeof(ldf_range));
+        pay.dst[pay.n] = str_scratch.back().get();
+        pay.dst_valid[pay.n] = nullptr;
+        if (c.valid) {
+          str_scratch.emplace_back(al, std::max<int64_t>(n, 1));
+          pay.dst_valid[pay.n] = str_scratch.back().get();
+        }
+      } else {
+        pay.dst[pay.n]       = out[j].data;
+        pay.dst_valid[pay.n] = out[j].valid;
+      }
+      ++pay.n;
+    } else if (c.type != LDF_STRING) {
+      fsrc.push_back(make_dcol(c));
+      fdst.push_back(&out[j]);
+    }
+  }
   Buffer<int32_t> perm(al, std::max<int64_t>(n, 1));
-  radix_sort_rows(ctx, passes, n, perm.get());
+  Buffer<int32_t> inv;
+  if (!fsrc.empty()) inv = Buffer<int32_t>(al, std::max<int64_t>(n, 1));
+  radix_sort_rows(ctx, passes, n, perm.get(), nullptr, fsrc.empty() ? nullptr : inv.get(), &pay);
   std::vector<unsigned long long> h(nparts);
   LDF_CUDA(cudaMemcpyAsync(h.data(), counts.get(), static_cast<size_t>(nparts) * 8, cudaMemcpyDeviceToHost, s));
-  gather_table(ctx, table, ncols, perm.get(), n, out);
+  scatter_fixed_columns(ctx, fsrc.data(), inv.get(), n, fdst.data(), static_cast<int>(fsrc.size()));
+  for (int q = 0; q < pay.n; ++q) {
+    const DCol& src = pay.src[q];
+    if (src.type != LDF_STRING) continue;
+    DCol ordered  = src;  // same characters; ranges and mask already in bucket order
+    ordered.data  = pay.dst[q];
+    ordered.valid = pay.dst_valid[q];
+    gather_strings(ctx, ordered, nullptr, n, out[pay_col[q]]);
+  }
+  for (int j = 0; j < ncols; ++j)
+    if (table[j].type == LDF_STRING && !in_pass[j]) gather_strings(ctx, make_dcol(table[j]), perm.get(), n, out[j]);
   ctx.finish();
   int64_t acc = 0;
   for (int b = 0; b < nparts; ++b) {

@@ -357,6 +357,65 @@ __global__ void __launch_bounds__(256) gather_fixed_kernel(GatherSet g, const in
   }
 }
 
+// dst[inv[r]] = src[r] for up to kGatherCols fixed-width columns: the source
+// is read in order and every output row is written once.  Used where the
+// output positions of consecutive rows fall into few runs (a partition by
+// bucket: a tile's rows of one bucket land side by side), so the writes
+// combine in L2 instead of the reads scattering.
+template <typename T>
+__device__ __forceinline__ void scatter_one(const T* src, const uint8_t* valid, T* dst, uint8_t* dst_valid,
+                                            const int64_t (&i)[kGatherRows], const int32_t (&pos)[kGatherRows],
+                                            int64_t rows)
+{
+  T v[kGatherRows];
+  uint8_t ok[kGatherRows];
+#pragma unroll
+  for (int j = 0; j < kGatherRows; ++j) {
+    v[j]  = i[j] < rows ? __ldg(src + i[j]) : T(0);
+    ok[j] = (i[j] < rows && valid != nullptr) ? (__ldg(valid + i[j]) != 0 ? 1 : 0) : 1;
+  }
+#pragma unroll
+  for (int j = 0; j < kGatherRows; ++j) {
+    if (i[j] >= rows) continue;
+    dst[pos[j]] = v[j];
+    if (dst_valid) dst_valid[pos[j]] = ok[j];
+  }
+}
+
+__global__ void __launch_bounds__(256) scatter_fixed_kernel(GatherSet g, const int32_t* inv, int64_t rows)
+{
+  const int64_t per_iter = static_cast<int64_t>(blockDim.x) * kGatherRows;
+  for (int64_t base = blockIdx.x * per_iter; base < rows; base += static_cast<int64_t>(gridDim.x) * per_iter) {
+    int64_t i[kGatherRows];
+    int32_t pos[kGatherRows];
+#pragma unroll
+    for (int j = 0; j < kGatherRows; ++j) {
+      i[j]   = base + j * blockDim.x + threadIdx.x;
+      pos[j] = i[j] < rows ? __ldg(inv + i[j]) : 0;
+    }
+    for (int c = 0; c < g.ncols; ++c) {
+      switch (g.width[c]) {
+        case 1:
+          scatter_one(static_cast<const uint8_t*>(g.src[c]), g.valid[c], static_cast<uint8_t*>(g.dst[c]),
+                      g.dst_valid[c], i, pos, rows);
+          break;
+        case 2:
+          scatter_one(static_cast<const uint16_t*>(g.src[c]), g.valid[c], static_cast<uint16_t*>(g.dst[c]),
+                      g.dst_valid[c], i, pos, rows);
+          break;
+        case 4:
+          scatter_one(static_cast<const uint32_t*>(g.src[c]), g.valid[c], static_cast<uint32_t*>(g.dst[c]),
+                      g.dst_valid[c], i, pos, rows);
+          break;
+        default:
+          scatter_one(static_cast<const unsigned long long*>(g.src[c]), g.valid[c],
+                      static_cast<unsigned long long*>(g.dst[c]), g.dst_valid[c], i, pos, rows);
+          break;
+      }
+    }
+  }
+}
+
 inline unsigned grid_for(int64_t n, int threads)
 {
   int64_t b = ceil_div(n, threads);
@@ -414,6 +473,28 @@ void gather_fixed_columns(const OpContext& ctx, const DCol* src, const int32_t* 
     }
     launch("gather_fixed", gather_fixed_kernel, grid_for(ceil_div(rows, kGatherRows), 256), 256, 0, ctx.stream(), g,
            map, rows);
+  }
+}
+
+void scatter_fixed_columns(const OpContext& ctx, const DCol* src, const int32_t* inv, int64_t rows,
+                           ldf_column* const* dst, int ncols)
+{
+  if (rows == 0) return;
+  for (int c0 = 0; c0 < ncols; c0 += kGatherCols) {
+    GatherSet g{};
+    g.ncols = ncols - c0 < kGatherCols ? ncols - c0 : kGatherCols;
+    for (int k = 0; k < g.ncols; ++k) {
+      const DCol& sc = src[c0 + k];
+      LDF_REQUIRE(sc.width == 1 || sc.width == 2 || sc.width == 4 || sc.width == 8,
+                  "scatter: unsupported fixed width");
+      g.width[k]     = sc.width;
+      g.src[k]       = sc.data;
+      g.valid[k]     = sc.valid;
+      g.dst[k]       = dst[c0 + k]->data;
+      g.dst_valid[k] = dst[c0 + k]->valid;
+    }
+    launch("scatter_fixed", scatter_fixed_kernel, grid_for(ceil_div(rows, kGatherRows), 256), 256, 0, ctx.stream(),
+           g, inv, rows);
   }
 }
 

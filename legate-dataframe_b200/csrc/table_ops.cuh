@@ -128,4 +128,9 @@ void gather_fixed(const OpContext& ctx, const DCol& src, const int32_t* map, int
 void gather_fixed_columns(const OpContext& ctx, const DCol* src, const int32_t* map, int64_t rows,
                           ldf_column* const* dst, int ncols);
 
+// dst[inv[r]] = src[r] for several fixed-width columns (inv: a permutation;
+// one launch per eight columns).
+void scatter_fixed_columns(const OpContext& ctx, const DCol* src, const int32_t* inv, int64_t rows,
+                           ldf_column* const* dst, int ncols);
+
 }  // namespace ldf

@@ -57,3 +57,25 @@ def test_partition_empty():
     t = pa.table({"k": pa.array([], pa.int64())})
     res, offs = run_partition(t, ["k"], 8)
     assert res.num_rows == 0 and offs == [0] * 9
+
+
+@pytest.mark.parametrize("nparts", [5, 256, 1000])
+def test_partition_many_columns(nparts):
+    """Up to four columns (string ranges included) move inside the radix pass;
+    further fixed-width columns are scattered and further strings gathered.
+    Nullable columns on each route; 1,000 buckets take two passes."""
+    rng = np.random.default_rng(nparts)
+    n = 60_000
+    t = pa.table({
+        "s1": pa.array([f"a{i % 777}" + "x" * (i % 9) for i in range(n)]),
+        "k": rng.integers(0, 5000, n),
+        "f": pa.array(rng.normal(size=n).astype(np.float32), mask=rng.random(n) < 0.1),
+        "b": pa.array(rng.random(n) < 0.5, mask=rng.random(n) < 0.05),
+        "s2": pa.array([None if i % 11 == 0 else f"q{i % 313}" for i in range(n)]),
+        "x": pa.array(rng.integers(-100, 100, n).astype(np.int16), mask=rng.random(n) < 0.2),
+        "s3": pa.array([f"z{i}" for i in range(n)], type=pa.large_string()),
+    })
+    got, offs = run_partition(t, ["k"], nparts)
+    exp, eoffs, _ = R.hash_partition(t, ["k"], nparts)
+    assert offs == eoffs
+    assert got.equals(exp)
