@@ -193,9 +193,11 @@ __device__ __forceinline__ void move_payload(const RadixPayload& p, int64_t pos,
       case 8:
         static_cast<unsigned long long*>(p.dst[c])[pos] = __ldg(static_cast<const unsigned long long*>(sc.data) + row);
         break;
-      default:  // 16: string ranges
-        static_cast<ulonglong2*>(p.dst[c])[pos] = __ldg(static_cast<const ulonglong2*>(sc.data) + row);
+      default: {  // 16: string ranges (8-byte aligned at the source; the scratch is 16-byte aligned)
+        const unsigned long long* r = static_cast<const unsigned long long*>(sc.data) + 2 * row;
+        static_cast<ulonglong2*>(p.dst[c])[pos] = make_ulonglong2(__ldg(r), __ldg(r + 1));
         break;
+      }
     }
     if (p.dst_valid[c]) p.dst_valid[c][pos] = dvalid(sc, row) ? 1 : 0;
   }
