@@ -17,8 +17,8 @@
 // (cpp/src/core/repartition_by_hash.cu:296-310): bucket = hash(keys) % nparts,
 // rows grouped by bucket, start offsets returned; here one pass hashes the
 // keys into a bucket id per row (and counts the buckets), then one stable
-// radix pass on the bucket ids (two for more than 256 buckets), then one
-// gather.
+// radix pass on the bucket ids (two for more than 256 buckets) that also
+// moves up to four columns into bucket order itself.
 #include "radix.cuh"
 
 namespace ldf {
