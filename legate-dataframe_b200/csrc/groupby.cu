@@ -13,7 +13,7 @@
 //
 // Device plan (stream ordered; the host reads back sizes between passes):
 //  1. sample  2^20 strided rows into scratch tables: GEE estimates (Charikar et
-//             al. 2000) of the groups (x8, heavy tails are underestimated) and
+//             al. 2000) of the groups (x4, heavy tails are underestimated) and
 //             of the (group, value) pairs of the first NUNIQUE column.
 //  2. assign  key -> dense id through an open-addressing key table (one word
 //             {id, key32} for <= 4-byte keys, {key word, id} otherwise, the
@@ -1529,14 +1529,15 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     unsigned long long h[4];
     LDF_CUDA(cudaMemcpyAsync(h, stats.get(), 32, cudaMemcpyDeviceToHost, s));
     ctx.finish();
-    // GEE (Charikar et al. 2000) for the groups, taken x8 below because it
-    // underestimates heavy tails; (group, value) pairs are mostly unique in a
+    // GEE (Charikar et al. 2000) for the groups, taken x4 below because it
+    // underestimates heavy tails (a table that turns out too small overflows
+    // and the pass re-runs with 4x the slots); (group, value) pairs are mostly unique in a
     // sample, where GEE fails, so they use the scale-up d * N / n, an
     // overestimate whenever pairs repeat.
     const double scale = std::sqrt(static_cast<double>(n) / static_cast<double>(ns));
     est_groups         = static_cast<int64_t>(scale * h[1] + (h[0] - h[1])) + 1;
     est_pairs          = static_cast<int64_t>(static_cast<double>(h[2]) * n / ns) + 1;
-    est_groups         = std::min<int64_t>(8 * est_groups, n);
+    est_groups         = std::min<int64_t>(4 * est_groups, n);
     est_pairs          = std::min<int64_t>(est_pairs, n);
   }
   if (std::getenv("LDF_B200_DEBUG"))
