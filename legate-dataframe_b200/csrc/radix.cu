@@ -203,6 +203,62 @@ __device__ __forceinline__ void move_payload(const RadixPayload& p, int64_t pos,
   }
 }
 
+// Rows of a thread whose payload loads are issued together in a pass that
+// moves columns.
+constexpr int kMoveBatch = 4;
+
+__device__ __forceinline__ uint8_t ld_row(const uint8_t* p) { return __ldg(p); }
+__device__ __forceinline__ uint16_t ld_row(const uint16_t* p) { return __ldg(p); }
+__device__ __forceinline__ uint32_t ld_row(const uint32_t* p) { return __ldg(p); }
+__device__ __forceinline__ unsigned long long ld_row(const unsigned long long* p) { return __ldg(p); }
+// string ranges: 8-byte aligned at the source, so two 8-byte loads
+__device__ __forceinline__ ulonglong2 ld_row(const ulonglong2* p)
+{
+  const unsigned long long* q = reinterpret_cast<const unsigned long long*>(p);
+  return make_ulonglong2(__ldg(q), __ldg(q + 1));
+}
+
+// dst[pos[k]] = src[row[k]] for the kMoveBatch rows (pos < 0: none), every
+// load issued before the first store.
+template <typename T>
+__device__ __forceinline__ void move_rows(const void* src, void* dst, const int32_t (&pos)[kMoveBatch],
+                                          const int32_t (&row)[kMoveBatch])
+{
+  const T* sp = static_cast<const T*>(src);
+  T* dp       = static_cast<T*>(dst);
+  T v[kMoveBatch];
+#pragma unroll
+  for (int k = 0; k < kMoveBatch; ++k)
+    if (pos[k] >= 0) v[k] = ld_row(sp + row[k]);
+#pragma unroll
+  for (int k = 0; k < kMoveBatch; ++k)
+    if (pos[k] >= 0) dp[pos[k]] = v[k];
+}
+
+// Every payload column's values (and masks) of kMoveBatch rows.
+__device__ __forceinline__ void move_payload_rows(const RadixPayload& p, const int32_t (&pos)[kMoveBatch],
+                                                  const int32_t (&row)[kMoveBatch])
+{
+  for (int c = 0; c < p.n; ++c) {
+    const DCol& sc = p.src[c];
+    switch (sc.width) {
+      case 1: move_rows<uint8_t>(sc.data, p.dst[c], pos, row); break;
+      case 2: move_rows<uint16_t>(sc.data, p.dst[c], pos, row); break;
+      case 4: move_rows<uint32_t>(sc.data, p.dst[c], pos, row); break;
+      case 8: move_rows<unsigned long long>(sc.data, p.dst[c], pos, row); break;
+      default: move_rows<ulonglong2>(sc.data, p.dst[c], pos, row); break;
+    }
+    if (p.dst_valid[c]) {
+      uint8_t m[kMoveBatch];
+#pragma unroll
+      for (int k = 0; k < kMoveBatch; ++k) m[k] = pos[k] >= 0 && dvalid(sc, row[k]) ? 1 : 0;
+#pragma unroll
+      for (int k = 0; k < kMoveBatch; ++k)
+        if (pos[k] >= 0) p.dst_valid[c][pos[k]] = m[k];
+    }
+  }
+}
+
 // Predecessor tiles whose status words one look-back round trip loads.
 constexpr int kLookback = 8;
 
@@ -222,7 +278,7 @@ struct OsShared {
 // s_keys / s_vals / s_dig (tile-local positions need no look-back), per-digit
 // decoupled look-back, then coalesced runs written out.  sh.whist must be zero
 // on entry.  Ends with every thread past its reads of the staging arrays.
-template <bool WRITE_KEYS>
+template <bool WRITE_KEYS, bool MOVE>
 __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile, uint64_t (&key)[RI],
                                                  int32_t (&val)[RI], uint32_t (&dr)[RI], OsShared& sh,
                                                  uint64_t* s_keys, int32_t* s_vals, uint8_t* s_dig)
@@ -313,14 +369,37 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
   }
   __syncthreads();
   const int64_t tbase = tile * RTILE;
-  const int64_t cnt   = a.n - tbase < RTILE ? a.n - tbase : RTILE;
-  for (int j = threadIdx.x; j < cnt; j += RT) {
-    const uint32_t d  = s_dig[j];
-    const int64_t pos = static_cast<int64_t>(sh.gbase[d]) + (j - static_cast<int64_t>(sh.tile_start[d]));
-    if (WRITE_KEYS) a.keys_out[pos] = s_keys[j];
-    a.vals_out[pos] = s_vals[j];
-    if (a.inv_out) a.inv_out[s_vals[j]] = static_cast<int32_t>(pos);
-    if (a.pay.n) move_payload(a.pay, pos, s_vals[j]);
+  const int cnt       = static_cast<int>(a.n - tbase < RTILE ? a.n - tbase : RTILE);
+  if (!MOVE) {
+    for (int j = threadIdx.x; j < cnt; j += RT) {
+      const uint32_t d  = s_dig[j];
+      const int64_t pos = static_cast<int64_t>(sh.gbase[d]) + (j - static_cast<int64_t>(sh.tile_start[d]));
+      if (WRITE_KEYS) a.keys_out[pos] = s_keys[j];
+      a.vals_out[pos] = s_vals[j];
+      if (a.inv_out) a.inv_out[s_vals[j]] = static_cast<int32_t>(pos);
+    }
+    return;
+  }
+  // a pass that moves columns: kMoveBatch rows of a thread at a time, so the
+  // payload's loads (random rows after the first pass) overlap.  Positions
+  // and rows fit 32 bits (fewer than 2^31 rows).
+  for (int j0 = threadIdx.x; j0 < cnt; j0 += RT * kMoveBatch) {
+    int32_t pos[kMoveBatch], row[kMoveBatch];
+#pragma unroll
+    for (int k = 0; k < kMoveBatch; ++k) {
+      const int j = j0 + k * RT;
+      pos[k]      = -1;
+      row[k]      = 0;
+      if (j < cnt) {
+        const uint32_t d = s_dig[j];
+        pos[k]           = static_cast<int32_t>(sh.gbase[d] + static_cast<uint32_t>(j) - sh.tile_start[d]);
+        row[k]           = s_vals[j];
+        if (WRITE_KEYS) a.keys_out[pos[k]] = s_keys[j];
+        a.vals_out[pos[k]] = row[k];
+        if (a.inv_out) a.inv_out[row[k]] = pos[k];
+      }
+    }
+    move_payload_rows(a.pay, pos, row);
   }
 }
 
@@ -352,8 +431,9 @@ __device__ __forceinline__ void load_tile_rows(const PassArgs& a, int64_t tile, 
 }
 
 // One tile per CTA.  WRITE_KEYS: later passes of the same word follow, so
-// carry the word along.
-template <bool GATHER, bool WRITE_KEYS>
+// carry the word along.  MOVE: the pass also moves a.pay's columns (the last
+// pass only, which carries no word).
+template <bool GATHER, bool WRITE_KEYS, bool MOVE = false>
 __global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs a)
 {
   __shared__ OsShared sh;
@@ -370,7 +450,7 @@ __global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs 
   int32_t val[RI];
   uint32_t dr[RI];
   load_tile_rows<GATHER>(a, tile, key, val, dr);
-  rank_and_scatter<WRITE_KEYS>(a, tile, key, val, dr, sh, s_keys, s_vals, s_dig);
+  rank_and_scatter<WRITE_KEYS, MOVE>(a, tile, key, val, dr, sh, s_keys, s_vals, s_dig);
 }
 
 constexpr size_t onesweep_smem(bool write_keys)
@@ -378,13 +458,14 @@ constexpr size_t onesweep_smem(bool write_keys)
   return (write_keys ? RTILE * sizeof(uint64_t) : 0) + RTILE * (sizeof(int32_t) + 1);
 }
 
-template <bool GATHER, bool WRITE_KEYS>
+template <bool GATHER, bool WRITE_KEYS, bool MOVE = false>
 void launch_onesweep(cudaStream_t s, unsigned tiles, const PassArgs& a)
 {
+  static_assert(!(MOVE && WRITE_KEYS), "the pass that moves columns is the last one");
   constexpr size_t smem = onesweep_smem(WRITE_KEYS);
-  LDF_CUDA(cudaFuncSetAttribute(onesweep_kernel<GATHER, WRITE_KEYS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  LDF_CUDA(cudaFuncSetAttribute(onesweep_kernel<GATHER, WRITE_KEYS, MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
-  launch("onesweep", onesweep_kernel<GATHER, WRITE_KEYS>, tiles, RT, smem, s, a);
+  launch("onesweep", onesweep_kernel<GATHER, WRITE_KEYS, MOVE>, tiles, RT, smem, s, a);
 }
 
 // Identity order: the payload columns copied as they are.
@@ -517,7 +598,10 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
     if (k + 1 == run.size() && payload) a.pay = *payload;
     a.err        = ctx.err();
     const unsigned g = static_cast<unsigned>(tiles);
-    if (gather && write_keys) launch_onesweep<true, true>(s, g, a);
+    const bool move = a.pay.n > 0;
+    if (move && gather) launch_onesweep<true, false, true>(s, g, a);
+    else if (move) launch_onesweep<false, false, true>(s, g, a);
+    else if (gather && write_keys) launch_onesweep<true, true>(s, g, a);
     else if (gather) launch_onesweep<true, false>(s, g, a);
     else if (write_keys) launch_onesweep<false, true>(s, g, a);
     else launch_onesweep<false, false>(s, g, a);

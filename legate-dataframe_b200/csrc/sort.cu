@@ -337,6 +337,58 @@ void gather_table(const OpContext& ctx, const ldf_column* table, int ncols, cons
   gather_fixed_columns(ctx, fsrc.data(), map, rows, fdst.data(), static_cast<int>(fsrc.size()));
 }
 
+namespace {
+// Columns that the last radix pass moves itself, up to kPassPayload of them in
+// table order (written with the pass's runs while the tile's rows are in
+// cache, instead of gathered through the permutation afterwards): fixed
+// widths straight into the allocated outputs, a string column's ranges (and
+// mask) into scratch in output order, from which move_strings_in_order then
+// copies its characters.
+struct PassMove {
+  RadixPayload pay{};
+  int col[kPassPayload];              // table column of each payload entry
+  std::vector<char> moved;            // per table column
+  std::vector<Buffer<uint8_t>> scratch;
+};
+
+void plan_pass_move(const Allocator& al, const ldf_column* table, int ncols, int64_t n, ldf_column* out,
+                    PassMove& m)
+{
+  m.moved.assign(ncols, 0);
+  for (int j = 0; j < ncols && m.pay.n < kPassPayload; ++j) {
+    const ldf_column& c = table[j];
+    const int q         = m.pay.n++;
+    m.col[q]            = j;
+    m.moved[j]          = 1;
+    m.pay.src[q]        = make_dcol(c);
+    if (c.type == LDF_STRING) {
+      m.scratch.emplace_back(al, std::max<int64_t>(n, 1) * sizeof(ldf_range));
+      m.pay.dst[q]       = m.scratch.back().get();
+      m.pay.dst_valid[q] = nullptr;
+      if (c.valid) {
+        m.scratch.emplace_back(al, std::max<int64_t>(n, 1));
+        m.pay.dst_valid[q] = m.scratch.back().get();
+      }
+    } else {
+      m.pay.dst[q]       = out[j].data;
+      m.pay.dst_valid[q] = out[j].valid;
+    }
+  }
+}
+
+void move_strings_in_order(const OpContext& ctx, const PassMove& m, int64_t n, ldf_column* out)
+{
+  for (int q = 0; q < m.pay.n; ++q) {
+    const DCol& src = m.pay.src[q];
+    if (src.type != LDF_STRING) continue;
+    DCol ordered  = src;  // same characters; ranges and mask already in output order
+    ordered.data  = m.pay.dst[q];
+    ordered.valid = m.pay.dst_valid[q];
+    gather_strings(ctx, ordered, nullptr, n, out[m.col[q]]);
+  }
+}
+}  // namespace
+
 void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const uint8_t* ascending, int nkeys,
                 bool nulls_at_end, int64_t limit, ldf_column* out, const OpContext& ctx)
 {
@@ -374,7 +426,6 @@ void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const u
     }
   }
   Buffer<int32_t> perm(al, std::max<int64_t>(n, 1));
-  radix_sort_rows(ctx, passes, n, perm.get());
   int64_t first = 0, rows = n;
   if (limit != INT64_MIN && (limit < 0 ? -limit : limit) < n) {
     if (limit < 0) {
@@ -384,7 +435,31 @@ void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const u
       rows = limit;
     }
   }
-  gather_table(ctx, table, ncols, perm.get() + first, rows, out);
+  if (rows < n) {
+    radix_sort_rows(ctx, passes, n, perm.get());
+    gather_table(ctx, table, ncols, perm.get() + first, rows, out);
+    ctx.finish();
+    return;
+  }
+  // the whole table: the last pass moves the first kPassPayload columns, the
+  // rest are gathered through the permutation
+  for (int j = 0; j < ncols; ++j) out[j] = alloc_out_column(al, table[j].type, n, table[j].valid != nullptr);
+  PassMove mv;
+  plan_pass_move(al, table, ncols, n, out, mv);
+  radix_sort_rows(ctx, passes, n, perm.get(), nullptr, nullptr, &mv.pay);
+  move_strings_in_order(ctx, mv, n, out);
+  std::vector<DCol> fsrc;
+  std::vector<ldf_column*> fdst;
+  for (int j = 0; j < ncols; ++j) {
+    if (mv.moved[j]) continue;
+    if (table[j].type == LDF_STRING) {
+      gather_strings(ctx, make_dcol(table[j]), perm.get(), n, out[j]);
+    } else {
+      fsrc.push_back(make_dcol(table[j]));
+      fdst.push_back(&out[j]);
+    }
+  }
+  gather_fixed_columns(ctx, fsrc.data(), perm.get(), n, fdst.data(), static_cast<int>(fsrc.size()));
   ctx.finish();
 }
 
@@ -448,59 +523,29 @@ void hash_partition(const ldf_column* table, int ncols, const int32_t* keys, int
     passes.push_back(p);
   }
   // The radix pass itself moves up to kPassPayload columns into bucket order
-  // (written with its runs, read while the tile's rows are in cache): fixed
-  // widths straight into the outputs, a string column's ranges (and mask)
-  // into scratch, from which its characters are then copied in order.  Any
-  // further fixed-width columns are scattered through the inverse
+  // (one pass over the rows in input order, so its reads are sequential).
+  // Any further fixed-width columns are scattered through the inverse
   // permutation, further string columns gathered.
-  RadixPayload pay{};
+  for (int j = 0; j < ncols; ++j) out[j] = alloc_out_column(al, table[j].type, n, table[j].valid != nullptr);
+  PassMove mv;
+  plan_pass_move(al, table, ncols, n, out, mv);
   std::vector<DCol> fsrc;
   std::vector<ldf_column*> fdst;
-  int pay_col[kPassPayload];                   // table column of each payload entry
-  std::vector<char> in_pass(ncols, 0);
-  std::vector<Buffer<uint8_t>> str_scratch;    // moved string ranges and masks, in bucket order
-  for (int j = 0; j < ncols; ++j) {
-    const ldf_column& c = table[j];
-    out[j]              = alloc_out_column(al, c.type, n, c.valid != nullptr);
-    if (pay.n < kPassPayload) {
-      pay_col[pay.n] = j;
-      in_pass[j]     = 1;
-      pay.src[pay.n] = make_dcol(c);
-      if (c.type == LDF_STRING) {
-        str_scratch.emplace_back(al, std::max<int64_t>(n, 1) * sizeof(ldf_range));
-        pay.dst[pay.n] = str_scratch.back().get();
-        pay.dst_valid[pay.n] = nullptr;
-        if (c.valid) {
-          str_scratch.emplace_back(al, std::max<int64_t>(n, 1));
-          pay.dst_valid[pay.n] = str_scratch.back().get();
-        }
-      } else {
-        pay.dst[pay.n]       = out[j].data;
-        pay.dst_valid[pay.n] = out[j].valid;
-      }
-      ++pay.n;
-    } else if (c.type != LDF_STRING) {
-      fsrc.push_back(make_dcol(c));
+  for (int j = 0; j < ncols; ++j)
+    if (!mv.moved[j] && table[j].type != LDF_STRING) {
+      fsrc.push_back(make_dcol(table[j]));
       fdst.push_back(&out[j]);
     }
-  }
   Buffer<int32_t> perm(al, std::max<int64_t>(n, 1));
   Buffer<int32_t> inv;
   if (!fsrc.empty()) inv = Buffer<int32_t>(al, std::max<int64_t>(n, 1));
-  radix_sort_rows(ctx, passes, n, perm.get(), nullptr, fsrc.empty() ? nullptr : inv.get(), &pay);
+  radix_sort_rows(ctx, passes, n, perm.get(), nullptr, fsrc.empty() ? nullptr : inv.get(), &mv.pay);
   std::vector<unsigned long long> h(nparts);
   LDF_CUDA(cudaMemcpyAsync(h.data(), counts.get(), static_cast<size_t>(nparts) * 8, cudaMemcpyDeviceToHost, s));
   scatter_fixed_columns(ctx, fsrc.data(), inv.get(), n, fdst.data(), static_cast<int>(fsrc.size()));
-  for (int q = 0; q < pay.n; ++q) {
-    const DCol& src = pay.src[q];
-    if (src.type != LDF_STRING) continue;
-    DCol ordered  = src;  // same characters; ranges and mask already in bucket order
-    ordered.data  = pay.dst[q];
-    ordered.valid = pay.dst_valid[q];
-    gather_strings(ctx, ordered, nullptr, n, out[pay_col[q]]);
-  }
+  move_strings_in_order(ctx, mv, n, out);
   for (int j = 0; j < ncols; ++j)
-    if (table[j].type == LDF_STRING && !in_pass[j]) gather_strings(ctx, make_dcol(table[j]), perm.get(), n, out[j]);
+    if (table[j].type == LDF_STRING && !mv.moved[j]) gather_strings(ctx, make_dcol(table[j]), perm.get(), n, out[j]);
   ctx.finish();
   int64_t acc = 0;
   for (int b = 0; b < nparts; ++b) {

@@ -132,3 +132,35 @@ def test_sort_strings_sampled_dictionary():
     assert all(enc[i] <= enc[i + 1] for i in range(n - 1))
     same = enc[1:] == enc[:-1]
     assert np.all(rows[1:][same] > rows[:-1][same])
+
+
+def test_sort_wide_table_moved_and_gathered_columns():
+    """A whole-table sort moves the first four columns inside its last radix
+    pass (fixed widths straight into the outputs, a string column's ranges
+    through scratch) and gathers the others through the permutation: every
+    fixed width with and without nulls, strings on both sides of that
+    boundary, and a constant key (no pass runs, the columns are copied)."""
+    rng = np.random.default_rng(21)
+    n = 200_000
+    words = np.array([f"w{i:x}" + "q" * (i % 23) for i in range(5000)], dtype=object)
+
+    def strings(null_frac):
+        w = words[rng.integers(0, len(words), n)]
+        return pa.array(w, pa.string(), mask=rng.random(n) < null_frac if null_frac else None)
+
+    t = pa.table({
+        "s1": strings(0.05),
+        "i8": pa.array(rng.integers(-128, 128, n).astype(np.int8), mask=rng.random(n) < 0.1),
+        "f32": rng.normal(size=n).astype(np.float32),
+        "i16": pa.array(rng.integers(-300, 300, n).astype(np.int16), mask=rng.random(n) < 0.02),
+        "s2": strings(0.0),
+        "i64": pa.array(rng.integers(-(2**40), 2**40, n), mask=rng.random(n) < 0.03),
+        "s3": strings(0.2),
+        "row": np.arange(n),
+    })
+    for keys, asc in ((["i16", "s1"], [True, False]), (["i64"], [False]), (["s2", "f32"], [True, True])):
+        for nulls_at_end in (True, False):
+            res = run_sort(t, keys, asc, nulls_at_end)
+            assert_tables_equal(res, R.sort(t, keys, asc, nulls_at_end), sort_by=None)
+    const = t.append_column("c", pa.array(np.zeros(n, np.int32)))
+    assert_tables_equal(run_sort(const, ["c"]), const, sort_by=None)
