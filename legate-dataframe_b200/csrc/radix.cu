@@ -205,49 +205,67 @@ __device__ __forceinline__ void move_payload(const RadixPayload& p, int64_t pos,
 
 // Rows of a thread whose payload loads are issued together in a pass that
 // moves columns.
-constexpr int kMoveBatch = 4;
+constexpr int kMoveBatch = 3;
 
-__device__ __forceinline__ uint8_t ld_row(const uint8_t* p) { return __ldg(p); }
-__device__ __forceinline__ uint16_t ld_row(const uint16_t* p) { return __ldg(p); }
-__device__ __forceinline__ uint32_t ld_row(const uint32_t* p) { return __ldg(p); }
-__device__ __forceinline__ unsigned long long ld_row(const unsigned long long* p) { return __ldg(p); }
-// string ranges: 8-byte aligned at the source, so two 8-byte loads
-__device__ __forceinline__ ulonglong2 ld_row(const ulonglong2* p)
+// dst[pos[k]] = src[row[k]] for 16-byte string ranges (8-byte aligned at the
+// source: two 8-byte loads; the scratch destination is 16-byte aligned), every
+// load issued before the first store.  pos < 0: no row.
+__device__ __forceinline__ void move_ranges(const void* src, void* dst, const int32_t (&pos)[kMoveBatch],
+                                            const int32_t (&row)[kMoveBatch])
 {
-  const unsigned long long* q = reinterpret_cast<const unsigned long long*>(p);
-  return make_ulonglong2(__ldg(q), __ldg(q + 1));
-}
-
-// dst[pos[k]] = src[row[k]] for the kMoveBatch rows (pos < 0: none), every
-// load issued before the first store.
-template <typename T>
-__device__ __forceinline__ void move_rows(const void* src, void* dst, const int32_t (&pos)[kMoveBatch],
-                                          const int32_t (&row)[kMoveBatch])
-{
-  const T* sp = static_cast<const T*>(src);
-  T* dp       = static_cast<T*>(dst);
-  T v[kMoveBatch];
+  const unsigned long long* sp = static_cast<const unsigned long long*>(src);
+  ulonglong2 v[kMoveBatch];
 #pragma unroll
   for (int k = 0; k < kMoveBatch; ++k)
-    if (pos[k] >= 0) v[k] = ld_row(sp + row[k]);
+    if (pos[k] >= 0) v[k] = make_ulonglong2(__ldg(sp + 2 * row[k]), __ldg(sp + 2 * row[k] + 1));
 #pragma unroll
   for (int k = 0; k < kMoveBatch; ++k)
-    if (pos[k] >= 0) dp[pos[k]] = v[k];
+    if (pos[k] >= 0) static_cast<ulonglong2*>(dst)[pos[k]] = v[k];
 }
 
-// Every payload column's values (and masks) of kMoveBatch rows.
+__device__ __forceinline__ unsigned long long ld_fixed(const DCol& c, int32_t row)
+{
+  switch (c.width) {
+    case 1: return __ldg(static_cast<const uint8_t*>(c.data) + row);
+    case 2: return __ldg(static_cast<const uint16_t*>(c.data) + row);
+    case 4: return __ldg(static_cast<const uint32_t*>(c.data) + row);
+    default: return __ldg(static_cast<const unsigned long long*>(c.data) + row);
+  }
+}
+
+__device__ __forceinline__ void st_fixed(void* dst, int width, int32_t pos, unsigned long long v)
+{
+  switch (width) {
+    case 1: static_cast<uint8_t*>(dst)[pos] = static_cast<uint8_t>(v); break;
+    case 2: static_cast<uint16_t*>(dst)[pos] = static_cast<uint16_t>(v); break;
+    case 4: static_cast<uint32_t*>(dst)[pos] = static_cast<uint32_t>(v); break;
+    default: static_cast<unsigned long long*>(dst)[pos] = v; break;
+  }
+}
+
+// Every payload column's values (and masks) of kMoveBatch rows.  The loads
+// of all fixed-width columns are issued before the first store, so the
+// random rows of every column are in flight together; string ranges follow.
 __device__ __forceinline__ void move_payload_rows(const RadixPayload& p, const int32_t (&pos)[kMoveBatch],
                                                   const int32_t (&row)[kMoveBatch])
 {
+  unsigned long long v[kPassPayload][kMoveBatch];
+#pragma unroll
+  for (int c = 0; c < kPassPayload; ++c)
+    if (c < p.n && p.src[c].width <= 8) {
+#pragma unroll
+      for (int k = 0; k < kMoveBatch; ++k) v[c][k] = pos[k] >= 0 ? ld_fixed(p.src[c], row[k]) : 0;
+    }
+#pragma unroll
+  for (int c = 0; c < kPassPayload; ++c)
+    if (c < p.n && p.src[c].width <= 8) {
+#pragma unroll
+      for (int k = 0; k < kMoveBatch; ++k)
+        if (pos[k] >= 0) st_fixed(p.dst[c], p.src[c].width, pos[k], v[c][k]);
+    }
   for (int c = 0; c < p.n; ++c) {
     const DCol& sc = p.src[c];
-    switch (sc.width) {
-      case 1: move_rows<uint8_t>(sc.data, p.dst[c], pos, row); break;
-      case 2: move_rows<uint16_t>(sc.data, p.dst[c], pos, row); break;
-      case 4: move_rows<uint32_t>(sc.data, p.dst[c], pos, row); break;
-      case 8: move_rows<unsigned long long>(sc.data, p.dst[c], pos, row); break;
-      default: move_rows<ulonglong2>(sc.data, p.dst[c], pos, row); break;
-    }
+    if (sc.width > 8) move_ranges(sc.data, p.dst[c], pos, row);
     if (p.dst_valid[c]) {
       uint8_t m[kMoveBatch];
 #pragma unroll
@@ -370,7 +388,7 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
   __syncthreads();
   const int64_t tbase = tile * RTILE;
   const int cnt       = static_cast<int>(a.n - tbase < RTILE ? a.n - tbase : RTILE);
-  if (!MOVE) {
+  if constexpr (!MOVE) {
     for (int j = threadIdx.x; j < cnt; j += RT) {
       const uint32_t d  = s_dig[j];
       const int64_t pos = static_cast<int64_t>(sh.gbase[d]) + (j - static_cast<int64_t>(sh.tile_start[d]));
@@ -378,28 +396,28 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
       a.vals_out[pos] = s_vals[j];
       if (a.inv_out) a.inv_out[s_vals[j]] = static_cast<int32_t>(pos);
     }
-    return;
-  }
-  // a pass that moves columns: kMoveBatch rows of a thread at a time, so the
-  // payload's loads (random rows after the first pass) overlap.  Positions
-  // and rows fit 32 bits (fewer than 2^31 rows).
-  for (int j0 = threadIdx.x; j0 < cnt; j0 += RT * kMoveBatch) {
-    int32_t pos[kMoveBatch], row[kMoveBatch];
+  } else {
+    // a pass that moves columns: kMoveBatch rows of a thread at a time, so the
+    // payload's loads (random rows after the first pass) overlap.  Positions
+    // and rows fit 32 bits (fewer than 2^31 rows).
+    for (int j0 = threadIdx.x; j0 < cnt; j0 += RT * kMoveBatch) {
+      int32_t pos[kMoveBatch], row[kMoveBatch];
 #pragma unroll
-    for (int k = 0; k < kMoveBatch; ++k) {
-      const int j = j0 + k * RT;
-      pos[k]      = -1;
-      row[k]      = 0;
-      if (j < cnt) {
-        const uint32_t d = s_dig[j];
-        pos[k]           = static_cast<int32_t>(sh.gbase[d] + static_cast<uint32_t>(j) - sh.tile_start[d]);
-        row[k]           = s_vals[j];
-        if (WRITE_KEYS) a.keys_out[pos[k]] = s_keys[j];
-        a.vals_out[pos[k]] = row[k];
-        if (a.inv_out) a.inv_out[row[k]] = pos[k];
+      for (int k = 0; k < kMoveBatch; ++k) {
+        const int j = j0 + k * RT;
+        pos[k]      = -1;
+        row[k]      = 0;
+        if (j < cnt) {
+          const uint32_t d = s_dig[j];
+          pos[k]           = static_cast<int32_t>(sh.gbase[d] + static_cast<uint32_t>(j) - sh.tile_start[d]);
+          row[k]           = s_vals[j];
+          if (WRITE_KEYS) a.keys_out[pos[k]] = s_keys[j];
+          a.vals_out[pos[k]] = row[k];
+          if (a.inv_out) a.inv_out[row[k]] = pos[k];
+        }
       }
+      move_payload_rows(a.pay, pos, row);
     }
-    move_payload_rows(a.pay, pos, row);
   }
 }
 
