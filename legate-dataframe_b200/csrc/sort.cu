@@ -158,12 +158,16 @@ __global__ void rank_scatter_kernel(const int32_t* perm, int64_t D, const int64_
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < D; i += (int64_t)gridDim.x * blockDim.x)
     rank[perm[i]] = static_cast<uint32_t>(scanned[i] + flags[i]);
 }
+// rank of every row's string (0 for null rows); with rep_out, also the
+// representative row of its string (-1 for null rows)
 __global__ void row_rank_kernel(const int32_t* row_slot, const int32_t* slot_id, const uint32_t* rank, int64_t n,
-                                uint32_t* out)
+                                uint32_t* out, const int32_t* repr, int32_t* rep_out)
 {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-    int32_t s = row_slot[r];
-    out[r]    = s >= 0 ? rank[slot_id[s]] : 0u;
+    const int32_t s = row_slot[r];
+    const int32_t d = s >= 0 ? slot_id[s] : -1;
+    out[r]          = d >= 0 ? rank[d] : 0u;
+    if (rep_out) rep_out[r] = d >= 0 ? repr[d] : -1;
   }
 }
 __global__ void max_len_kernel(DCol col, const int32_t* repr, int64_t D, unsigned long long* out)
@@ -187,6 +191,14 @@ DCol u32_col(const uint32_t* p)
   DCol d{};
   d.data  = p;
   d.type  = LDF_UINT32;
+  d.width = 4;
+  return d;
+}
+DCol i32_col(const int32_t* p)
+{
+  DCol d{};
+  d.data  = p;
+  d.type  = LDF_INT32;
   d.width = 4;
   return d;
 }
@@ -214,7 +226,10 @@ void add_word_passes(std::vector<RadixPass>& v, const SortKeyDesc& k)
 
 // Dense bytewise rank of every row's string (nulls get 0; they are ordered
 // by the CLASS pass).  `out` has n entries.
-void string_ranks(const OpContext& ctx, const DCol& col, int64_t n, uint32_t* out)
+// Rank of every row's string among the column's distinct strings (bytewise
+// order, shorter prefix first); rep_out (optional): a row holding the same
+// string for every row, -1 for null rows.
+void string_ranks(const OpContext& ctx, const DCol& col, int64_t n, uint32_t* out, int32_t* rep_out = nullptr)
 {
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
@@ -315,7 +330,8 @@ void string_ranks(const OpContext& ctx, const DCol& col, int64_t n, uint32_t* ou
       if (ndistinct_ranks == D) break;
     }
   }
-  launch("row_rank", row_rank_kernel, blocks_for(n), 256, 0, s, row_slot.get(), slot_id.get(), rank.get(), n, out);
+  launch("row_rank", row_rank_kernel, blocks_for(n), 256, 0, s, row_slot.get(), slot_id.get(), rank.get(), n, out,
+         static_cast<const int32_t*>(repr.get()), rep_out);
   LDF_CHECK_LAUNCH();
 }
 
@@ -343,25 +359,37 @@ namespace {
 // cache, instead of gathered through the permutation afterwards): fixed
 // widths straight into the allocated outputs, a string column's ranges (and
 // mask) into scratch in output order, from which move_strings_in_order then
-// copies its characters.
+// copies its characters.  A string column with representative rows (rep[j]:
+// for every row, a row holding the same string, -1 for null) moves those
+// 4-byte row ids instead, and its strings are then copied from the
+// representatives: as many source strings as distinct values, which stay in
+// L2 when there are few.
 struct PassMove {
   RadixPayload pay{};
   int col[kPassPayload];              // table column of each payload entry
+  bool by_rep[kPassPayload];          // the entry moves representative rows
   std::vector<char> moved;            // per table column
   std::vector<Buffer<uint8_t>> scratch;
 };
 
 void plan_pass_move(const Allocator& al, const ldf_column* table, int ncols, int64_t n, ldf_column* out,
-                    PassMove& m)
+                    PassMove& m, const std::vector<const int32_t*>* rep = nullptr)
 {
   m.moved.assign(ncols, 0);
   for (int j = 0; j < ncols && m.pay.n < kPassPayload; ++j) {
     const ldf_column& c = table[j];
     const int q         = m.pay.n++;
     m.col[q]            = j;
+    m.by_rep[q]         = false;
     m.moved[j]          = 1;
     m.pay.src[q]        = make_dcol(c);
-    if (c.type == LDF_STRING) {
+    if (c.type == LDF_STRING && rep && (*rep)[j]) {
+      m.by_rep[q]        = true;
+      m.pay.src[q]       = i32_col((*rep)[j]);
+      m.scratch.emplace_back(al, std::max<int64_t>(n, 1) * sizeof(int32_t));
+      m.pay.dst[q]       = m.scratch.back().get();
+      m.pay.dst_valid[q] = nullptr;
+    } else if (c.type == LDF_STRING) {
       m.scratch.emplace_back(al, std::max<int64_t>(n, 1) * sizeof(ldf_range));
       m.pay.dst[q]       = m.scratch.back().get();
       m.pay.dst_valid[q] = nullptr;
@@ -376,9 +404,14 @@ void plan_pass_move(const Allocator& al, const ldf_column* table, int ncols, int
   }
 }
 
-void move_strings_in_order(const OpContext& ctx, const PassMove& m, int64_t n, ldf_column* out)
+void move_strings_in_order(const OpContext& ctx, const ldf_column* table, const PassMove& m, int64_t n,
+                           ldf_column* out)
 {
   for (int q = 0; q < m.pay.n; ++q) {
+    if (m.by_rep[q]) {
+      gather_strings(ctx, make_dcol(table[m.col[q]]), static_cast<const int32_t*>(m.pay.dst[q]), n, out[m.col[q]]);
+      continue;
+    }
     const DCol& src = m.pay.src[q];
     if (src.type != LDF_STRING) continue;
     DCol ordered  = src;  // same characters; ranges and mask already in output order
@@ -400,7 +433,19 @@ void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const u
   const Allocator& al = ctx.alloc();
   const int64_t n     = ncols > 0 ? table[0].size : 0;
   LDF_REQUIRE(n < (int64_t(1) << 31), "tables of 2^31 rows or more per task are not supported");
+  int64_t first = 0, rows = n;
+  if (limit != INT64_MIN && (limit < 0 ? -limit : limit) < n) {
+    if (limit < 0) {
+      first = n + limit;
+      rows  = -limit;
+    } else {
+      rows = limit;
+    }
+  }
+  const bool whole = rows == n;
   std::vector<Buffer<uint32_t>> ranks;
+  std::vector<Buffer<int32_t>> reps;                   // representative rows of string keys
+  std::vector<const int32_t*> rep_of(ncols, nullptr);  // per table column
   std::vector<RadixPass> passes;
   // least significant key first
   for (int j = nkeys - 1; j >= 0; --j) {
@@ -411,7 +456,13 @@ void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const u
     k.nulls_at_end = nulls_at_end ? 1 : 0;
     if (c.type == LDF_STRING) {
       ranks.emplace_back(al, std::max<int64_t>(n, 1));
-      string_ranks(ctx, k.col, n, ranks.back().get());
+      int32_t* rep = nullptr;
+      if (whole && keys[j] < kPassPayload) {  // a column the last pass moves
+        reps.emplace_back(al, std::max<int64_t>(n, 1));
+        rep            = reps.back().get();
+        rep_of[keys[j]] = rep;
+      }
+      string_ranks(ctx, k.col, n, ranks.back().get(), rep);
       DCol rc  = u32_col(ranks.back().get());
       rc.valid = c.valid;
       k.col    = rc;
@@ -426,28 +477,20 @@ void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const u
     }
   }
   Buffer<int32_t> perm(al, std::max<int64_t>(n, 1));
-  int64_t first = 0, rows = n;
-  if (limit != INT64_MIN && (limit < 0 ? -limit : limit) < n) {
-    if (limit < 0) {
-      first = n + limit;
-      rows  = -limit;
-    } else {
-      rows = limit;
-    }
-  }
-  if (rows < n) {
+  if (!whole) {
     radix_sort_rows(ctx, passes, n, perm.get());
     gather_table(ctx, table, ncols, perm.get() + first, rows, out);
     ctx.finish();
     return;
   }
-  // the whole table: the last pass moves the first kPassPayload columns, the
-  // rest are gathered through the permutation
+  // the whole table: the last pass moves the first kPassPayload columns
+  // (string keys as their representative rows), the rest are gathered
+  // through the permutation
   for (int j = 0; j < ncols; ++j) out[j] = alloc_out_column(al, table[j].type, n, table[j].valid != nullptr);
   PassMove mv;
-  plan_pass_move(al, table, ncols, n, out, mv);
+  plan_pass_move(al, table, ncols, n, out, mv, &rep_of);
   radix_sort_rows(ctx, passes, n, perm.get(), nullptr, nullptr, &mv.pay);
-  move_strings_in_order(ctx, mv, n, out);
+  move_strings_in_order(ctx, table, mv, n, out);
   std::vector<DCol> fsrc;
   std::vector<ldf_column*> fdst;
   for (int j = 0; j < ncols; ++j) {
@@ -543,7 +586,7 @@ void hash_partition(const ldf_column* table, int ncols, const int32_t* keys, int
   std::vector<unsigned long long> h(nparts);
   LDF_CUDA(cudaMemcpyAsync(h.data(), counts.get(), static_cast<size_t>(nparts) * 8, cudaMemcpyDeviceToHost, s));
   scatter_fixed_columns(ctx, fsrc.data(), inv.get(), n, fdst.data(), static_cast<int>(fsrc.size()));
-  move_strings_in_order(ctx, mv, n, out);
+  move_strings_in_order(ctx, table, mv, n, out);
   for (int j = 0; j < ncols; ++j)
     if (table[j].type == LDF_STRING && !mv.moved[j]) gather_strings(ctx, make_dcol(table[j]), perm.get(), n, out[j]);
   ctx.finish();
