@@ -177,31 +177,9 @@ struct PassArgs {
   uint64_t* status;            // [tiles * 256]
   unsigned long long* counter;
   int32_t* inv_out;  // != null: inv_out[row] = the row's output position
-  RadixPayload pay;  // columns moved by this pass (pay.n = 0: none)
+  RadixPayload pay;  // columns moved by this pass (payload_empty: none)
   int* err;
 };
-
-// dst[pos] = src[row] for every payload column.
-__device__ __forceinline__ void move_payload(const RadixPayload& p, int64_t pos, int64_t row)
-{
-  for (int c = 0; c < p.n; ++c) {
-    const DCol& sc = p.src[c];
-    switch (sc.width) {
-      case 1: static_cast<uint8_t*>(p.dst[c])[pos] = __ldg(static_cast<const uint8_t*>(sc.data) + row); break;
-      case 2: static_cast<uint16_t*>(p.dst[c])[pos] = __ldg(static_cast<const uint16_t*>(sc.data) + row); break;
-      case 4: static_cast<uint32_t*>(p.dst[c])[pos] = __ldg(static_cast<const uint32_t*>(sc.data) + row); break;
-      case 8:
-        static_cast<unsigned long long*>(p.dst[c])[pos] = __ldg(static_cast<const unsigned long long*>(sc.data) + row);
-        break;
-      default: {  // 16: string ranges (8-byte aligned at the source; the scratch is 16-byte aligned)
-        const unsigned long long* r = static_cast<const unsigned long long*>(sc.data) + 2 * row;
-        static_cast<ulonglong2*>(p.dst[c])[pos] = make_ulonglong2(__ldg(r), __ldg(r + 1));
-        break;
-      }
-    }
-    if (p.dst_valid[c]) p.dst_valid[c][pos] = dvalid(sc, row) ? 1 : 0;
-  }
-}
 
 // Rows of a thread whose payload loads are issued together in a pass that
 // moves columns.
@@ -233,7 +211,7 @@ __device__ __forceinline__ unsigned long long ld_fixed(const DCol& c, int32_t ro
   }
 }
 
-__device__ __forceinline__ void st_fixed(void* dst, int width, int32_t pos, unsigned long long v)
+__device__ __forceinline__ void st_fixed(void* dst, int width, int64_t pos, unsigned long long v)
 {
   switch (width) {
     case 1: static_cast<uint8_t*>(dst)[pos] = static_cast<uint8_t>(v); break;
@@ -243,12 +221,48 @@ __device__ __forceinline__ void st_fixed(void* dst, int width, int32_t pos, unsi
   }
 }
 
+// Part of a packed payload record at byte offset `off` (the store truncates it
+// to the part's width).
+__device__ __forceinline__ unsigned long long record_part(const ulonglong2& r, int off)
+{
+  return (off < 8 ? r.x : r.y) >> ((off & 7) * 8);
+}
+
+// dst[pos] = src[row] for every payload column (one row: the identity copy).
+__device__ __forceinline__ void move_payload(const RadixPayload& p, int64_t pos, int64_t row)
+{
+  if (p.nparts) {
+    const ulonglong2 r = __ldg(p.packed + row);
+    for (int k = 0; k < p.nparts; ++k) st_fixed(p.pdst[k], p.pwidth[k], pos, record_part(r, p.poff[k]));
+  }
+  for (int c = 0; c < p.n; ++c) {
+    const DCol& sc = p.src[c];
+    if (sc.width <= 8) {
+      st_fixed(p.dst[c], sc.width, pos, ld_fixed(sc, static_cast<int32_t>(row)));
+    } else {  // 16: string ranges (8-byte aligned at the source; the scratch is 16-byte aligned)
+      const unsigned long long* r = static_cast<const unsigned long long*>(sc.data) + 2 * row;
+      static_cast<ulonglong2*>(p.dst[c])[pos] = make_ulonglong2(__ldg(r), __ldg(r + 1));
+    }
+    if (p.dst_valid[c]) p.dst_valid[c][pos] = dvalid(sc, row) ? 1 : 0;
+  }
+}
+
 // Every payload column's values (and masks) of kMoveBatch rows.  The loads
 // of all fixed-width columns are issued before the first store, so the
 // random rows of every column are in flight together; string ranges follow.
 __device__ __forceinline__ void move_payload_rows(const RadixPayload& p, const int32_t (&pos)[kMoveBatch],
                                                   const int32_t (&row)[kMoveBatch])
 {
+  if (p.nparts) {
+    ulonglong2 rv[kMoveBatch];
+#pragma unroll
+    for (int k = 0; k < kMoveBatch; ++k)
+      if (pos[k] >= 0) rv[k] = __ldg(p.packed + row[k]);
+#pragma unroll
+    for (int k = 0; k < kMoveBatch; ++k)
+      if (pos[k] >= 0)
+        for (int q = 0; q < p.nparts; ++q) st_fixed(p.pdst[q], p.pwidth[q], pos[k], record_part(rv[k], p.poff[q]));
+  }
   unsigned long long v[kPassPayload][kMoveBatch];
 #pragma unroll
   for (int c = 0; c < kPassPayload; ++c)
@@ -571,7 +585,8 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
   if (run.empty()) {
     if (n > 0) launch("iota", iota_kernel, hblocks(n), RT, 0, s, perm, n);
     if (n > 0 && inv) launch("iota", iota_kernel, hblocks(n), RT, 0, s, inv, n);
-    if (n > 0 && payload && payload->n) launch("copy_payload", copy_payload_kernel, hblocks(n), RT, 0, s, *payload, n);
+    if (n > 0 && payload && !payload_empty(*payload))
+      launch("copy_payload", copy_payload_kernel, hblocks(n), RT, 0, s, *payload, n);
     LDF_CHECK_LAUNCH();
     return;
   }
@@ -616,7 +631,7 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
     if (k + 1 == run.size() && payload) a.pay = *payload;
     a.err        = ctx.err();
     const unsigned g = static_cast<unsigned>(tiles);
-    const bool move = a.pay.n > 0;
+    const bool move = !payload_empty(a.pay);
     if (move && gather) launch_onesweep<true, false, true>(s, g, a);
     else if (move) launch_onesweep<false, false, true>(s, g, a);
     else if (gather && write_keys) launch_onesweep<true, true>(s, g, a);

@@ -56,13 +56,24 @@ void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes
 // src[j][row] (and the null masks), written as the pass's coalesced runs
 // while the tile's source rows are still in cache.  Widths 1, 2, 4, 8, and 16
 // (the ranges of a string column; its characters stay where they are).
+// A payload may also carry one 16-byte record per row (`packed`, 16-byte
+// aligned) holding up to kPassPayload non-nullable fixed-width values: part k
+// is pwidth[k] bytes at byte offset poff[k] (a multiple of its width) and goes
+// to pdst[k].  One random load per row then serves all of them.
 constexpr int kPassPayload = 4;
 struct RadixPayload {
   int n;
   DCol src[kPassPayload];
   void* dst[kPassPayload];
   uint8_t* dst_valid[kPassPayload];
+  const ulonglong2* packed;
+  int nparts;
+  int pwidth[kPassPayload];
+  int poff[kPassPayload];
+  void* pdst[kPassPayload];
 };
+
+inline bool payload_empty(const RadixPayload& p) { return p.n == 0 && p.nparts == 0; }
 
 // `inv` (optional, n entries): inv[row] = the row's position in the sorted
 // order, written by the last pass.  `payload` (optional): columns the last

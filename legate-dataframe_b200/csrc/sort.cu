@@ -19,6 +19,8 @@
 // keys into a bucket id per row (and counts the buckets), then one stable
 // radix pass on the bucket ids (two for more than 256 buckets) that also
 // moves up to four columns into bucket order itself.
+#include <algorithm>
+
 #include "radix.cuh"
 
 namespace ldf {
@@ -404,6 +406,81 @@ void plan_pass_move(const Allocator& al, const ldf_column* table, int ncols, int
   }
 }
 
+struct PackArgs {
+  const void* src[kPassPayload];
+  int width[kPassPayload];
+  int off[kPassPayload];
+  int nparts;
+};
+
+// rec[r] = the parts of row r at their byte offsets (in order over the rows)
+__global__ void pack_records_kernel(PackArgs a, int64_t n, ulonglong2* rec)
+{
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    unsigned long long w[2] = {0, 0};
+    for (int q = 0; q < a.nparts; ++q) {
+      unsigned long long v;
+      switch (a.width[q]) {
+        case 1: v = static_cast<const uint8_t*>(a.src[q])[r]; break;
+        case 2: v = static_cast<const uint16_t*>(a.src[q])[r]; break;
+        case 4: v = static_cast<const uint32_t*>(a.src[q])[r]; break;
+        default: v = static_cast<const unsigned long long*>(a.src[q])[r]; break;
+      }
+      w[a.off[q] >> 3] |= v << ((a.off[q] & 7) * 8);
+    }
+    rec[r] = make_ulonglong2(w[0], w[1]);
+  }
+}
+
+// The payload a pass over rows in random order runs with: the non-nullable
+// fixed-width entries of `pay` (representative rows included) packed into
+// one 16-byte record per row while they fit, widest first so that every part
+// sits at an offset that is a multiple of its width, and the other entries
+// as they are.  The pass then loads one record per row instead of one value
+// per column; packing costs one read and write of the records in order.
+RadixPayload pack_payload(const OpContext& ctx, const RadixPayload& pay, int64_t n, Buffer<ulonglong2>& rec)
+{
+  int order[kPassPayload];
+  int m = 0;
+  for (int q = 0; q < pay.n; ++q) {
+    const DCol& c = pay.src[q];
+    if (c.type != LDF_STRING && c.width <= 8 && c.valid == nullptr && pay.dst_valid[q] == nullptr) order[m++] = q;
+  }
+  std::stable_sort(order, order + m, [&](int x, int y) { return pay.src[x].width > pay.src[y].width; });
+  RadixPayload out{};
+  PackArgs pa{};
+  bool in_rec[kPassPayload] = {};
+  int used                  = 0;
+  for (int i = 0; i < m; ++i) {
+    const int q = order[i];
+    const int w = pay.src[q].width;
+    if (used + w > 16) continue;
+    in_rec[q]              = true;
+    pa.src[pa.nparts]      = pay.src[q].data;
+    pa.width[pa.nparts]    = w;
+    pa.off[pa.nparts]      = used;
+    out.pdst[pa.nparts]    = pay.dst[q];
+    out.pwidth[pa.nparts]  = w;
+    out.poff[pa.nparts]    = used;
+    used += w;
+    ++pa.nparts;
+  }
+  if (pa.nparts < 2 || n == 0) return pay;
+  out.nparts = pa.nparts;
+  for (int q = 0; q < pay.n; ++q) {
+    if (in_rec[q]) continue;
+    out.src[out.n]       = pay.src[q];
+    out.dst[out.n]       = pay.dst[q];
+    out.dst_valid[out.n] = pay.dst_valid[q];
+    ++out.n;
+  }
+  rec = Buffer<ulonglong2>(ctx.alloc(), static_cast<size_t>(n));
+  launch("pack_records", pack_records_kernel, blocks_for(n), 256, 0, ctx.stream(), pa, n, rec.get());
+  LDF_CHECK_LAUNCH();
+  out.packed = rec.get();
+  return out;
+}
+
 void move_strings_in_order(const OpContext& ctx, const ldf_column* table, const PassMove& m, int64_t n,
                            ldf_column* out)
 {
@@ -489,7 +566,9 @@ void sort_table(const ldf_column* table, int ncols, const int32_t* keys, const u
   for (int j = 0; j < ncols; ++j) out[j] = alloc_out_column(al, table[j].type, n, table[j].valid != nullptr);
   PassMove mv;
   plan_pass_move(al, table, ncols, n, out, mv, &rep_of);
-  radix_sort_rows(ctx, passes, n, perm.get(), nullptr, nullptr, &mv.pay);
+  Buffer<ulonglong2> rec;
+  const RadixPayload pay = pack_payload(ctx, mv.pay, n, rec);
+  radix_sort_rows(ctx, passes, n, perm.get(), nullptr, nullptr, &pay);
   move_strings_in_order(ctx, table, mv, n, out);
   std::vector<DCol> fsrc;
   std::vector<ldf_column*> fdst;

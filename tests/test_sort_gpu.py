@@ -164,3 +164,35 @@ def test_sort_wide_table_moved_and_gathered_columns():
             assert_tables_equal(res, R.sort(t, keys, asc, nulls_at_end), sort_by=None)
     const = t.append_column("c", pa.array(np.zeros(n, np.int32)))
     assert_tables_equal(run_sort(const, ["c"]), const, sort_by=None)
+
+
+@pytest.mark.parametrize("const_key", [False, True])
+def test_sort_packed_payload_records(const_key):
+    """Non-nullable fixed-width columns among the four the last pass moves
+    (a string key's representative rows included) travel packed in one
+    16-byte record per row: 8+4+4 bytes with a string key, 8+4+2+1 bytes of
+    integers; a constant key runs no pass and copies the records in order."""
+    rng = np.random.default_rng(31)
+    n = 150_000
+    words = np.array([f"k{i}" + "x" * (i % 17) for i in range(3000)], dtype=object)
+    key = np.zeros(n, np.int32) if const_key else rng.integers(0, 50, n).astype(np.int32)
+    t1 = pa.table({
+        "s": pa.array(words[rng.integers(0, len(words), n)], pa.string(), mask=rng.random(n) < 0.04),
+        "ts": rng.integers(-(2**62), 2**62, n),
+        "v": rng.normal(size=n).astype(np.float32),
+        "h": rng.integers(-(2**15), 2**15, n).astype(np.int16),
+        "k": key,
+        "row": np.arange(n),
+    })
+    t2 = pa.table({
+        "b": rng.integers(-128, 128, n).astype(np.int8),
+        "h": rng.integers(-(2**15), 2**15, n).astype(np.int16),
+        "i": rng.integers(-(2**31), 2**31, n).astype(np.int32),
+        "l": rng.integers(-(2**63), 2**63 - 1, n, dtype=np.int64),
+        "k": key,
+        "row": np.arange(n),
+    })
+    for t, keys in ((t1, ["k", "s"] if not const_key else ["k"]), (t1, ["s"]), (t2, ["k", "h"]), (t2, ["k"])):
+        for asc in (True, False):
+            res = run_sort(t, keys, [asc] * len(keys))
+            assert_tables_equal(res, R.sort(t, keys, [asc] * len(keys), True), sort_by=None)
