@@ -413,22 +413,41 @@ struct PackArgs {
   int nparts;
 };
 
-// rec[r] = the parts of row r at their byte offsets (in order over the rows)
-__global__ void pack_records_kernel(PackArgs a, int64_t n, ulonglong2* rec)
+constexpr int kPackRows = 4;  // rows per thread, their loads in flight together
+
+__device__ __forceinline__ unsigned long long load_part(const void* p, int width, int64_t r)
 {
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-    unsigned long long w[2] = {0, 0};
-    for (int q = 0; q < a.nparts; ++q) {
-      unsigned long long v;
-      switch (a.width[q]) {
-        case 1: v = static_cast<const uint8_t*>(a.src[q])[r]; break;
-        case 2: v = static_cast<const uint16_t*>(a.src[q])[r]; break;
-        case 4: v = static_cast<const uint32_t*>(a.src[q])[r]; break;
-        default: v = static_cast<const unsigned long long*>(a.src[q])[r]; break;
+  switch (width) {
+    case 1: return static_cast<const uint8_t*>(p)[r];
+    case 2: return static_cast<const uint16_t*>(p)[r];
+    case 4: return static_cast<const uint32_t*>(p)[r];
+    default: return static_cast<const unsigned long long*>(p)[r];
+  }
+}
+
+// rec[r] = the parts of row r at their byte offsets (in order over the rows)
+__global__ void __launch_bounds__(256) pack_records_kernel(PackArgs a, int64_t n, ulonglong2* rec)
+{
+  const int64_t per = static_cast<int64_t>(blockDim.x) * kPackRows;
+  for (int64_t base = blockIdx.x * per; base < n; base += static_cast<int64_t>(gridDim.x) * per) {
+    unsigned long long v[kPassPayload][kPackRows];
+#pragma unroll
+    for (int q = 0; q < kPassPayload; ++q)
+#pragma unroll
+      for (int k = 0; k < kPackRows; ++k) {
+        const int64_t r = base + k * blockDim.x + threadIdx.x;
+        v[q][k]         = q < a.nparts && r < n ? load_part(a.src[q], a.width[q], r) : 0;
       }
-      w[a.off[q] >> 3] |= v << ((a.off[q] & 7) * 8);
+#pragma unroll
+    for (int k = 0; k < kPackRows; ++k) {
+      const int64_t r = base + k * blockDim.x + threadIdx.x;
+      if (r >= n) continue;
+      unsigned long long w[2] = {0, 0};
+#pragma unroll
+      for (int q = 0; q < kPassPayload; ++q)
+        if (q < a.nparts) w[a.off[q] >> 3] |= v[q][k] << ((a.off[q] & 7) * 8);
+      rec[r] = make_ulonglong2(w[0], w[1]);
     }
-    rec[r] = make_ulonglong2(w[0], w[1]);
   }
 }
 
@@ -475,7 +494,8 @@ RadixPayload pack_payload(const OpContext& ctx, const RadixPayload& pay, int64_t
     ++out.n;
   }
   rec = Buffer<ulonglong2>(ctx.alloc(), static_cast<size_t>(n));
-  launch("pack_records", pack_records_kernel, blocks_for(n), 256, 0, ctx.stream(), pa, n, rec.get());
+  launch("pack_records", pack_records_kernel, blocks_for(ceil_div(n, int64_t(kPackRows))), 256, 0, ctx.stream(), pa, n,
+         rec.get());
   LDF_CHECK_LAUNCH();
   out.packed = rec.get();
   return out;
