@@ -3,9 +3,10 @@
 10% nulls; int32 U[0, 1e6)); SUM and MEAN of the float64 column, COUNT(*) and
 COUNT of the float64 column, MIN/MAX and NUNIQUE of the int32 column.
 
-`--workload join` / `--workload strings` instead print one line per op of
-the 200M x 20M int32-key joins / the 100M-row string-key groupby, stable sort
-and hash partition (device ms, rows/s, per-kernel ms).
+`--workload join` / `--workload strings` / `--workload sort` instead print one
+line per op of the 200M x 20M int32-key joins / the 100M-row string-key
+groupby, stable sort and hash partition / a 100M-row int64-key sort (device
+ms, rows/s, per-kernel ms).
 
 One step = one groupby_aggregation call through the public API (C ABI) on
 device-resident inputs (4.2 GB, far larger than the 126 MB L2, so no flush is
@@ -446,6 +447,34 @@ def run_strings_workload(args):
     return 0
 
 
+def run_sort_workload(args):
+    """--rows (default 100M) rows: uniform random int64 key over
+    [-2^62, 2^62) and an int32 payload; stable ascending sort on the key."""
+    import pyarrow as pa
+    import torch
+
+    from legate_dataframe import LogicalColumn, LogicalTable
+    from legate_dataframe import _native as N
+    from legate_dataframe.lib.sort import sort
+
+    dev = torch.device("cuda", 0)
+    n = args.rows
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    k = torch.randint(-(2**62), 2**62, (n,), device=dev, generator=g)
+    v = torch.arange(n, device=dev, dtype=torch.int32)
+    t = LogicalTable([LogicalColumn.from_torch(k, pa.int64()), LogicalColumn.from_torch(v, pa.int32())], ["k", "v"])
+    algo = 2 * n * 12  # key + payload in, sorted table out
+    peak, kind = measured_peak_gbs()
+    ms, rows, kern = _profiled(N, lambda: sort(t, ["k"], stable=True), args.steps)
+    print(json.dumps({"workload": f"stable sort (int64 key, int32 payload): {n} rows", "ms": round(ms, 3),
+                      "rows_per_s": n / (ms / 1e3), "out_rows": rows,
+                      "op_GBps_algorithmic": algo / (ms / 1e3) / 1e9,
+                      "op_frac_of_peak": algo / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
+                      "kernels_ms": kern}), flush=True)
+    return 0
+
+
 def run_ingest_workload(args):
     """--rows (default 20M) rows as a host Arrow table shaped like the string
     workload (string key from a 2M-entry dictionary, 10% null int64 ts,
@@ -530,16 +559,18 @@ def main():
     ap.add_argument("--served-requests", type=int, default=8192)
     ap.add_argument("--ref-rows", type=int, default=8_000_000, help="rows per step of the reference arm")
     ap.add_argument("--ops", default="", help="--workload strings: comma list of groupby,sort,partition (default all)")
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "join", "strings", "ingest"],
-                    help="groupby = the benchmark line; join / strings / ingest print per-op lines")
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "join", "strings", "sort", "ingest"],
+                    help="groupby = the benchmark line; join / strings / sort / ingest print per-op lines")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload != "groupby":
-        if args.rows == N_ROWS and args.workload in ("strings", "ingest"):
-            args.rows = 100_000_000 if args.workload == "strings" else 20_000_000
+        if args.rows == N_ROWS and args.workload in ("strings", "sort", "ingest"):
+            args.rows = 20_000_000 if args.workload == "ingest" else 100_000_000
         if args.workload == "ingest":
             return run_ingest_workload(args)
+        if args.workload == "sort":
+            return run_sort_workload(args)
         return run_join_workload(args) if args.workload == "join" else run_strings_workload(args)
 
     import torch
