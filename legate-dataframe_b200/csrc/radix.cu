@@ -247,9 +247,10 @@ __device__ __forceinline__ void move_payload(const RadixPayload& p, int64_t pos,
   }
 }
 
-// Every payload column's values (and masks) of kMoveBatch rows.  The loads
-// of all fixed-width columns are issued before the first store, so the
-// random rows of every column are in flight together; string ranges follow.
+// Every payload column's values (and masks) of kMoveBatch rows: the packed
+// records first (one load per row for all their parts), then the other
+// fixed-width columns with all their loads issued before the first store, so
+// that their random rows are in flight together, then string ranges.
 __device__ __forceinline__ void move_payload_rows(const RadixPayload& p, const int32_t (&pos)[kMoveBatch],
                                                   const int32_t (&row)[kMoveBatch])
 {
@@ -425,7 +426,6 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
           const uint32_t d = s_dig[j];
           pos[k]           = static_cast<int32_t>(sh.gbase[d] + static_cast<uint32_t>(j) - sh.tile_start[d]);
           row[k]           = s_vals[j];
-          if (WRITE_KEYS) a.keys_out[pos[k]] = s_keys[j];
           a.vals_out[pos[k]] = row[k];
           if (a.inv_out) a.inv_out[row[k]] = pos[k];
         }

@@ -13,6 +13,12 @@
 // chunks (rank of the previous chunks as the major key), and every row then
 // sorts on the uint32 rank.
 //
+// Output: a sort that returns the whole table lets its last radix pass move
+// the first four columns into sorted order (the non-nullable fixed-width ones
+// packed into one 16-byte record per row, a string key as the row id of a
+// representative of its string, other strings as their ranges); the other
+// columns, and the rows of a `limit`, are gathered through the permutation.
+//
 // hash_partition: reference task::repartition_by_hash local step
 // (cpp/src/core/repartition_by_hash.cu:296-310): bucket = hash(keys) % nparts,
 // rows grouped by bucket, start offsets returned; here one pass hashes the
