@@ -1,21 +1,32 @@
-"""Benchmark of the B200 relational hot path: hash groupby aggregation,
-200M rows (Zipf(1.1) int64 keys over 10M distinct values; float64 N(0,1) with
-10% nulls; int32 U[0, 1e6)); SUM and MEAN of the float64 column, COUNT(*) and
-COUNT of the float64 column, MIN/MAX and NUNIQUE of the int32 column.
+"""Benchmark of the B200 relational hot path.
 
-`--workload join` / `--workload strings` / `--workload sort` instead print one
-line per op of the 200M x 20M int32-key joins / the 100M-row string-key
-groupby, stable sort and hash partition / a 100M-row int64-key sort (device
-ms, rows/s, per-kernel ms).
+The headline line is hash groupby aggregation, 200M rows (Zipf(1.1) int64
+keys over 10M distinct values; float64 N(0,1) with 10% nulls; int32
+U[0, 1e6)); SUM and MEAN of the float64 column, COUNT(*) and COUNT of the
+float64 column, MIN/MAX and NUNIQUE of the int32 column.  One step = one
+groupby_aggregation call through the public API (C ABI) on device-resident
+inputs (4.2 GB, far larger than the 126 MB L2, so no flush is needed).  The
+step's result is checked outside the timed region (`parity`).
 
-One step = one groupby_aggregation call through the public API (C ABI) on
-device-resident inputs (4.2 GB, far larger than the 126 MB L2, so no flush is
-needed).  Prints ONE JSON line (rank 0).  At N=1 the line also carries
-`served`: the batched/served mix (8,192 small joins and groupbys arriving at
-2,000 req/s) through the continuous-batching server and, for comparison, the
-same requests issued one op per launch (--no-served skips it).
+At N=1 the same JSON line also carries
+  * `joins`: inner / left / full hash joins, 200M probe x 20M build rows
+    (int32 keys, 5% null probe keys, Zipf(0.9) hits);
+  * `strings`: 100M string-key rows: groupby SUM/COUNT(*), stable sort
+    (key asc, ts desc), hash_partition into 256 buckets;
+  * `served`: the batched/served mix (8,192 small joins and groupbys arriving
+    at 2,000 req/s) through the continuous-batching server and, for
+    comparison, the same requests issued one op per launch.
+(--no-joins / --no-strings / --no-served skip them.)
+
+`--workload join|strings|sort|ingest` instead prints one line per op.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the reference's CPU implementation of the path (the
+Arrow Acero calls of GroupByAggregationTask::cpu_variant) on the same
+200M-row workload every step: the rows hash-sharded over the host cores, one
+single-threaded task body per shard, all shards at once (legate --cpus N;
+the shuffle itself is not timed).
 
 Multi-GPU runs (torchrun) are independent replicas: the path is a single-GPU
 task body and shards by rows with no data-path collective (weak scaling);
@@ -40,16 +51,7 @@ sys.path.insert(0, str(ROOT / "legate-dataframe_b200"))
 
 METRIC = "join/groupby rows/s + % HBM roofline (1 B200); batched p50/p99 vs unbatched"
 N_ROWS = 200_000_000
-N_KEYS = 10_000_000
-AGGS = [
-    ("v", "sum", "sum_v"),
-    ("v", "mean", "mean_v"),
-    (None, "count_all", "count"),
-    ("v", "count", "count_v"),
-    ("i", "min", "min_i"),
-    ("i", "max", "max_i"),
-    ("i", "count_distinct", "nunique_i"),
-]
+from legate_dataframe.workloads import GROUPBY_AGGS as AGGS  # noqa: E402
 IN_BYTES_PER_ROW = 8 + 8 + 1 + 4  # key + f64 + its null mask + i32 (legate layout)
 
 
@@ -63,61 +65,11 @@ def measured_peak_gbs():
     return 6650.0, "fallback"
 
 
-# ---------------------------------------------------------------------------
-# synthetic input (seeded, generated on the device)
-# ---------------------------------------------------------------------------
-def make_input_device(n_rows: int, device):
-    import torch
-
-    g = torch.Generator(device=device)
-    ranks = torch.arange(1, N_KEYS + 1, device=device, dtype=torch.float64)
-    w = ranks.pow(-1.1)
-    cdf = torch.cumsum(w, 0)
-    cdf /= cdf[-1].clone()
-    g.manual_seed(3)
-    perm = torch.randperm(N_KEYS, device=device, generator=g)
-    key_values = perm.to(torch.int64) * 2_654_435_761 + 12_345  # 10M distinct int64 values
-    keys = torch.empty(n_rows, dtype=torch.int64, device=device)
-    g.manual_seed(1)
-    chunk = 50_000_000
-    for s in range(0, n_rows, chunk):
-        e = min(n_rows, s + chunk)
-        u = torch.rand(e - s, dtype=torch.float64, device=device, generator=g)
-        r = torch.searchsorted(cdf, u).clamp_(max=N_KEYS - 1)
-        keys[s:e] = key_values[r]
-        del u, r
-    del cdf, w, ranks, perm
-    g.manual_seed(4)
-    v = torch.randn(n_rows, dtype=torch.float64, device=device, generator=g)
-    valid = (torch.rand(n_rows, device=device, generator=g) >= 0.10).to(torch.uint8)
-    g.manual_seed(5)
-    i = torch.randint(0, 1_000_000, (n_rows,), dtype=torch.int32, device=device, generator=g)
-    torch.cuda.synchronize(device)
-    return keys, v, valid, i
-
-
-def device_table(keys, v, valid, i):
+def host_table(keys, v, valid, i):
     import pyarrow as pa
 
-    from legate_dataframe import LogicalColumn, LogicalTable
-
-    cols = [
-        LogicalColumn.from_torch(keys, pa.int64()),
-        LogicalColumn.from_torch(v, pa.float64(), valid),
-        LogicalColumn.from_torch(i, pa.int32()),
-    ]
-    return LogicalTable(cols, ["k", "v", "i"])
-
-
-def host_sample(keys, v, valid, i, n):
-    import numpy as np
-    import pyarrow as pa
-
-    k = keys[:n].cpu().numpy()
-    vv = v[:n].cpu().numpy()
-    m = valid[:n].cpu().numpy().astype(bool)
-    ii = i[:n].cpu().numpy()
-    return pa.table({"k": k, "v": pa.array(vv, mask=~m), "i": ii})
+    return pa.table({"k": keys.cpu().numpy(), "v": pa.array(v.cpu().numpy(), mask=valid.cpu().numpy() == 0),
+                     "i": i.cpu().numpy()})
 
 
 def output_bytes(tbl) -> int:
@@ -195,69 +147,144 @@ def max_over_ranks(value: float, world: int, device) -> float:
 
 
 # ---------------------------------------------------------------------------
-# CPU baselines: the reference's CPU path (Arrow Acero aggregate, the calls of
-# GroupByAggregationTask::cpu_variant) on a bounded sample
+# CPU side: the reference's CPU path (Arrow Acero aggregate, the calls of
+# GroupByAggregationTask::cpu_variant, one single-threaded task body per
+# legate CPU) on hash shards of the same workload
 # ---------------------------------------------------------------------------
-def cpu_groupby_rate(sample, use_threads: bool, min_seconds: float = 10.0):
-    from oracle import arrow_ref
-
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        arrow_ref.groupby(sample, ["k"], AGGS, use_threads=use_threads)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el >= min_seconds or reps >= 20:
-            break
-    return sample.num_rows * reps / el, el, reps
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
-def run_reference(args):
-    """--impl reference: the reference's CPU implementation of the path (Arrow
-    Acero aggregate) with every host thread, on bounded samples."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
+def shard_of(keys, nshards: int):
+    """Hash shard of every int64 key (multiplicative hash, top bits), as
+    legate's hash repartitioning sends each key's rows to one CPU task."""
+    import numpy as np
+
+    with np.errstate(over="ignore"):
+        h = keys.view(np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+    return ((h >> np.uint64(32)) % np.uint64(nshards)).astype(np.uint8)
+
+
+def reference_shards(n: int, nshards: int, threads: int):
+    """The 200M-row groupby workload on the host (numpy, seeded; the same
+    distributions as the device generator), cut into `nshards` hash shards
+    of the key: a list of Arrow tables.  Rows are generated in chunks on
+    `threads` threads; each chunk is split by shard, and a shard's table is
+    the concatenation of its pieces (no further copy)."""
+    from concurrent.futures import ThreadPoolExecutor
+
     import numpy as np
     import pyarrow as pa
 
-    n = args.ref_rows
-    rng = np.random.default_rng(3)
-    ranks = np.arange(1, N_KEYS + 1, dtype=np.float64)
-    cdf = np.cumsum(ranks ** -1.1)
+    from legate_dataframe import workloads as W
+
+    nk = W.GROUPBY_KEYS
+    cdf = np.cumsum(np.arange(1, nk + 1, dtype=np.float64) ** -1.1)
     cdf /= cdf[-1]
-    key_values = rng.permutation(N_KEYS).astype(np.int64) * 2_654_435_761 + 12_345
-    k = key_values[np.minimum(np.searchsorted(cdf, np.random.default_rng(1).random(n)), N_KEYS - 1)]
-    r4 = np.random.default_rng(4)
-    v = r4.normal(size=n)
-    m = r4.random(n) < 0.10
-    i = np.random.default_rng(5).integers(0, 1_000_000, n).astype(np.int32)
-    sample = pa.table({"k": k, "v": pa.array(v, mask=m), "i": i})
+    key_values = np.random.default_rng(3).permutation(nk).astype(np.int64) * 2_654_435_761 + 12_345
+    nchunks = max(threads, 1)
+    bounds = [n * c // nchunks for c in range(nchunks + 1)]
+
+    def chunk(c):
+        m = bounds[c + 1] - bounds[c]
+        rng = np.random.default_rng([1, c])
+        k = key_values[np.minimum(np.searchsorted(cdf, rng.random(m)), nk - 1)]
+        v = rng.normal(size=m)
+        null = rng.random(m) < 0.10
+        i = rng.integers(0, 1_000_000, m).astype(np.int32)
+        s = shard_of(k, nshards)
+        order = np.argsort(s, kind="stable")
+        off = np.zeros(nshards + 1, np.int64)
+        np.cumsum(np.bincount(s, minlength=nshards), out=off[1:])
+        k, v, null, i = k[order], v[order], null[order], i[order]
+        return [pa.table({"k": k[off[j]:off[j + 1]], "v": pa.array(v[off[j]:off[j + 1]], mask=null[off[j]:off[j + 1]]),
+                          "i": i[off[j]:off[j + 1]]}) for j in range(nshards)]
+
+    with ThreadPoolExecutor(nchunks) as ex:
+        pieces = list(ex.map(chunk, range(nchunks)))
+    return [pa.concat_tables([p[j] for p in pieces]) for j in range(nshards)]
+
+
+def run_shards(shards, threads: int):
+    """One Acero aggregate (use_threads=False: one task body) per shard, all
+    shards at once on `threads` host threads (Acero releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
     from oracle import arrow_ref
 
+    with ThreadPoolExecutor(threads) as ex:
+        return list(ex.map(lambda s: arrow_ref.groupby(s, ["k"], AGGS, use_threads=False), shards))
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation of the path on the
+    full 200M-row workload every step, with every host core."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import pyarrow as pa
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    n = args.rows
+    cores = host_cores()
+    shards = reference_shards(n, cores, cores)
     for _ in range(args.warmup):
-        arrow_ref.groupby(sample, ["k"], AGGS, use_threads=True)
+        run_shards(shards, cores)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        arrow_ref.groupby(sample, ["k"], AGGS, use_threads=True)
+        res = run_shards(shards, cores)
     el = time.perf_counter() - t0
+    groups = sum(r.num_rows for r in res)
     rate = n * args.steps / el
-    cores = os.cpu_count()
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": "rows/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+int64",
-        "data": "synthetic (seeded, config-1 distributions)",
-        "config": {"workload": "groupby config 1 (Zipf 1.1 int64 keys over 10M, f64 N(0,1) 10% nulls, i32)",
-                   "rows_per_step": n, "full_rows": N_ROWS},
+        "data": "synthetic (seeded on the host with numpy: the workload's distributions)",
+        "config": groupby_config(n, world),
+        "groups": groups,
         "cpu_baseline": {"value": rate, "unit": "rows/s", "cores": cores, "kind": "port",
-                         "sample": f"{n} rows/step of the config-1 distribution; Arrow {pa.__version__} Acero "
-                                   "aggregate (hash_sum/mean/count_all/count/min/max/count_distinct), "
-                                   "use_threads=True: the Arrow calls of the reference's cpu_variant"},
+                         "sample": f"every step the whole {n}-row workload: {cores} hash shards of the key, one "
+                                   f"Arrow {pa.__version__} Acero aggregate (hash_sum/mean/count_all/count/min/max/"
+                                   "count_distinct, use_threads=False: one cpu_variant task body) per shard, "
+                                   f"{cores} shards at once on {cores} host threads (legate --cpus {cores}); "
+                                   "the shuffle into shards is not timed"},
         "e2e": {"value": rate, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+def groupby_config(n: int, world: int) -> dict:
+    return {"workload": "hash groupby, 200M rows; int64 Zipf(1.1) keys over 10M values, f64 N(0,1) 10% nulls, "
+                        "i32 U[0,1e6); SUM/MEAN(f64), COUNT(*), COUNT(f64), MIN/MAX(i32), NUNIQUE(i32)",
+            "rows": n, "l2": "inputs 4.2 GB >> 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"}
+
+
+def cpu_task_rate(keys, v, valid, i, nshards: int, min_seconds: float = 10.0):
+    """One legate CPU task's rate: shard 0 of `nshards` hash shards of the
+    device input (the same rows the GPU step aggregates) through one Acero
+    aggregate with use_threads=False, repeated for >= min_seconds."""
+    import numpy as np
+
+    from oracle import arrow_ref
+
+    host = host_table(keys, v, valid, i)
+    sel = np.nonzero(shard_of(host.column("k").to_numpy(), nshards) == 0)[0]
+    sample = host.take(sel)
+    del host
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        arrow_ref.groupby(sample, ["k"], AGGS, use_threads=False)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or reps >= 20:
+            break
+    return sample.num_rows * reps / el, sample.num_rows, el, reps
 
 
 # ---------------------------------------------------------------------------
@@ -308,10 +335,10 @@ def run_served(device, n_requests: int):
 
 
 # ---------------------------------------------------------------------------
-# other workloads of the path (not the default line): `--workload join` runs
-# the 200M x 20M int32-key hash joins, `--workload strings` the 100M-row
-# string-key groupby / stable sort / hash partition; one JSON line per op
-# with device ms, rows/s and per-kernel ms (CUDA events on the stream)
+# the joins and the string workload (sub-records of the default line, or one
+# line per op with --workload join / strings): device ms of the op (CUDA
+# events on the stream), rows/s, the op's algorithmic bytes against the
+# measured HBM peak, and per-kernel device ms
 # ---------------------------------------------------------------------------
 def _profiled(N, fn, steps):
     import torch
@@ -320,130 +347,178 @@ def _profiled(N, fn, steps):
         r = fn()
         del r
     torch.cuda.synchronize()
-    N.profile_enable(True)
-    N.profile_report(reset=True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(steps):
         r = fn()
-        rows = r[0].num_rows() if isinstance(r, tuple) else r.num_rows()
         del r
     e1.record()
     torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    N.profile_enable(True)
+    N.profile_report(reset=True)
+    r = fn()
+    torch.cuda.synchronize()
     prof = N.profile_report(reset=True)
     N.profile_enable(False)
-    return e0.elapsed_time(e1) / steps, rows, {k: [c // steps, round(t / steps, 3)] for k, (c, t) in
-                                               sorted(prof.items(), key=lambda kv: -kv[1][1])}
+    return ms, r, {k: [c, round(t, 4)] for k, (c, t) in sorted(prof.items(), key=lambda kv: -kv[1][1])}
 
 
-def run_join_workload(args):
-    """Build 20M rows (int32 keys = a permutation of [0, 20M), two int64
-    payloads); probe rows (--rows, default 200M): with p=0.8 a build key of
-    Zipf(0.9) rank, else U[20M, 40M); 5% null keys; one float64 payload."""
-    import pyarrow as pa
+def _record(name, ms, rows_in, out_rows, algo, kern, peak, kind):
+    total = sum(t for _, t in kern.values()) or 1.0
+    dom = next(iter(kern), None)
+    return {"op": name, "ms": round(ms, 4), "rows_per_s": rows_in / (ms / 1e3), "out_rows": out_rows,
+            "algorithmic_bytes": int(algo), "GBps": algo / (ms / 1e3) / 1e9,
+            "frac": algo / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
+            "dominant_kernel": dom, "dominant_ms": kern[dom][1] if dom else None,
+            "dominant_share": round(kern[dom][1] / total, 4) if dom else None, "kernels_ms": kern}
+
+
+_C1 = 0xFF51AFD7ED558CCD - (1 << 64)
+_C2 = 0xC4CEB9FE1A85EC53 - (1 << 64)
+
+
+def _mix(x):
+    m31 = (1 << 31) - 1
+    x = x ^ ((x >> 33) & m31)
+    x = x * _C1
+    x = x ^ ((x >> 33) & m31)
+    x = x * _C2
+    return x ^ ((x >> 33) & m31)
+
+
+def _row_checksum(cols):
+    """Order-independent checksum of rows given as (int64 bits, valid) columns."""
     import torch
 
-    from legate_dataframe import LogicalColumn, LogicalTable
+    h = None
+    for j, (x, ok) in enumerate(cols):
+        a = torch.where(ok, _mix(x + (j + 1) * 0x9E3779B9), torch.full_like(x, 0x5BD1E995 + j))
+        h = a if h is None else _mix(h + a)
+    m = 0xFFFFFFFF
+    return int((h & m).sum()), int(((h >> 32) & m).sum()), [int(ok.sum()) for _, ok in cols]
+
+
+def _col_bits(c):
+    import torch
+
     from legate_dataframe import _native as N
+
+    n = c.size
+    w = N.TYPE_WIDTH[c.ldf_type]
+    x = c.data[: n * w].view({1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}[w]).to(torch.int64)
+    ok = c.valid[:n].bool() if c.valid is not None else torch.ones(n, dtype=torch.bool, device=x.device)
+    return x, ok
+
+
+def _join_expected(J, how):
+    """The join's rows by definition (unique build keys: a probe row with a
+    valid key matches the build row holding that key), as (bits, valid)."""
+    import torch
+
+    dev = J.bkey.device
+    nb = J.bkey.numel()
+    inv = torch.empty(nb, dtype=torch.int64, device=dev)
+    inv[J.bkey.long()] = torch.arange(nb, device=dev)
+    inr = J.pvalid & (J.pkey >= 0) & (J.pkey < nb)
+    brow = torch.where(inr, inv[J.pkey.long().clamp(0, nb - 1)], torch.full_like(inv[:1], -1))
+    hit = brow >= 0
+    one = torch.ones_like(hit)
+    safe = brow.clamp(min=0)
+    cols = [(J.pkey.to(torch.int64), J.pvalid), (J.ppay.view(torch.int64), one),
+            (J.bkey[safe].to(torch.int64), hit), (J.bp1[safe], hit), (J.bp2[safe], hit)]
+    if how == "inner":
+        return [(x[hit], one[hit]) for x, _ in cols]
+    if how == "left":
+        return cols
+    used = torch.zeros(nb, dtype=torch.bool, device=dev)
+    used[brow[hit]] = True
+    un = torch.nonzero(~used).squeeze(1)
+    z = torch.zeros(un.numel(), dtype=torch.int64, device=dev)
+    f = torch.zeros(un.numel(), dtype=torch.bool, device=dev)
+    t = ~f
+    tail = [(z, f), (z, f), (J.bkey[un].to(torch.int64), t), (J.bp1[un], t), (J.bp2[un], t)]
+    return [(torch.cat([a, b]), torch.cat([m, mb])) for (a, m), (b, mb) in zip(cols, tail)]
+
+
+def join_records(steps: int, n_probe: int, n_build: int = 20_000_000, check: bool = True):
+    """Inner / left / full join of the 200M x 20M int32-key workload."""
+    import torch
+
+    from legate_dataframe import _native as N
+    from legate_dataframe import workloads as W
     from legate_dataframe.lib.join import JoinType, join
 
-    dev = torch.device("cuda", 0)
-    nb, npr = 20_000_000, args.rows
-    g = torch.Generator(device=dev)
-    g.manual_seed(6)
-    bkey = torch.randperm(nb, device=dev, generator=g).to(torch.int32)
-    bp1 = torch.randint(-(2**40), 2**40, (nb,), device=dev, generator=g)
-    bp2 = torch.randint(-(2**40), 2**40, (nb,), device=dev, generator=g)
-    g.manual_seed(7)
-    cdf = torch.cumsum(torch.arange(1, nb + 1, device=dev, dtype=torch.float64).pow(-0.9), 0)
-    cdf /= cdf[-1].clone()
-    u = torch.rand(npr, device=dev, generator=g, dtype=torch.float64)
-    hit = torch.rand(npr, device=dev, generator=g) < 0.8
-    idx = torch.searchsorted(cdf, u).clamp_(max=nb - 1)
-    miss = torch.randint(nb, 2 * nb, (npr,), device=dev, generator=g, dtype=torch.int32)
-    pkey = torch.where(hit, bkey[idx], miss)
-    pvalid = torch.rand(npr, device=dev, generator=g) >= 0.05
-    ppay = torch.rand(npr, device=dev, generator=g, dtype=torch.float64)
-    del cdf, u, hit, idx, miss
-    lt = LogicalTable([LogicalColumn.from_torch(pkey, pa.int32(), valid=pvalid),
-                       LogicalColumn.from_torch(ppay, pa.float64())], ["lk", "lv"])
-    rt = LogicalTable([LogicalColumn.from_torch(bkey, pa.int32()), LogicalColumn.from_torch(bp1, pa.int64()),
-                       LogicalColumn.from_torch(bp2, pa.int64())], ["rk", "r1", "r2"])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    J = W.int32_join(n_probe, n_build, dev)
+    lt, rt = J.tables()
     peak, kind = measured_peak_gbs()
+    out = []
     for jt in (JoinType.INNER, JoinType.LEFT, JoinType.FULL):
-        ms, rows, kern = _profiled(N, lambda: join(lt, rt, lhs_keys=["lk"], rhs_keys=["rk"], join_type=jt),
-                                   args.steps)
-        in_b = nb * 20 + npr * 13
-        out_b = rows * (4 + 1 + 8 + 4 + 8 + 8 + (3 if jt != JoinType.INNER else 0))
-        print(json.dumps({"workload": f"join {jt.name.lower()}: {npr} probe x {nb} build rows", "ms": round(ms, 3),
-                          "rows_per_s": (npr + nb) / (ms / 1e3), "out_rows": rows,
-                          "op_GBps_algorithmic": (in_b + out_b) / (ms / 1e3) / 1e9,
-                          "op_frac_of_peak": (in_b + out_b) / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
-                          "kernels_ms": kern}), flush=True)
-    return 0
+        ms, res, kern = _profiled(N, lambda: join(lt, rt, lhs_keys=["lk"], rhs_keys=["rk"], join_type=jt), steps)
+        algo = n_build * 20 + n_probe * 13 + output_bytes(res)
+        rec = _record(f"join {jt.name.lower()}: {n_probe} probe x {n_build} build rows (int32 keys)", ms,
+                      n_probe + n_build, res.num_rows(), algo, kern, peak, kind)
+        if check:
+            got = _row_checksum([_col_bits(c) for c in res.get_columns()])
+            rec["parity"] = "ok" if got == _row_checksum(_join_expected(J, jt.name.lower())) else "MISMATCH"
+        del res
+        out.append(rec)
+    del J, lt, rt
+    torch.cuda.empty_cache()
+    return out
 
 
-def run_strings_workload(args):
-    """--rows (default 100M) rows: string key drawn Zipf(1.0) from a 2M-entry
-    dictionary of [a-z0-9] strings of length U{8..24}; int64 timestamps over
-    one year; float32 LogNormal(0,1) values.  groupby SUM/COUNT(*) on the key,
-    stable sort (key asc, ts desc), hash_partition(key, 256)."""
-    import numpy as np
-    import pyarrow as pa
+def string_records(steps: int, n: int, ops: str = ""):
+    """groupby SUM/COUNT(*) on the string key, stable sort (key asc, ts
+    desc), hash_partition(key, 256) of the 100M-row string workload."""
     import torch
 
-    from legate_dataframe import LogicalColumn, LogicalTable
     from legate_dataframe import _native as N
+    from legate_dataframe import workloads as W
     from legate_dataframe.lib.groupby_aggregation import groupby_aggregation
     from legate_dataframe.lib.hash_partition import hash_partition
     from legate_dataframe.lib.sort import sort
 
-    dev = torch.device("cuda", 0)
-    n, nd = args.rows, 2_000_000
-    rng = np.random.default_rng(9)
-    lens = rng.integers(8, 25, nd)
-    alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz0123456789", dtype=np.uint8)
-    d_chars = torch.from_numpy(alphabet[rng.integers(0, 36, int(lens.sum()))].copy()).to(dev)
-    doff = np.zeros(nd + 1, np.int64)
-    np.cumsum(lens, out=doff[1:])
-    d_off = torch.from_numpy(doff).to(dev)
-    g = torch.Generator(device=dev)
-    g.manual_seed(9)
-    cdf = torch.cumsum(1.0 / torch.arange(1, nd + 1, device=dev, dtype=torch.float64), 0)
-    cdf /= cdf[-1].clone()
-    pick = torch.searchsorted(cdf, torch.rand(n, device=dev, generator=g, dtype=torch.float64)).clamp_(max=nd - 1)
-    row_len = (d_off[1:] - d_off[:-1])[pick]
-    row_off = torch.cumsum(row_len, 0) - row_len
-    rowid = torch.repeat_interleave(torch.arange(n, device=dev), row_len)
-    pos = torch.arange(int(row_len.sum()), device=dev)
-    chars = d_chars[d_off[pick][rowid] + (pos - row_off[rowid])]
-    del rowid, pos, cdf
-    ranges = torch.stack([row_off, row_off + row_len - 1], 1).contiguous()
-    t0 = 1_600_000_000_000_000
-    ts = torch.randint(t0, t0 + 365 * 86400 * 10**6, (n,), device=dev, generator=g)
-    val = torch.exp(torch.randn(n, device=dev, generator=g)).to(torch.float32)
-    key = LogicalColumn(pa.string(), N.LDF_STRING, n, ranges.view(torch.uint8).reshape(-1), None, chars=chars,
-                        chars_base=0, num_chars=chars.numel())
-    t = LogicalTable([key, LogicalColumn.from_torch(ts, pa.timestamp("us")),
-                      LogicalColumn.from_torch(val, pa.float32())], ["k", "ts", "v"])
-    row_bytes = 16 + chars.numel() / n + 8 + 4
-    ops = {
-        "groupby SUM/COUNT(*) on the string key": (lambda: groupby_aggregation(
-            t, ["k"], [("v", "sum", "s"), (None, "count_all", "c")]), n * (16 + chars.numel() / n + 4)),
-        "stable sort (key asc, ts desc)": (lambda: sort(t, ["k", "ts"], sort_ascending=[True, False], stable=True),
-                                           2 * n * row_bytes),
+    dev = torch.device("cuda", torch.cuda.current_device())
+    S = W.string_rows(n, dev)
+    t = S.table()
+    nchars = S.chars.numel()
+    row_bytes = 16 + nchars / n + 8 + 4
+    todo = {
+        "groupby SUM/COUNT(*) on the string key": (
+            lambda: groupby_aggregation(t, ["k"], [("v", "sum", "s"), (None, "count_all", "c")]),
+            n * (16 + nchars / n + 4)),
+        "stable sort (key asc, ts desc)": (
+            lambda: sort(t, ["k", "ts"], sort_ascending=[True, False], stable=True), 2 * n * row_bytes),
         "hash_partition(key, 256)": (lambda: hash_partition(t, ["k"], 256), 2 * n * row_bytes),
     }
-    peak, kind = measured_peak_gbs()
     wanted = {"groupby": "groupby", "sort": "stable sort", "partition": "hash_partition"}
-    if args.ops:
-        ops = {k: v for k, v in ops.items() if any(k.startswith(wanted[o]) for o in args.ops.split(","))}
-    for name, (fn, algo) in ops.items():
-        ms, rows, kern = _profiled(N, fn, args.steps)
-        print(json.dumps({"workload": f"{name}: {n} rows", "ms": round(ms, 3), "rows_per_s": n / (ms / 1e3),
-                          "out_rows": rows, "op_GBps_algorithmic": algo / (ms / 1e3) / 1e9,
-                          "op_frac_of_peak": algo / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
-                          "kernels_ms": kern}), flush=True)
+    if ops:
+        todo = {k: v for k, v in todo.items() if any(k.startswith(wanted[o]) for o in ops.split(","))}
+    peak, kind = measured_peak_gbs()
+    out = []
+    for name, (fn, algo) in todo.items():
+        ms, res, kern = _profiled(N, fn, steps)
+        tbl = res[0] if isinstance(res, tuple) else res
+        if name.startswith("groupby"):
+            algo += output_bytes(tbl) + sum(int(c.num_chars) for c in tbl.get_columns() if c.chars is not None)
+        out.append(_record(f"{name}: {n} rows", ms, n, tbl.num_rows(), algo, kern, peak, kind))
+        del res, tbl
+    del S, t
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_join_workload(args):
+    for rec in join_records(args.steps, args.rows, check=False):
+        print(json.dumps(rec), flush=True)
+    return 0
+
+
+def run_strings_workload(args):
+    for rec in string_records(args.steps, args.rows, args.ops):
+        print(json.dumps(rec), flush=True)
     return 0
 
 
@@ -466,12 +541,9 @@ def run_sort_workload(args):
     t = LogicalTable([LogicalColumn.from_torch(k, pa.int64()), LogicalColumn.from_torch(v, pa.int32())], ["k", "v"])
     algo = 2 * n * 12  # key + payload in, sorted table out
     peak, kind = measured_peak_gbs()
-    ms, rows, kern = _profiled(N, lambda: sort(t, ["k"], stable=True), args.steps)
-    print(json.dumps({"workload": f"stable sort (int64 key, int32 payload): {n} rows", "ms": round(ms, 3),
-                      "rows_per_s": n / (ms / 1e3), "out_rows": rows,
-                      "op_GBps_algorithmic": algo / (ms / 1e3) / 1e9,
-                      "op_frac_of_peak": algo / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
-                      "kernels_ms": kern}), flush=True)
+    ms, res, kern = _profiled(N, lambda: sort(t, ["k"], stable=True), args.steps)
+    print(json.dumps(_record(f"stable sort (int64 key, int32 payload): {n} rows", ms, n, res.num_rows(), algo, kern,
+                             peak, kind)), flush=True)
     return 0
 
 
@@ -553,11 +625,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-sample", type=int, default=4_000_000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-requests", type=int, default=8192)
-    ap.add_argument("--ref-rows", type=int, default=8_000_000, help="rows per step of the reference arm")
+    ap.add_argument("--no-joins", action="store_true")
+    ap.add_argument("--no-strings", action="store_true")
+    ap.add_argument("--sub-steps", type=int, default=5, help="timed steps of each join / string op record")
     ap.add_argument("--ops", default="", help="--workload strings: comma list of groupby,sort,partition (default all)")
     ap.add_argument("--workload", default="groupby", choices=["groupby", "join", "strings", "sort", "ingest"],
                     help="groupby = the benchmark line; join / strings / sort / ingest print per-op lines")
@@ -587,12 +660,13 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
 
     from legate_dataframe import _native as N
+    from legate_dataframe import workloads as W
     from legate_dataframe.lib.groupby_aggregation import groupby_aggregation
 
     N.lib()
     n = args.rows
-    keys, v, valid, i = make_input_device(n, device)
-    table = device_table(keys, v, valid, i)
+    keys, v, valid, i = W.zipf_groupby(n, device)
+    table = W.groupby_table(keys, v, valid, i)
 
     def step():
         return groupby_aggregation(table, ["k"], AGGS)
@@ -631,18 +705,18 @@ def main():
     N.profile_report(reset=True)
     for _ in range(2):
         out = step()
-        del out
     torch.cuda.synchronize()
     prof = N.profile_report(reset=True)
     N.profile_enable(False)
+
+    # ---- the step's result, checked outside the timed region ----------------
+    parity = {"groupby": groupby_parity(keys, v, valid, i, out)}
+    del out
+    torch.cuda.empty_cache()
+
     # algorithmic bytes each kernel streams per launch (the input columns it
-    # reads once): assign reads the keys, the column kernels the float64 value
-    # + its null mask or the int32 value, nunique the int32 value
-    per_launch_bytes = {
-        "assign": 8 * n,
-        "column": (9 * n + 4 * n) / 2,
-        "nunique": 4 * n,
-    }
+    # reads once)
+    per_launch_bytes = kernel_algorithmic_bytes(n)
     total_prof = sum(t for _, t in prof.values())
     dom = max((k for k in prof if k in per_launch_bytes), key=lambda k: prof[k][1], default=None)
     peak, peak_kind = measured_peak_gbs()
@@ -680,7 +754,7 @@ def main():
         def e2e_step():
             # the table's columns are pinned host memory: the op copies each
             # to the device itself, overlapping the copies with its passes
-            res = groupby_aggregation(device_table(hk, hv, hm, hi), ["k"], AGGS)
+            res = groupby_aggregation(W.groupby_table(hk, hv, hm, hi), ["k"], AGGS)
             res.to_arrow()
             return output_bytes(res)
 
@@ -698,23 +772,33 @@ def main():
                "h2d_bytes_per_step": n * IN_BYTES_PER_ROW, "d2h_bytes_per_step": d2h}
         del hk, hv, hm, hi
 
-    # ---- CPU baseline (rank 0, N=1 only) ------------------------------------
+    # ---- CPU baseline (rank 0, N=1 only): one legate CPU task's shard -------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         import pyarrow as pa
 
-        sample = host_sample(keys, v, valid, i, min(args.cpu_sample, n))
-        rate, el, reps = cpu_groupby_rate(sample, use_threads=False)
+        shards = host_cores()
+        rate, rows, el, reps = cpu_task_rate(keys, v, valid, i, shards)
         cpu = {"value": rate, "unit": "rows/s", "cores": 1, "kind": "port",
-               "sample": f"first {sample.num_rows} rows of the same input x{reps} ({el:.1f} s); Arrow "
-                         f"{pa.__version__} Acero aggregate hash_sum/mean/count_all/count/min/max/count_distinct, "
-                         "use_threads=False: the Arrow calls of the reference's cpu_variant (one legate CPU task)"}
+               "sample": f"hash shard 0 of {shards} of the same {n}-row input ({rows} rows, the share of one "
+                         f"legate CPU task at --cpus {shards}) x{reps} ({el:.1f} s); Arrow {pa.__version__} Acero "
+                         "aggregate hash_sum/mean/count_all/count/min/max/count_distinct, use_threads=False: "
+                         "the Arrow calls of the reference's cpu_variant"}
+    del keys, v, valid, i, table
+    torch.cuda.empty_cache()
+
+    # ---- joins and the string workload (rank 0, N=1 only) -------------------
+    joins = strings = None
+    if rank == 0 and world == 1 and not args.no_joins:
+        joins = join_records(args.sub_steps, 200_000_000)
+    if rank == 0 and world == 1 and not args.no_strings:
+        strings = string_records(args.sub_steps, 100_000_000)
+    if joins is not None:
+        parity["joins"] = "ok" if all(r.get("parity") == "ok" for r in joins) else "MISMATCH"
 
     # ---- served mix (rank 0, N=1 only) --------------------------------------
     served = None
     if rank == 0 and world == 1 and not args.no_served:
-        del keys, v, valid, i, table
-        torch.cuda.empty_cache()
         served = run_served(device, args.served_requests)
 
     if world > 1:
@@ -734,9 +818,9 @@ def main():
         "vs_baseline": None,
         "dtype": "f64+int64 (fixed-point exact f64 sums)",
         "data": "synthetic (seeded on device: Zipf(1.1) keys over 10M int64, f64 N(0,1) 10% nulls, i32 U[0,1e6))",
-        "config": {"workload": "groupby config 1: 200M rows; SUM/MEAN(f64), COUNT(*), COUNT(f64), MIN/MAX(i32), "
-                               "NUNIQUE(i32)", "rows": n, "groups": groups,
-                   "l2": "inputs 4.2 GB >> 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
+        "config": groupby_config(n, world),
+        "groups": groups,
+        "parity": parity,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes": algo_kernel, "kernel_ms": dom_ms,
@@ -747,10 +831,80 @@ def main():
         "clocks": clk.summary(),
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "joins": joins,
+        "strings": strings,
         "served": served,
     }
     print(json.dumps(line))
     return 0
+
+
+def kernel_algorithmic_bytes(n: int) -> dict:
+    """Algorithmic bytes per launch of the groupby's row passes: the input
+    columns each reads once (assign the keys; the column passes the float64
+    value + its null mask or the int32 value; nunique the int32 value)."""
+    return {"assign": 8 * n, "column": (9 * n + 4 * n) / 2, "nunique": 4 * n}
+
+
+def groupby_parity(keys, v, valid, i, out) -> str:
+    """The step's result against the aggregates recomputed with torch's sorts
+    (rows sorted by key, then by the int32 value inside a key): COUNT(*),
+    COUNT, MIN, MAX and NUNIQUE exact; SUM and MEAN within the rounding bound
+    of an fp64 sum in any order ((count + 2) x 2^-52 x the sum of |x|)."""
+    import torch
+
+    n = keys.numel()
+    p = torch.sort(i, stable=True).indices
+    perm = p[torch.sort(keys[p], stable=True).indices]
+    del p
+    sk, si = keys[perm], i[perm]
+    sm = valid[perm].bool()
+    sv = torch.where(sm, v[perm], torch.zeros((), dtype=v.dtype, device=v.device))
+    del perm
+    uniq, counts = torch.unique_consecutive(sk, return_counts=True)
+    g = uniq.numel()
+    end = torch.cumsum(counts, 0)
+    start = end - counts
+    seg = torch.repeat_interleave(torch.arange(g, device=keys.device), counts)
+    new = torch.ones(n, dtype=torch.int64, device=keys.device)
+    new[1:] = ((si[1:] != si[:-1]) | (sk[1:] != sk[:-1])).to(torch.int64)
+    del sk
+    zeros = torch.zeros(g, dtype=torch.int64, device=keys.device)
+    nd = zeros.clone().index_add_(0, seg, new)
+    cv = zeros.clone().index_add_(0, seg, sm.to(torch.int64))
+    fz = torch.zeros(g, dtype=torch.float64, device=keys.device)
+    s = fz.clone().index_add_(0, seg, sv)
+    a = fz.clone().index_add_(0, seg, sv.abs())
+    mn, mx = si[start], si[end - 1]
+    del si, sm, sv, seg, new
+
+    cols = dict(zip(out.get_column_names(), out.get_columns()))
+
+    def col(name, dt):
+        c = cols[name]
+        return c.data[: c.size * torch.empty((), dtype=dt).element_size()].view(dt), \
+            (c.valid[: c.size].bool() if c.valid is not None else None)
+
+    k, _ = col("k", torch.int64)
+    if k.numel() != g:
+        return f"MISMATCH: {k.numel()} groups, expected {g}"
+    o = torch.sort(k).indices
+    bad = []
+    if not torch.equal(k[o], uniq):
+        bad.append("k")
+    for name, dt, want in (("count", torch.int64, counts), ("count_v", torch.int64, cv), ("min_i", torch.int32, mn),
+                           ("max_i", torch.int32, mx), ("nunique_i", torch.int64, nd)):
+        x, _ = col(name, dt)
+        if not torch.equal(x[o].to(want.dtype), want):
+            bad.append(name)
+    has = cv > 0
+    bound = (cv.to(torch.float64) + 2) * 2.0**-52 * a + 1e-300
+    for name, want, lim in (("sum_v", s, bound), ("mean_v", s / cv.clamp(min=1), bound / cv.clamp(min=1))):
+        x, ok = col(name, torch.float64)
+        x, ok = x[o], ok[o] if ok is not None else torch.ones_like(has)
+        if not torch.equal(ok, has) or not bool(((x - want).abs() <= lim)[has].all()):
+            bad.append(name)
+    return "ok" if not bad else "MISMATCH: " + ",".join(bad)
 
 
 if __name__ == "__main__":

@@ -196,6 +196,17 @@ int ldf_b200_arrow_bits_to_bytes(const uint8_t* bits, int64_t bit_offset, int64_
 int ldf_b200_arrow_offsets_to_ranges(const void* offsets, int32_t offset_bytes, int64_t n,
                                      ldf_range* ranges, void* stream);
 
+/* ---- test hook: a bounded wait that runs out ------------------------------ */
+/* No counterpart in the reference (its waits are inside libcudf).  Runs the
+ * library's look-back scan kernel as one block that takes the second tile of
+ * a two-tile input, so its look-back waits on a predecessor status word that
+ * nothing writes.  The wait ends after `spin_limit` polls (1 .. the
+ * library's own limit of 2^22) and the call returns LDF_ERR_TIMEOUT, the
+ * status every op returns when one of its bounded device-side waits expires;
+ * the context stays usable.  Scratch comes from `alloc` (NULL: stream-ordered
+ * cudaMallocAsync). */
+int ldf_b200_test_stalled_lookback(uint32_t spin_limit, const ldf_allocator* alloc, void* stream);
+
 /* ---- hash partition without device allocation ----------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory themselves -- a task body running concurrently with other tasks on the
@@ -210,7 +221,10 @@ int ldf_b200_arrow_offsets_to_ranges(const void* offsets, int32_t offset_bytes, 
  * device image, held by every GPU that loads the library until the process
  * exits; no cudaMalloc/cudaFree or allocating library routine is called.  The
  * first call on a device looks up the array's device address, so make that
- * first call before any stream capture.  Every call shares the array: calls
+ * first call before any stream capture; the address is kept for the life of
+ * the process, so do not call this again on a device after a cudaDeviceReset
+ * of it.  Each call synchronizes `stream` twice: the bucket counts and the
+ * wait status are read back to the host.  Every call shares the array: calls
  * whose work overlaps on the GPU race and must be serialized. */
 #define LDF_B200_NOALLOC_MAX_ROWS (1 << 20)
 int ldf_b200_hash_partition_noalloc(const ldf_column* table, int32_t ncols,

@@ -46,7 +46,9 @@ constexpr size_t kScratchBytes = kOffErr + 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 // Device address of g_noalloc_scratch for each device, looked up on the first
-// call made with that device current.
+// call made with that device current and kept for the life of the process
+// (so the entry point must not be called again on a device after a
+// cudaDeviceReset of it).
 std::mutex g_mu;
 void* g_addr[256] = {};
 
@@ -69,10 +71,17 @@ void* scratch_address()
   return g_addr[dev];
 }
 
-__global__ void gather_rows_kernel(ldf::DCol src, const int32_t* rows, int64_t n, void* dst, uint8_t* dst_valid)
+// Output row i takes input row rows[i].  When the radix pass gave up on a
+// bounded wait (err set), some rows[] entries were never written and still
+// hold row ids of an earlier call: the kernel then copies nothing, and any
+// entry outside [0, n) is skipped, so no read leaves the input columns.
+__global__ void gather_rows_kernel(ldf::DCol src, const int32_t* rows, int64_t n, void* dst, uint8_t* dst_valid,
+                                   const int* err)
 {
+  if (*reinterpret_cast<const volatile int*>(err) != 0) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = rows[i];
+    if (r < 0 || r >= n) continue;
     ldf::copy_fixed(dst, i, src.data, r, src.width);
     if (dst_valid) dst_valid[i] = ldf::dvalid(src, r) ? 1 : 0;
   }
@@ -143,7 +152,7 @@ extern "C" int ldf_b200_hash_partition_noalloc(const ldf_column* table, int32_t 
         ldf::DCol src = ldf::make_dcol(table[j]);
         uint8_t* ov   = table[j].valid ? out[j].valid : nullptr;
         ldf::launch("gather_rows", gather_rows_kernel, 296u, 256u, 0, s, src, static_cast<const int32_t*>(perm), n,
-                    out[j].data, ov);
+                    out[j].data, ov, static_cast<const int*>(err));
       }
       int e = 0;
       LDF_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, s));

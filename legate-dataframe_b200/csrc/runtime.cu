@@ -8,6 +8,7 @@
 #include "scan.cuh"
 
 namespace ldf {
+void set_last_error(const std::string& msg);
 
 // ---------------------------------------------------------------------------
 // Launch accounting.  When profiling is on, each launch is bracketed by two
@@ -201,8 +202,10 @@ constexpr int kScanTile    = kScanThreads * kScanItems;
 
 // Exclusive prefix of `tile` over the tile aggregates before it; every lane
 // of one warp calls it.  Publishes the tile's aggregate first and its
-// inclusive prefix at the end.
-__device__ __forceinline__ uint64_t warp_lookback(uint64_t* status, int64_t tile, uint64_t aggregate, int* err)
+// inclusive prefix at the end.  A predecessor that has not published after
+// `spin_limit` polls sets LDF_ERR_TIMEOUT in *err and ends the wait.
+__device__ __forceinline__ uint64_t warp_lookback(uint64_t* status, int64_t tile, uint64_t aggregate, int* err,
+                                                  uint32_t spin_limit)
 {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
@@ -222,7 +225,7 @@ __device__ __forceinline__ uint64_t warp_lookback(uint64_t* status, int64_t tile
     const int first_prefix   = prefix ? __ffs(prefix) - 1 : 32;
     const int first_waiting  = not_ready ? __ffs(not_ready) - 1 : 32;
     if (first_waiting < first_prefix) {  // a tile before the nearest prefix has not published yet
-      if (++spins > kSpinLimit) {
+      if (++spins > spin_limit) {
         if (lane == 0) atomicExch(err, LDF_ERR_TIMEOUT);
         break;
       }
@@ -240,7 +243,7 @@ __device__ __forceinline__ uint64_t warp_lookback(uint64_t* status, int64_t tile
 template <typename TIn>
 __global__ void __launch_bounds__(kScanThreads)
   scan_kernel(const TIn* in, int64_t* out, int64_t n, uint64_t* status,
-              unsigned long long* counter, int64_t* total, int* err)
+              unsigned long long* counter, int64_t* total, int* err, uint32_t spin_limit)
 {
   __shared__ int64_t s_warp[kScanWarps + 1];
   __shared__ int64_t s_tile;
@@ -270,7 +273,7 @@ __global__ void __launch_bounds__(kScanThreads)
     const int64_t inc = warp_inclusive_scan(w);
     if (lane < kScanWarps) s_warp[lane] = inc - w;
     const int64_t tile_total = __shfl_sync(0xffffffffu, inc, kScanWarps - 1);
-    const uint64_t excl = warp_lookback(status, tile, static_cast<uint64_t>(tile_total), err);
+    const uint64_t excl = warp_lookback(status, tile, static_cast<uint64_t>(tile_total), err, spin_limit);
     if (lane == 0) {
       s_prefix = excl;
       if (tile == static_cast<int64_t>(gridDim.x) - 1) *total = static_cast<int64_t>(excl) + tile_total;
@@ -299,11 +302,32 @@ void exclusive_scan_impl(const TIn* in, int64_t* out, int64_t n, int64_t* d_tota
   Buffer<uint64_t> status(alloc, tiles + 2);
   unsigned long long* counter = reinterpret_cast<unsigned long long*>(status.get() + tiles);
   LDF_CUDA(cudaMemsetAsync(status.get(), 0, (tiles + 2) * sizeof(uint64_t), s));
-  launch("scan", scan_kernel<TIn>, static_cast<unsigned>(tiles), kScanThreads, 0, s, 
-    in, out, n, status.get(), counter, d_total, ctx.err());
+  launch("scan", scan_kernel<TIn>, static_cast<unsigned>(tiles), kScanThreads, 0, s, in, out, n, status.get(),
+         counter, d_total, ctx.err(), kSpinLimit);
   LDF_CHECK_LAUNCH();
 }
 }  // namespace
+
+// The scan kernel of exclusive_scan_i64 launched as one block that takes
+// tile 1 of a two-tile input, so the look-back waits on tile 0, whose status
+// word nothing writes: the wait ends after `spin_limit` polls with
+// LDF_ERR_TIMEOUT in the error word, which finish() turns into the op's
+// error.  Exercises the timeout path of every look-back without a hang.
+void stalled_lookback(uint32_t spin_limit, const OpContext& ctx)
+{
+  cudaStream_t s = ctx.stream();
+  Buffer<int64_t> io(ctx.alloc(), 4 * kScanTile + 1);  // input, output, total
+  Buffer<uint64_t> status(ctx.alloc(), 4);
+  LDF_CUDA(cudaMemsetAsync(io.get(), 0, (4 * kScanTile + 1) * sizeof(int64_t), s));
+  LDF_CUDA(cudaMemsetAsync(status.get(), 0, 4 * sizeof(uint64_t), s));
+  static const unsigned long long kFirstTile = 1;  // the block takes tile 1
+  LDF_CUDA(cudaMemcpyAsync(status.get() + 2, &kFirstTile, sizeof(kFirstTile), cudaMemcpyHostToDevice, s));
+  launch("scan", scan_kernel<int64_t>, 1u, kScanThreads, 0, s, static_cast<const int64_t*>(io.get()),
+         io.get() + 2 * kScanTile, static_cast<int64_t>(2 * kScanTile), status.get(),
+         reinterpret_cast<unsigned long long*>(status.get() + 2), io.get() + 4 * kScanTile, ctx.err(), spin_limit);
+  LDF_CHECK_LAUNCH();
+  ctx.finish();
+}
 
 void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, int64_t* d_total,
                         const OpContext& ctx)
@@ -319,6 +343,23 @@ void exclusive_scan_u32(const uint32_t* in, int64_t* out, int64_t n, int64_t* d_
 }  // namespace ldf
 
 extern "C" {
+int ldf_b200_test_stalled_lookback(uint32_t spin_limit, const ldf_allocator* alloc, void* stream)
+{
+  ldf::set_last_error("");
+  try {
+    LDF_REQUIRE(spin_limit >= 1 && spin_limit <= ldf::kSpinLimit, "spin_limit must be in [1, kSpinLimit]");
+    ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
+    ldf::stalled_lookback(spin_limit, ctx);
+    return LDF_OK;
+  } catch (const ldf::LdfError& e) {
+    ldf::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    ldf::set_last_error(e.what());
+    return LDF_ERR_INTERNAL;
+  }
+}
+
 void ldf_b200_profile_enable(int on)
 {
   ldf::prof::collect();

@@ -147,6 +147,8 @@ def lib():
             L.ldf_b200_arrow_offsets_to_ranges.argtypes = [
                 ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
             ]
+            L.ldf_b200_test_stalled_lookback.argtypes = [ctypes.c_uint32, P(ldf_allocator), ctypes.c_void_p]
+            L.ldf_b200_test_stalled_lookback.restype = ctypes.c_int
             L.ldf_b200_arrow_bits_to_bytes.restype = ctypes.c_int
             L.ldf_b200_arrow_offsets_to_ranges.restype = ctypes.c_int
             L.ldf_b200_launch_count.restype = ctypes.c_ulonglong

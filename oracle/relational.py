@@ -365,6 +365,31 @@ def _hash_bytes(b: bytes) -> int:
     return mix(h)
 
 
+def string_hashes(chars: np.ndarray, offsets: np.ndarray) -> np.ndarray:
+    """`_hash_bytes` of every string [offsets[j], offsets[j+1]) of `chars`,
+    vectorized over the strings: word w of all strings long enough to have it
+    is folded in at once (the tail word zero-padded, as `_hash_bytes` does)."""
+    chars = np.asarray(chars, dtype=np.uint8)
+    off = np.asarray(offsets, dtype=np.int64)
+    n = off[1:] - off[:-1]
+    with np.errstate(over="ignore"):
+        h = np.uint64(0x27D4EB2F165667C5) ^ (n.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15))
+    padded = np.concatenate([chars, np.zeros(8, np.uint8)])
+    nwords = (n + 7) // 8
+    for w in range(int(nwords.max()) if len(n) else 0):
+        sel = np.nonzero(nwords > w)[0]
+        start = off[:-1][sel] + 8 * w
+        rem = np.minimum(n[sel] - 8 * w, 8)
+        word = np.zeros(len(sel), np.uint64)
+        for b in range(8):
+            byte = padded[start + b].astype(np.uint64)
+            byte = np.where(rem > b, byte, np.uint64(0))
+            word |= byte << np.uint64(8 * b)
+        with np.errstate(over="ignore"):
+            h[sel] = _mix64(h[sel] ^ word) + np.uint64(0x165667B19E3779F9)
+    return _mix64(h)
+
+
 def _raw_bits(arr: pa.Array) -> tuple[np.ndarray, int]:
     t = arr.type
     width = t.bit_width // 8 if not pa.types.is_boolean(t) else 1
@@ -386,8 +411,11 @@ def row_hashes(table: pa.Table, keys) -> np.ndarray:
         arr = table.column(k).combine_chunks()
         valid = np.asarray(arr.is_valid(), dtype=bool)
         if pa.types.is_string(arr.type) or pa.types.is_large_string(arr.type):
-            hv = np.array([_hash_bytes(s.encode("utf-8")) if s is not None else 0 for s in arr.to_pylist()],
-                          dtype=np.uint64)
+            large = pa.types.is_large_string(arr.type)
+            bufs = arr.buffers()
+            offs = np.frombuffer(bufs[1], dtype=np.int64 if large else np.int32)[arr.offset:arr.offset + n + 1]
+            chars = np.frombuffer(bufs[2], dtype=np.uint8) if bufs[2] is not None else np.zeros(0, np.uint8)
+            hv = string_hashes(chars, offs.astype(np.int64)) if n else np.zeros(0, np.uint64)
         else:
             raw, width = _raw_bits(arr)
             with np.errstate(over="ignore"):

@@ -39,4 +39,7 @@ def _built_library():
         except (RuntimeError, FileNotFoundError):
             if not ldf_build.LIB.exists():
                 raise
+    from oracle import native as oracle_native
+
+    oracle_native.build()
     yield

@@ -1,8 +1,11 @@
 """Batched execution (one graph replay for many joins/groupbys) and the
-continuous-batching server: every batched result equals the per-op result
-of the same request, alone and in a mix (bit-exact: integer columns, row sets
+continuous-batching server: every batched result equals the oracle's result
+for the request (the reference's CPU path: Acero hashjoin for joins; groupby
+COUNT exact and SUM within 1e-12 of a Neumaier sum) and the per-op result of
+the same request, alone and in a mix (bit-exact: integer columns, row sets
 after a canonical sort, and float sums, which both paths compute from an exact
-fixed-point sum), and overflowing requests fall back to the per-op path."""
+fixed-point sum); a 512-request slice of the served trace is checked request
+by request; overflowing requests fall back to the per-op path."""
 
 import numpy as np
 import pyarrow as pa
@@ -74,9 +77,35 @@ def run_batch(reqs, arena_bytes=1 << 30, tile_rows=4096, ctas=2, lf=0.5):
     return out, ovf
 
 
-def check(q, res):
-    exp = per_op_arrow(q)
-    assert_tables_equal(res, exp, check_types=False)
+def oracle_arrow(q):
+    """The request's result from the oracle: Acero hashjoin (the calls of
+    JoinTask::cpu_variant) for joins; for groupbys the valid count per key
+    and the sum of the valid values (Neumaier for float64, exact for int64)."""
+    from oracle import arrow_ref as A
+    from oracle import native
+
+    k1 = q.k1.cpu().numpy()
+    if q.kind == JOIN:
+        lhs = pa.table({"lk": k1, "lv": q.v1.cpu().numpy()})
+        rhs = pa.table({"rk": q.k2.cpu().numpy(), "rv": q.v2.cpu().numpy()})
+        return A.join(lhs, rhs, ["lk"], ["rk"], "inner", True, use_threads=True)
+    v = q.v1.cpu().numpy()
+    ok = q.valid.cpu().numpy() if q.valid is not None else np.ones(len(k1), bool)
+    order = np.argsort(k1, kind="stable")
+    keys, start = np.unique(k1[order], return_index=True)
+    off = np.append(start, len(k1)).astype(np.int64)
+    if v.dtype == np.float64:
+        sums, cnt = native.segment_sums(v[order], ok[order].astype(np.uint8), off)
+    else:
+        cnt = np.add.reduceat(ok[order].astype(np.int64), start) if len(k1) else np.zeros(0, np.int64)
+        sums = np.add.reduceat(np.where(ok, v, 0)[order], start) if len(k1) else np.zeros(0, np.int64)
+    return pa.table({"k": keys, "sum": pa.array(sums, mask=cnt == 0), "count": cnt})
+
+
+def check(q, res, per_op=True):
+    assert_tables_equal(res, oracle_arrow(q), check_types=False, rtol=1e-12)
+    if per_op:
+        assert_tables_equal(res, per_op_arrow(q), check_types=False)
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.int64])
@@ -146,6 +175,54 @@ def test_server_results_match_per_op():
         assert_tables_equal(q.result, per_op_arrow(q), check_types=False)
     base = run_one_op_per_launch(reqs[:8], realtime=False)
     assert base.requests == 8
+
+
+def _np_mix(x):
+    x = x.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        x ^= x >> np.uint64(33)
+        x *= np.uint64(0xFF51AFD7ED558CCD)
+        x ^= x >> np.uint64(33)
+        x *= np.uint64(0xC4CEB9FE1A85EC53)
+        x ^= x >> np.uint64(33)
+    return x
+
+
+def _row_checksum(t: pa.Table) -> int:
+    """Order-independent checksum of a table of int64 columns (row hashes of
+    all columns together, summed modulo 2^64)."""
+    h = np.zeros(t.num_rows, np.uint64)
+    for j, c in enumerate(t.columns):
+        x = c.combine_chunks().to_numpy().view(np.uint64) if t.num_rows else np.zeros(0, np.uint64)
+        with np.errstate(over="ignore"):
+            h = _np_mix(h + _np_mix(x + np.uint64(j + 1)))
+    with np.errstate(over="ignore"):
+        return int(h.sum(dtype=np.uint64))
+
+
+def test_trace_slice_matches_oracle():
+    """The first 512 requests of the served trace (LogNormal sizes, half
+    joins, half groupbys), batched by the server and checked one by one:
+    groupbys in full, joins by row count and an order-independent checksum of
+    their rows (together about 2e8 output rows)."""
+    reqs = make_trace(n_requests=512, seed=12)
+    srv = Server(arena_bytes=16 << 30, tile_rows=16384, ctas_per_sm=8, load_factor=0.35, keep_results=True)
+    served = 0
+    for part in range(0, len(reqs), 64):  # 64 requests at a time keeps the host copies small
+        chunk = reqs[part:part + 64]
+        served += srv.serve(chunk, realtime=False).requests
+        for q in chunk:
+            exp = oracle_arrow(q)
+            if q.kind == JOIN:
+                got = q.result.rename_columns(["lk", "lv", "rk", "rv"])
+                assert got.num_rows == exp.num_rows, q.rid
+                assert _row_checksum(got) == _row_checksum(exp), q.rid
+            else:
+                assert_tables_equal(q.result.rename_columns(["k", "sum", "count"]), exp, check_types=False,
+                                    rtol=1e-12)
+            q.result = None
+    srv.close()
+    assert served == 512
 
 
 def test_autotuner_persists_choice(tmp_path):

@@ -142,3 +142,35 @@ def test_oracle_special_float_keys_vs_arrow(dtype):
         exp = A.join(lhs, rhs, ["k"], ["k2"], how, True)
         res = R.join(lhs, rhs, ["k"], ["k2"], how, True)
         assert_tables_equal(res, exp, sort_by=[c for c in exp.column_names if c in ("a", "b")], check_types=False)
+
+
+def test_oracle_string_hashes_vectorized():
+    # the vectorized string hash (used at full size) equals the byte-wise
+    # definition on strings of every length class, tails included
+    rng = np.random.default_rng(11)
+    strs = [bytes(rng.integers(48, 123, int(n))) for n in rng.integers(0, 41, 2000)] + [b"", b"x" * 8, b"y" * 24]
+    off = np.zeros(len(strs) + 1, np.int64)
+    off[1:] = np.cumsum([len(s) for s in strs])
+    got = R.string_hashes(np.frombuffer(b"".join(strs), np.uint8), off)
+    assert [int(g) for g in got] == [R._hash_bytes(s) for s in strs]
+
+
+def test_oracle_segment_sums_c():
+    # the C Neumaier segment sums agree with math.fsum (exactly rounded)
+    import math
+
+    from oracle import native
+
+    rng = np.random.default_rng(12)
+    x = rng.normal(size=30000) * np.exp(rng.normal(size=30000) * 8)
+    x = np.concatenate([x, -x[:20000] * (1 + 1e-15)])
+    valid = (rng.random(len(x)) >= 0.1).astype(np.uint8)
+    off = np.concatenate([[0], np.sort(rng.choice(np.arange(1, len(x)), 40, replace=False)), [len(x)]])
+    sums, cnt = native.segment_sums(x, valid, off)
+    for s in range(len(off) - 1):
+        seg = x[off[s]:off[s + 1]][valid[off[s]:off[s + 1]] == 1]
+        exact = math.fsum(seg)
+        assert cnt[s] == len(seg)
+        assert abs(sums[s] - exact) <= 1e-12 * abs(exact) + 1e-300
+    s32, c32 = native.segment_sums(x.astype(np.float32), None, off)
+    assert abs(s32[0] - math.fsum(x[:off[1]].astype(np.float32).astype(np.float64))) <= 1e-12 * abs(s32[0])

@@ -53,7 +53,7 @@ def test_reference_arm_under_torchrun_world2():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--ref-rows", "20000"]
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--rows", "20000"]
     res = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=ROOT)
     assert res.returncode == 0, res.stderr[-2000:]
     lines = [json.loads(x) for x in res.stdout.splitlines() if x.startswith("{")]
