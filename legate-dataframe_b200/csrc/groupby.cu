@@ -1945,6 +1945,1157 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
   }
 }
 
+
+// ===========================================================================
+// Partitioned plan: one fixed-width key, at most two fixed-width value
+// columns (the second at most 4 bytes wide), NUNIQUE of at most one column
+// of <= 4-byte values.  Every row is read once by a routing pass:
+//  * the keys the sample saw most often ("hot", at most kPartHotMax, plus the
+//    null key) are aggregated in shared memory (flushed once per CTA) and
+//    their NUNIQUE values set bits of per-group value bitmaps;
+//  * every other row is written as one 24-byte record {key, value 0,
+//    value 1 | validity bits} into the hash bucket of its key (2^logP
+//    buckets, sized by a counting pre-pass over the keys).
+// A bucket pass then aggregates each bucket in shared memory (a CTA per
+// bucket: local key table, records, then a pair set for NUNIQUE) and writes
+// its groups' output rows; buckets too large for shared memory take the same
+// code on per-CTA global scratch.  No per-row group id is ever written.
+// Float sums are the exact fixed-point sums of the general plan; a float
+// SUM/MEAN value outside the fixed-point range (NaN, inf, |x| < 2^-44 or
+// >= 2^95) makes the call fall back to the general plan.
+// ===========================================================================
+constexpr int kPartThreads    = 512;   // routing pass
+constexpr int kCountThreads   = 1024;  // counting pre-pass
+constexpr int kPartHotMax     = 1024;  // hot keys (the null key takes one more record)
+constexpr int kPartHotSlots   = 2048;  // shared hot key table (power of two)
+constexpr uint32_t kPartNoId  = 0xffffffffu;
+constexpr uint32_t kPartBusy  = 0xfffffffeu;
+constexpr int kBucketThreads  = 1024;  // bucket pass
+constexpr int kBucketKeySlots = 2048;  // shared local key table (power of two)
+constexpr int kBucketRecBytes = 128 * 1024;  // shared records, then the pair set
+constexpr int kBucketGroupsMax = 1024;
+
+struct PVal {  // one value column of the partitioned plan
+  DCol col;
+  int nullable;
+  uint32_t states;  // ST_SUM | ST_MIN | ST_MAX | ST_NDIST
+  int fixed;        // float sum: six fixed-point chunks
+  int chunks;       // sum chunks (6 float, 2 integer)
+  int mm64;         // min/max as 64-bit ordered words
+  // shared (32-bit) record: byte offsets of the fields
+  int b_vc, b_sum, b_mn, b_mx;
+  // global hot record (64-bit words): word offsets of the fields
+  int w_vc, w_sum, w_mn, w_mx;
+};
+
+struct PartOut {
+  OCol key;
+  int nagg;
+  AggOut a[kMaxAggs];  // AggOut::col = value column (0 / 1), -1 for COUNT_ALL
+};
+
+struct PartArgs {
+  DCol key;
+  int64_t n;
+  int ncol;
+  PVal c[2];
+  int nd;  // value column with NUNIQUE, -1 for none
+  // hot keys
+  const unsigned long long* hot_keys;
+  int H;       // hot keys; record H is the null key's
+  int rb;      // bytes of a shared record
+  int rw;      // words of a global hot record
+  unsigned long long* hot_rec;  // [(H + 1) * rw]
+  uint32_t* bits;               // [(H + 1) * wpr] NUNIQUE value bitmaps
+  uint32_t wpr, vbase, vflip;
+  // buckets
+  int logP;
+  const int64_t* bstart;     // [P + 1] first record of each bucket
+  unsigned int* hist;        // [P] cold rows per bucket (counting pre-pass)
+  unsigned int* bcursor;     // [P] records written so far (routing pass)
+  unsigned long long* recs;  // 3 words per cold row
+  int* flag;                 // a float sum value outside the fixed-point range
+};
+
+__device__ __forceinline__ uint64_t part_ord64(uint64_t raw, int type)
+{
+  switch (type) {
+    case LDF_FLOAT32: {
+      const uint32_t b = static_cast<uint32_t>(raw);
+      return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    }
+    case LDF_FLOAT64: return (raw >> 63) ? ~raw : (raw | (1ull << 63));
+    case LDF_INT8: return static_cast<uint64_t>(static_cast<int64_t>(static_cast<int8_t>(raw))) ^ (1ull << 63);
+    case LDF_INT16: return static_cast<uint64_t>(static_cast<int64_t>(static_cast<int16_t>(raw))) ^ (1ull << 63);
+    case LDF_INT32: return static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(raw))) ^ (1ull << 63);
+    case LDF_INT64:
+    case LDF_TIMESTAMP_US: return raw ^ (1ull << 63);
+    default: return raw;
+  }
+}
+__device__ __forceinline__ uint32_t part_ord32(uint64_t raw, int type)
+{
+  switch (type) {
+    case LDF_FLOAT32: {
+      const uint32_t b = static_cast<uint32_t>(raw);
+      return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    }
+    case LDF_INT8: return static_cast<uint32_t>(static_cast<int32_t>(static_cast<int8_t>(raw))) ^ 0x80000000u;
+    case LDF_INT16: return static_cast<uint32_t>(static_cast<int32_t>(static_cast<int16_t>(raw))) ^ 0x80000000u;
+    case LDF_INT32: return static_cast<uint32_t>(raw) ^ 0x80000000u;
+    default: return static_cast<uint32_t>(raw);
+  }
+}
+// 32-bit ordered form -> the 64-bit ordered form of the same value
+__device__ __forceinline__ uint64_t part_widen32(uint32_t o32, int type)
+{
+  if (type == LDF_INT8 || type == LDF_INT16 || type == LDF_INT32) {
+    const int32_t v = static_cast<int32_t>(o32 ^ 0x80000000u);
+    return static_cast<uint64_t>(static_cast<int64_t>(v)) ^ (1ull << 63);
+  }
+  return o32;
+}
+
+__device__ __forceinline__ uint64_t part_load(const DCol& c, int64_t r)
+{
+  switch (c.width) {
+    case 1: return __ldg(static_cast<const uint8_t*>(c.data) + r);
+    case 2: return __ldg(static_cast<const uint16_t*>(c.data) + r);
+    case 4: return __ldg(static_cast<const uint32_t*>(c.data) + r);
+    default: return __ldg(static_cast<const unsigned long long*>(c.data) + r);
+  }
+}
+
+// Add one valid value of column `c` into a 32-bit record (shared memory or
+// per-CTA global scratch; generic addresses).  Returns false for a float sum
+// value outside the fixed-point range.
+__device__ __forceinline__ bool part_add(const PVal& c, unsigned char* rec, uint64_t raw)
+{
+  bool ok = true;
+  if (c.nullable) atomicAdd(reinterpret_cast<uint32_t*>(rec + c.b_vc), 1u);
+  if (c.states & ST_SUM) {
+    uint32_t* sum = reinterpret_cast<uint32_t*>(rec + c.b_sum);
+    if (c.fixed) {
+      const double x = c.col.width == 8 ? __longlong_as_double(static_cast<long long>(raw))
+                                        : static_cast<double>(__uint_as_float(static_cast<uint32_t>(raw)));
+      uint64_t m;
+      int sh;
+      bool neg;
+      if (fixed_parts(x, m, sh, neg)) {
+        if (m) {
+          const int j0 = sh >> 5, b = sh & 31;
+          sh_add_magnitude(sum, c.chunks, j0, m << b, b ? (m >> (64 - b)) : 0, neg);
+        }
+      } else {
+        ok = false;
+      }
+    } else {
+      uint64_t mag = raw;
+      bool neg     = false;
+      if (is_signed_int_dev(c.col.type)) {
+        const int64_t v = c.col.width == 1 ? static_cast<int8_t>(raw) : c.col.width == 2 ? static_cast<int16_t>(raw)
+                        : c.col.width == 4 ? static_cast<int32_t>(raw) : static_cast<int64_t>(raw);
+        neg = v < 0;
+        mag = neg ? (0ull - static_cast<uint64_t>(v)) : static_cast<uint64_t>(v);
+      }
+      sh_add_magnitude(sum, c.chunks, 0, mag, 0, neg);
+    }
+  }
+  if (c.states & (ST_MIN | ST_MAX)) {
+    if (c.mm64) {
+      const uint64_t o = part_ord64(raw, c.col.type);
+      if (c.states & ST_MIN) atomicMax(reinterpret_cast<unsigned long long*>(rec + c.b_mn), ~o);
+      if (c.states & ST_MAX) atomicMax(reinterpret_cast<unsigned long long*>(rec + c.b_mx), o);
+    } else {
+      const uint32_t o = part_ord32(raw, c.col.type);
+      if (c.states & ST_MIN) atomicMax(reinterpret_cast<uint32_t*>(rec + c.b_mn), ~o);
+      if (c.states & ST_MAX) atomicMax(reinterpret_cast<uint32_t*>(rec + c.b_mx), o);
+    }
+  }
+  return ok;
+}
+
+// The aggregates of one group, unpacked from either record form.
+struct PartVals {
+  uint64_t call;
+  uint64_t vc[2];
+  unsigned long long acc[2][kSumChunks];  // signed chunk sums (float) / acc[c][0] = sum mod 2^64 (integer)
+  uint64_t omn[2], omx[2];                // 64-bit ordered min / max
+};
+
+// from a 32-bit record (bucket pass)
+__device__ __forceinline__ void part_unpack32(const PartArgs& a, const unsigned char* rec, PartVals& v)
+{
+  v.call = *reinterpret_cast<const uint32_t*>(rec + 8);
+  for (int ci = 0; ci < a.ncol; ++ci) {
+    const PVal& c = a.c[ci];
+    v.vc[ci]      = c.nullable ? *reinterpret_cast<const uint32_t*>(rec + c.b_vc) : v.call;
+    if (c.states & ST_SUM) {
+      const uint32_t* sum = reinterpret_cast<const uint32_t*>(rec + c.b_sum);
+      uint64_t tot        = 0;
+      for (int q = 0; q < c.chunks; ++q) {
+        const int64_t pos = static_cast<int64_t>(sum[q * 4 + 0]) + (static_cast<int64_t>(sum[q * 4 + 1]) << 32);
+        const int64_t neg = static_cast<int64_t>(sum[q * 4 + 2]) + (static_cast<int64_t>(sum[q * 4 + 3]) << 32);
+        v.acc[ci][q]      = static_cast<unsigned long long>(pos - neg);
+        tot += static_cast<uint64_t>(pos - neg) << (32 * q);
+      }
+      if (!c.fixed) v.acc[ci][0] = tot;
+    }
+    if (c.states & (ST_MIN | ST_MAX)) {
+      if (c.mm64) {
+        v.omn[ci] = ~*reinterpret_cast<const unsigned long long*>(rec + c.b_mn);
+        v.omx[ci] = *reinterpret_cast<const unsigned long long*>(rec + c.b_mx);
+      } else {
+        v.omn[ci] = part_widen32(~*reinterpret_cast<const uint32_t*>(rec + c.b_mn), c.col.type);
+        v.omx[ci] = part_widen32(*reinterpret_cast<const uint32_t*>(rec + c.b_mx), c.col.type);
+      }
+    }
+  }
+}
+
+// from a global 64-bit hot record (after every CTA flushed into it)
+__device__ __forceinline__ void part_unpack64(const PartArgs& a, const unsigned long long* w, PartVals& v)
+{
+  v.call = w[0];
+  for (int ci = 0; ci < a.ncol; ++ci) {
+    const PVal& c = a.c[ci];
+    v.vc[ci]      = c.nullable ? w[c.w_vc] : v.call;
+    if (c.states & ST_SUM)
+      for (int q = 0; q < (c.fixed ? c.chunks : 1); ++q) v.acc[ci][q] = w[c.w_sum + q];
+    if (c.states & ST_MIN) v.omn[ci] = ~w[c.w_mn];
+    if (c.states & ST_MAX) v.omx[ci] = w[c.w_mx];
+  }
+}
+
+// Output row i of one group: key and every aggregation but NUNIQUE.
+__device__ __forceinline__ void part_emit(const PartArgs& a, const PartOut& o, int64_t i, uint64_t kb, bool knull,
+                                          const PartVals& v)
+{
+  store_int(OCol{o.key.data, nullptr, LDF_UINT64, o.key.width}, i, knull ? 0 : kb);
+  if (o.key.valid) o.key.valid[i] = knull ? 0 : 1;
+  double fsum[2];
+  bool fsum_done[2] = {false, false};
+  for (int k = 0; k < o.nagg; ++k) {
+    const AggOut& g = o.a[k];
+    const OCol& d   = g.dst;
+    if (g.kind == LDF_AGG_COUNT_ALL) {
+      store_int(d, i, v.call);
+      if (d.valid) d.valid[i] = 1;
+      continue;
+    }
+    if (g.kind == LDF_AGG_COUNT_DISTINCT) continue;
+    const int ci  = g.col;
+    const PVal& c = a.c[ci];
+    const uint64_t vc = v.vc[ci];
+    bool ok           = vc > 0;
+    switch (g.kind) {
+      case LDF_AGG_COUNT: {
+        store_int(d, i, g.count_mode == LDF_COUNT_ALL ? v.call : g.count_mode == LDF_COUNT_ONLY_NULL ? v.call - vc : vc);
+        ok = true;
+        break;
+      }
+      case LDF_AGG_SUM:
+      case LDF_AGG_MEAN: {
+        if (!ok) {
+          store_int(d, i, 0);
+          break;
+        }
+        if (c.fixed) {
+          if (!fsum_done[ci]) {
+            fsum[ci]      = chunks_to_double(v.acc[ci], 1);
+            fsum_done[ci] = true;
+          }
+          store_double(d, i, g.kind == LDF_AGG_MEAN ? fsum[ci] / static_cast<double>(vc) : fsum[ci]);
+        } else {
+          const uint64_t s = v.acc[ci][0];
+          const double sd  = is_signed_int_dev(g.in_type) ? static_cast<double>(static_cast<int64_t>(s))
+                                                          : static_cast<double>(s);
+          if (g.kind == LDF_AGG_MEAN) store_double(d, i, sd / static_cast<double>(vc));
+          else if (d.type == LDF_FLOAT64 || d.type == LDF_FLOAT32) store_double(d, i, sd);
+          else store_int(d, i, s);
+        }
+        break;
+      }
+      case LDF_AGG_MIN:
+      case LDF_AGG_MAX: {
+        if (!ok) {
+          store_int(d, i, 0);
+          break;
+        }
+        const uint64_t b = unordered_bits(g.in_type, g.kind == LDF_AGG_MIN ? v.omn[ci] : v.omx[ci]);
+        if (d.type == g.in_type) store_int(OCol{d.data, nullptr, LDF_UINT64, d.width}, i, b);
+        else if (g.in_type == LDF_FLOAT32) store_double(d, i, static_cast<double>(__uint_as_float(static_cast<uint32_t>(b))));
+        else if (g.in_type == LDF_FLOAT64) store_double(d, i, __longlong_as_double(static_cast<long long>(b)));
+        else store_int(d, i, b);
+        break;
+      }
+      default: break;
+    }
+    if (d.valid) d.valid[i] = ok ? 1 : 0;
+  }
+}
+
+// NUNIQUE outputs of output row i: nd distinct valid values; has_null: the
+// group has a null in the column.
+__device__ __forceinline__ void part_emit_nd(const PartOut& o, int64_t i, uint64_t nd, bool has_null)
+{
+  for (int k = 0; k < o.nagg; ++k) {
+    const AggOut& g = o.a[k];
+    if (g.kind != LDF_AGG_COUNT_DISTINCT) continue;
+    const uint64_t hn = has_null ? 1 : 0;
+    store_int(g.dst, i, g.count_mode == LDF_COUNT_ALL ? nd + hn : g.count_mode == LDF_COUNT_ONLY_NULL ? hn : nd);
+    if (g.dst.valid) g.dst.valid[i] = 1;
+  }
+}
+
+// Shared hot key table: slot -> hot id (kPartNoId empty) and key.
+__device__ __forceinline__ void hot_table_build(const PartArgs& a, uint32_t* ids, unsigned long long* keys)
+{
+  for (int i = threadIdx.x; i < kPartHotSlots; i += blockDim.x) ids[i] = kPartNoId;
+  __syncthreads();
+  for (int i = threadIdx.x; i < a.H; i += blockDim.x) {
+    const uint64_t kb = a.hot_keys[i];
+    uint32_t idx      = static_cast<uint32_t>(mix64(kb)) & (kPartHotSlots - 1);
+    for (int probe = 0; probe < kPartHotSlots; ++probe) {
+      if (atomicCAS(ids + idx, kPartNoId, static_cast<uint32_t>(i)) == kPartNoId) {
+        keys[idx] = kb;
+        break;
+      }
+      idx = (idx + 1) & (kPartHotSlots - 1);
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t hot_lookup(const uint32_t* ids, const unsigned long long* keys, uint64_t kb,
+                                               uint64_t h)
+{
+  uint32_t idx = static_cast<uint32_t>(h) & (kPartHotSlots - 1);
+  for (int probe = 0; probe < kPartHotSlots; ++probe) {
+    const uint32_t id = ids[idx];
+    if (id == kPartNoId) return kPartNoId;
+    if (keys[idx] == kb) return id;
+    idx = (idx + 1) & (kPartHotSlots - 1);
+  }
+  return kPartNoId;
+}
+
+__device__ __forceinline__ uint32_t bucket_of(uint64_t h, int logP)
+{
+  return logP == 0 ? 0u : static_cast<uint32_t>(h >> (64 - logP));
+}
+
+// ---- counting pre-pass: cold rows per bucket ---------------------------------
+__global__ void __launch_bounds__(kCountThreads, 1) part_count_kernel(PartArgs a)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* ids            = reinterpret_cast<uint32_t*>(smem);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem + kPartHotSlots * 4);
+  uint32_t* hist           = reinterpret_cast<uint32_t*>(smem + kPartHotSlots * 12);
+  const uint32_t P         = 1u << a.logP;
+  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) hist[i] = 0;
+  hot_table_build(a, ids, keys);
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x * kRows;
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x * kRows; base < a.n; base += step) {
+    uint64_t kb[kRows];
+    bool ok[kRows];
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+      const int64_t r = base + static_cast<int64_t>(j) * blockDim.x + threadIdx.x;
+      ok[j]           = r < a.n && dvalid(a.key, r);
+      kb[j]           = ok[j] ? part_load(a.key, r) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+      if (!ok[j]) continue;
+      const uint64_t h = mix64(kb[j]);
+      if (hot_lookup(ids, keys, kb[j], h) == kPartNoId) atomicAdd(hist + bucket_of(h, a.logP), 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
+    if (hist[i]) atomicAdd(a.hist + i, hist[i]);
+}
+
+// ---- routing pass -----------------------------------------------------------
+__global__ void __launch_bounds__(kPartThreads) part_route_kernel(PartArgs a)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* ids            = reinterpret_cast<uint32_t*>(smem);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem + kPartHotSlots * 4);
+  unsigned char* recs      = smem + kPartHotSlots * 12;
+  const int nrec           = a.H + 1;
+  {
+    uint4* z       = reinterpret_cast<uint4*>(recs);
+    const int n16  = nrec * a.rb / 16;
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) z[i] = make_uint4(0, 0, 0, 0);
+  }
+  hot_table_build(a, ids, keys);
+  bool range_ok      = true;
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x * kRows;
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x * kRows; base < a.n; base += step) {
+    uint64_t kb[kRows], v0[kRows], v1[kRows];
+    uint32_t fl[kRows];  // bit 0: row exists, 1: key valid, 2: value 0 valid, 3: value 1 valid
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+      const int64_t r = base + static_cast<int64_t>(j) * blockDim.x + threadIdx.x;
+      fl[j]           = 0;
+      kb[j] = v0[j] = v1[j] = 0;
+      if (r < a.n) {
+        fl[j] = 1;
+        if (dvalid(a.key, r)) {
+          fl[j] |= 2;
+          kb[j] = part_load(a.key, r);
+        }
+        v0[j] = part_load(a.c[0].col, r);
+        if (dvalid(a.c[0].col, r)) fl[j] |= 4;
+        if (a.ncol > 1) {
+          v1[j] = part_load(a.c[1].col, r);
+          if (dvalid(a.c[1].col, r)) fl[j] |= 8;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+      if (!(fl[j] & 1)) continue;
+      const uint64_t h = mix64(kb[j]);
+      const uint32_t hid = (fl[j] & 2) ? hot_lookup(ids, keys, kb[j], h) : static_cast<uint32_t>(a.H);
+      if (hid != kPartNoId) {
+        unsigned char* rec = recs + static_cast<int64_t>(hid) * a.rb;
+        atomicAdd(reinterpret_cast<uint32_t*>(rec + 8), 1u);
+        if (fl[j] & 4) range_ok &= part_add(a.c[0], rec, v0[j]);
+        if (a.ncol > 1 && (fl[j] & 8)) range_ok &= part_add(a.c[1], rec, v1[j]);
+        if (a.nd >= 0 && (fl[j] & (a.nd == 0 ? 4 : 8))) {
+          const uint32_t off = (static_cast<uint32_t>(a.nd == 0 ? v0[j] : v1[j]) ^ a.vflip) - a.vbase;
+          red_or32(a.bits + static_cast<uint64_t>(hid) * a.wpr + (off >> 5), 1u << (off & 31));
+        }
+      } else {
+        // a cold row: the validity bits ride in the top of the third word
+        // (value 1 is at most 4 bytes)
+        if (a.c[0].fixed && (a.c[0].states & ST_SUM) && (fl[j] & 4)) {
+          const double x = a.c[0].col.width == 8 ? __longlong_as_double(static_cast<long long>(v0[j]))
+                                                 : static_cast<double>(__uint_as_float(static_cast<uint32_t>(v0[j])));
+          uint64_t m;
+          int sh;
+          bool neg;
+          range_ok &= fixed_parts(x, m, sh, neg);
+        }
+        if (a.ncol > 1 && a.c[1].fixed && (a.c[1].states & ST_SUM) && (fl[j] & 8)) {
+          const double x = static_cast<double>(__uint_as_float(static_cast<uint32_t>(v1[j])));
+          uint64_t m;
+          int sh;
+          bool neg;
+          range_ok &= fixed_parts(x, m, sh, neg);
+        }
+        const uint32_t b    = bucket_of(h, a.logP);
+        const int64_t pos   = a.bstart[b] + atomicAdd(a.bcursor + b, 1u);
+        unsigned long long* d = a.recs + 3 * pos;
+        d[0] = kb[j];
+        d[1] = v0[j];
+        d[2] = (v1[j] & 0xffffffffull) | (static_cast<uint64_t>((fl[j] >> 2) & 3) << 32);
+      }
+    }
+  }
+  if (!range_ok) atomicExch(a.flag, 1);
+  __syncthreads();
+  // flush the hot records
+  for (int g = threadIdx.x; g < nrec; g += blockDim.x) {
+    const unsigned char* rec = recs + static_cast<int64_t>(g) * a.rb;
+    const uint32_t call      = *reinterpret_cast<const uint32_t*>(rec + 8);
+    if (call == 0) continue;
+    unsigned long long* w = a.hot_rec + static_cast<int64_t>(g) * a.rw;
+    red_add(w, call);
+    for (int ci = 0; ci < a.ncol; ++ci) {
+      const PVal& c = a.c[ci];
+      if (c.nullable) red_add(w + c.w_vc, *reinterpret_cast<const uint32_t*>(rec + c.b_vc));
+      if (c.states & ST_SUM) {
+        const uint32_t* sum = reinterpret_cast<const uint32_t*>(rec + c.b_sum);
+        uint64_t tot        = 0;
+        for (int q = 0; q < c.chunks; ++q) {
+          const int64_t pos = static_cast<int64_t>(sum[q * 4 + 0]) + (static_cast<int64_t>(sum[q * 4 + 1]) << 32);
+          const int64_t neg = static_cast<int64_t>(sum[q * 4 + 2]) + (static_cast<int64_t>(sum[q * 4 + 3]) << 32);
+          if (c.fixed) {
+            if (pos != neg) red_add(w + c.w_sum + q, static_cast<uint64_t>(pos - neg));
+          } else {
+            tot += static_cast<uint64_t>(pos - neg) << (32 * q);
+          }
+        }
+        if (!c.fixed && tot) red_add(w + c.w_sum, tot);
+      }
+      if (c.states & (ST_MIN | ST_MAX)) {
+        if (c.mm64) {
+          if (c.states & ST_MIN) red_max(w + c.w_mn, *reinterpret_cast<const unsigned long long*>(rec + c.b_mn));
+          if (c.states & ST_MAX) red_max(w + c.w_mx, *reinterpret_cast<const unsigned long long*>(rec + c.b_mx));
+        } else {
+          // an untouched word flushes the identity of the opposite extreme
+          if (c.states & ST_MIN)
+            red_max(w + c.w_mn, ~part_widen32(~*reinterpret_cast<const uint32_t*>(rec + c.b_mn), c.col.type));
+          if (c.states & ST_MAX)
+            red_max(w + c.w_mx, part_widen32(*reinterpret_cast<const uint32_t*>(rec + c.b_mx), c.col.type));
+        }
+      }
+    }
+  }
+}
+
+// ---- hot groups: one output row each (a CTA per hot record) ----------------
+__global__ void __launch_bounds__(256) part_hot_emit_kernel(PartArgs a, PartOut o, unsigned long long* out_count,
+                                                            int64_t out_cap)
+{
+  __shared__ unsigned long long part[8];
+  __shared__ int64_t s_pos;
+  for (int g = blockIdx.x; g <= a.H; g += gridDim.x) {
+    const unsigned long long* w = a.hot_rec + static_cast<int64_t>(g) * a.rw;
+    if (w[0] == 0) continue;  // uniform across the block
+    unsigned long long c = 0;
+    if (a.nd >= 0) {
+      const uint4* w4 = reinterpret_cast<const uint4*>(a.bits + static_cast<uint64_t>(g) * a.wpr);
+      for (uint32_t i = threadIdx.x; i < a.wpr / 4; i += blockDim.x) {
+        const uint4 q = w4[i];
+        c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+      }
+      for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+      if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    }
+    if (threadIdx.x == 0) s_pos = static_cast<int64_t>(atomicAdd(out_count, 1ull));
+    __syncthreads();
+    const int64_t pos = s_pos;
+    if (threadIdx.x == 0 && pos < out_cap) {
+      PartVals v;
+      part_unpack64(a, w, v);
+      const bool knull = g == a.H;
+      part_emit(a, o, pos, knull ? 0 : a.hot_keys[g], knull, v);
+      if (a.nd >= 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < static_cast<int>((blockDim.x + 31) >> 5); ++i) t += part[i];
+        part_emit_nd(o, pos, t, v.call > v.vc[a.nd]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- bucket pass ---------------------------------------------------------------
+// Work memory of one bucket: local key table (ids + keys, `ks` slots, a power
+// of two), records (`gc` groups of a.rb bytes; key word at offset 0, the
+// group's row count at 8), NUNIQUE counts and null flags per group, and a
+// pair set of `ps` 8-byte slots that reuses the record space once the
+// records have been written out.
+struct BucketMem {
+  uint32_t* ids;
+  unsigned long long* keys;
+  unsigned char* recs;
+  uint32_t* nd;
+  uint8_t* hasnull;
+  unsigned long long* pairs;
+  int ks;
+  int gc;
+  int64_t ps;
+};
+
+struct BucketArgs {
+  PartArgs a;
+  PartOut o;
+  unsigned long long* out_count;
+  int64_t out_cap;
+  const int32_t* list;         // large pass: bucket ids to take (nullptr: every bucket)
+  int64_t nlist;
+  unsigned long long* next;    // bucket counter
+  int32_t* deferred;           // shared-memory pass: buckets that did not fit
+  unsigned int* ndeferred;
+  int64_t small_rows;          // shared-memory pass: buckets above this many rows are skipped
+  // large pass: per-CTA global work memory
+  unsigned char* scratch;
+  int64_t scratch_stride;
+  int ks, gc;
+  int64_t ps;
+  int* err;
+};
+
+// Local id of key kb in the bucket's key table, inserting it when new (the
+// inserting thread claims the slot, then publishes the key and the id; a
+// reader that finds the slot claimed waits for the id, bounded).  *fresh is
+// set for the inserting thread.
+__device__ __forceinline__ uint32_t local_id(const BucketMem& m, uint32_t* nlocal, uint64_t kb, uint64_t h,
+                                             int* err, bool* fresh)
+{
+  uint32_t idx = static_cast<uint32_t>(h) & (m.ks - 1);
+  *fresh       = false;
+  for (int probe = 0; probe < m.ks; ++probe) {
+    uint32_t id = *reinterpret_cast<volatile uint32_t*>(m.ids + idx);
+    if (id == kPartNoId) {
+      id = atomicCAS(m.ids + idx, kPartNoId, kPartBusy);
+      if (id == kPartNoId) {  // claimed: publish key, then id
+        const uint32_t lid = atomicAdd(nlocal, 1u);
+        m.keys[idx]        = kb;
+        __threadfence_block();
+        atomicExch(m.ids + idx, lid);
+        *fresh = true;
+        return lid;
+      }
+    }
+    if (id == kPartBusy) {  // another thread of the CTA is publishing this slot
+      uint32_t spin = 0;
+      do {
+        id = *reinterpret_cast<volatile uint32_t*>(m.ids + idx);
+        if (++spin > kSpinLimit) {
+          atomicExch(err, LDF_ERR_TIMEOUT);
+          return kPartNoId;
+        }
+      } while (id == kPartBusy);
+      __threadfence_block();
+    }
+    if (reinterpret_cast<volatile unsigned long long*>(m.keys)[idx] == kb) return id;
+    idx = (idx + 1) & (m.ks - 1);
+  }
+  return kPartNoId;  // the table is sized above the rows: not reached
+}
+
+// Aggregates one bucket: rows [r0, r1) of a.recs.  Returns false (nothing
+// written) when the bucket has more groups than m.gc.
+__device__ bool process_bucket(const BucketArgs& B, const BucketMem& m, int64_t r0, int64_t r1, uint32_t* sh_nlocal,
+                               int64_t* sh_base)
+{
+  const PartArgs& a = B.a;
+  const int64_t rows = r1 - r0;
+  // clear the work memory
+  for (int i = threadIdx.x; i < m.ks; i += blockDim.x) m.ids[i] = kPartNoId;
+  {
+    const int64_t n16 = static_cast<int64_t>(m.gc) * a.rb / 16;
+    uint4* z          = reinterpret_cast<uint4*>(m.recs);
+    for (int64_t i = threadIdx.x; i < n16; i += blockDim.x) z[i] = make_uint4(0, 0, 0, 0);
+  }
+  if (threadIdx.x == 0) *sh_nlocal = 0;
+  __syncthreads();
+  // records into the local groups
+  for (int64_t i = threadIdx.x; i < rows; i += blockDim.x) {
+    const unsigned long long* s = a.recs + 3 * (r0 + i);
+    const uint64_t kb = s[0], w1 = s[1], w2 = s[2];
+    bool fresh;
+    const uint32_t lid = local_id(m, sh_nlocal, kb, mix64(kb), B.err, &fresh);
+    if (lid >= static_cast<uint32_t>(m.gc)) continue;
+    unsigned char* rec = m.recs + static_cast<int64_t>(lid) * a.rb;
+    if (fresh) *reinterpret_cast<unsigned long long*>(rec) = kb;
+    atomicAdd(reinterpret_cast<uint32_t*>(rec + 8), 1u);
+    if ((w2 >> 32) & 1) part_add(a.c[0], rec, w1);
+    if (a.ncol > 1 && ((w2 >> 33) & 1)) part_add(a.c[1], rec, w2 & 0xffffffffull);
+  }
+  __syncthreads();
+  const uint32_t ng = *sh_nlocal;
+  if (ng > static_cast<uint32_t>(m.gc)) return false;
+  if (threadIdx.x == 0) *sh_base = static_cast<int64_t>(atomicAdd(B.out_count, static_cast<unsigned long long>(ng)));
+  __syncthreads();
+  const int64_t base = *sh_base;
+  for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
+    const unsigned char* rec = m.recs + static_cast<int64_t>(g) * a.rb;
+    PartVals v;
+    part_unpack32(a, rec, v);
+    if (a.nd >= 0) {
+      m.nd[g]      = 0;
+      m.hasnull[g] = v.call > v.vc[a.nd] ? 1 : 0;
+    }
+    if (base + g < B.out_cap) part_emit(a, B.o, base + g, *reinterpret_cast<const unsigned long long*>(rec), false, v);
+  }
+  if (a.nd < 0) {
+    __syncthreads();
+    return true;
+  }
+  // NUNIQUE: (local id, value) pairs of the valid rows, counted when new
+  __syncthreads();
+  const int64_t ps = m.ps < 2 * rows + 64 ? m.ps : 2 * rows + 64;
+  for (int64_t i = threadIdx.x; i < ps; i += blockDim.x) m.pairs[i] = kEmpty;
+  __syncthreads();
+  const uint64_t vbit = a.nd == 0 ? (1ull << 32) : (2ull << 32);
+  for (int64_t i = threadIdx.x; i < rows; i += blockDim.x) {
+    const unsigned long long* s = a.recs + 3 * (r0 + i);
+    const uint64_t kb = s[0], w2 = s[2];
+    if (!(w2 & vbit)) continue;
+    const uint32_t x   = static_cast<uint32_t>(a.nd == 0 ? s[1] : w2);
+    bool fresh;
+    const uint32_t lid = local_id(m, sh_nlocal, kb, mix64(kb), B.err, &fresh);  // present: a pure lookup
+    if (lid >= ng) continue;  // only after an expired wait (reported through B.err)
+    const uint64_t e   = (static_cast<uint64_t>(lid) << 32) | x;
+    uint64_t idx       = fastrange(mix64(e), static_cast<uint64_t>(ps));
+    for (int64_t probe = 0; probe < ps; ++probe) {
+      const unsigned long long cur = atomicCAS(m.pairs + idx, kEmpty, e);
+      if (cur == kEmpty) {
+        atomicAdd(m.nd + lid, 1u);
+        break;
+      }
+      if (cur == e) break;
+      idx = idx + 1 == static_cast<uint64_t>(ps) ? 0 : idx + 1;
+    }
+  }
+  __syncthreads();
+  for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x)
+    if (base + g < B.out_cap) part_emit_nd(B.o, base + g, m.nd[g], m.hasnull[g] != 0);
+  __syncthreads();
+  return true;
+}
+
+// Shared-memory bucket pass: persistent CTAs take buckets in order; a bucket
+// above `small_rows` rows is left to the large pass, one with more groups
+// than the shared records hold is deferred to it.
+__global__ void __launch_bounds__(kBucketThreads, 1) part_bucket_kernel(BucketArgs B)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t s_nlocal;
+  __shared__ int64_t s_base;
+  __shared__ int64_t s_bucket;
+  BucketMem m;
+  m.ids     = reinterpret_cast<uint32_t*>(smem);
+  m.keys    = reinterpret_cast<unsigned long long*>(smem + kBucketKeySlots * 4);
+  m.recs    = smem + kBucketKeySlots * 12;
+  m.pairs   = reinterpret_cast<unsigned long long*>(m.recs);
+  m.nd      = reinterpret_cast<uint32_t*>(m.recs + kBucketRecBytes);
+  m.hasnull = reinterpret_cast<uint8_t*>(m.nd + kBucketGroupsMax);
+  m.ks      = kBucketKeySlots;
+  m.gc      = min(kBucketGroupsMax, kBucketRecBytes / B.a.rb);
+  m.ps      = kBucketRecBytes / 8;
+  const uint32_t P = 1u << B.a.logP;
+  for (;;) {
+    if (threadIdx.x == 0) s_bucket = static_cast<int64_t>(atomicAdd(B.next, 1ull));
+    __syncthreads();
+    const int64_t b = s_bucket;
+    __syncthreads();
+    if (b >= P) break;
+    const int64_t r0 = B.a.bstart[b], r1 = B.a.bstart[b + 1];
+    if (r1 == r0 || r1 - r0 > B.small_rows) continue;
+    if (!process_bucket(B, m, r0, r1, &s_nlocal, &s_base)) {
+      if (threadIdx.x == 0) B.deferred[atomicAdd(B.ndeferred, 1u)] = static_cast<int32_t>(b);
+      __syncthreads();
+    }
+  }
+}
+
+// Large bucket pass: the same work on per-CTA global memory sized for the
+// largest of the listed buckets.
+__global__ void __launch_bounds__(kBucketThreads, 1) part_bucket_large_kernel(BucketArgs B)
+{
+  __shared__ uint32_t s_nlocal;
+  __shared__ int64_t s_base;
+  __shared__ int64_t s_item;
+  unsigned char* w = B.scratch + static_cast<int64_t>(blockIdx.x) * B.scratch_stride;
+  BucketMem m;
+  m.ids     = reinterpret_cast<uint32_t*>(w);
+  m.keys    = reinterpret_cast<unsigned long long*>(w + static_cast<int64_t>(B.ks) * 4);
+  m.recs    = w + static_cast<int64_t>(B.ks) * 12;
+  m.pairs   = reinterpret_cast<unsigned long long*>(m.recs);
+  const int64_t rbytes = static_cast<int64_t>(B.gc) * B.a.rb > B.ps * 8 ? static_cast<int64_t>(B.gc) * B.a.rb : B.ps * 8;
+  m.nd      = reinterpret_cast<uint32_t*>(m.recs + rbytes);
+  m.hasnull = reinterpret_cast<uint8_t*>(m.nd + B.gc);
+  m.ks      = B.ks;
+  m.gc      = B.gc;
+  m.ps      = B.ps;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = static_cast<int64_t>(atomicAdd(B.next, 1ull));
+    __syncthreads();
+    const int64_t it = s_item;
+    __syncthreads();
+    if (it >= B.nlist) break;
+    const int32_t b = B.list[it];
+    process_bucket(B, m, B.a.bstart[b], B.a.bstart[b + 1], &s_nlocal, &s_base);
+  }
+}
+
+// ---- sample: the most frequent keys -------------------------------------------
+// Strided sample of the keys into an open-addressing table {key, count}
+// (slot taken when its count word leaves 0), counts warp-aggregated.
+__global__ void part_sample_kernel(DCol key, int64_t n_sample, int64_t stride, unsigned long long* keys,
+                                   unsigned int* counts, uint64_t cap)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_sample;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i * stride;
+    int64_t g       = -1;
+    if (dvalid(key, r)) {
+      const uint64_t kb = part_load(key, r);
+      uint64_t idx      = fastrange(mix64(kb), cap);
+      for (int probe = 0; probe < kMaxProbe; ++probe) {
+        const unsigned long long v = atomicCAS(keys + idx, kEmpty, kb);
+        if (v == kEmpty || v == kb) {
+          g = static_cast<int64_t>(idx);
+          break;
+        }
+        idx = idx + 1 == cap ? 0 : idx + 1;
+      }
+    }
+    const uint32_t active = __activemask();
+    const uint32_t peers  = __match_any_sync(active, static_cast<unsigned long long>(g));
+    if (g >= 0 && (threadIdx.x & 31) == static_cast<unsigned>(__ffs(peers) - 1))
+      atomicAdd(&counts[g], static_cast<unsigned>(__popc(peers)));
+  }
+}
+
+// hist[min(count, 4095)] over the occupied slots; out[0] occupied, out[1] singletons
+__global__ void part_sample_stats_kernel(const unsigned int* counts, uint64_t cap, unsigned int* hist,
+                                         unsigned long long* out)
+{
+  unsigned long long occ = 0, f1 = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < static_cast<int64_t>(cap);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned int c = counts[i];
+    if (c == 0) continue;
+    ++occ;
+    f1 += c == 1;
+    atomicAdd(hist + min(c, 4095u), 1u);
+  }
+  occ = warp_reduce_sum(occ);
+  f1  = warp_reduce_sum(f1);
+  if ((threadIdx.x & 31) == 0) {
+    if (occ) atomicAdd(&out[0], occ);
+    if (f1) atomicAdd(&out[1], f1);
+  }
+}
+
+// keys with count >= threshold -> hot list (at most hmax)
+__global__ void part_hot_select_kernel(const unsigned long long* keys, const unsigned int* counts, uint64_t cap,
+                                       unsigned int threshold, unsigned long long* hot, unsigned int* nhot, int hmax)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < static_cast<int64_t>(cap);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (counts[i] < threshold || counts[i] == 0) continue;
+    const unsigned int at = atomicAdd(nhot, 1u);
+    if (at < static_cast<unsigned>(hmax)) hot[at] = keys[i];
+  }
+}
+
+// ---- host ----------------------------------------------------------------------
+// Runs the partitioned plan when it applies; false (nothing written to `out`)
+// when it does not, or when a float sum value fell outside the fixed-point
+// range, so the caller runs the general plan.
+bool try_partitioned(const OpContext& ctx, const GbPlan& p, const ldf_column* table, const int32_t* keys, int nkeys,
+                     const ldf_aggregation* aggs, int naggs, const std::vector<int>& agg_col, ldf_column* out,
+                     const HostStaging& hs, const std::vector<int>& col_of_plan)
+{
+  if (const char* e = std::getenv("LDF_B200_GB_PART"))
+    if (std::atoi(e) == 0) return false;
+  int64_t min_rows = int64_t(1) << 22;
+  if (const char* e = std::getenv("LDF_B200_GB_PART_MIN_ROWS")) min_rows = std::max(0ll, std::atoll(e));
+  const int64_t n = p.n;
+  if (nkeys != 1 || n < std::max<int64_t>(min_rows, 1) || p.ncols < 1 || p.ncols > 2) return false;
+  const ldf_column& kc = table[keys[0]];
+  if (kc.type == LDF_STRING) return false;
+  // value columns: the one of at most 4 bytes second
+  int order[2] = {0, 1};
+  if (p.ncols == 2 && type_width(p.c[1].col.type) > 4) std::swap(order[0], order[1]);
+  if (p.ncols == 2 && type_width(p.c[order[1]].col.type) > 4) return false;
+  int nd = -1;
+  for (int q = 0; q < p.ncols; ++q) {
+    const ColPlan& c = p.c[order[q]];
+    if (c.col.type == LDF_STRING) return false;
+    if (c.states & ST_NDIST) {
+      if (nd >= 0 || type_width(c.col.type) > 4) return false;
+      nd = q;
+    }
+  }
+  const Allocator& al = ctx.alloc();
+  cudaStream_t s      = ctx.stream();
+  const int nsm       = num_sms();
+
+  PartArgs a{};
+  a.key  = make_dcol(kc);
+  a.n    = n;
+  a.ncol = p.ncols;
+  a.nd   = nd;
+  // record layouts
+  int b = 12, w = 1;
+  for (int q = 0; q < a.ncol; ++q) {
+    PVal& v     = a.c[q];
+    const ColPlan& c = p.c[order[q]];
+    v.col       = c.col;
+    v.nullable  = c.nullable;
+    v.states    = c.states;
+    v.fixed     = c.fixed;
+    v.chunks    = c.fixed ? kSumChunks : 2;
+    v.mm64      = type_width(c.col.type) > 4 ? 1 : 0;
+    if (v.nullable) {
+      v.b_vc = b;
+      b += 4;
+      v.w_vc = w++;
+    }
+  }
+  b = (b + 15) & ~15;
+  for (int q = 0; q < a.ncol; ++q) {
+    PVal& v = a.c[q];
+    if (v.states & ST_SUM) {
+      v.b_sum = b;
+      b += 16 * v.chunks;
+      v.w_sum = w;
+      w += v.fixed ? v.chunks : 1;
+    }
+  }
+  for (int q = 0; q < a.ncol; ++q) {
+    PVal& v       = a.c[q];
+    const int mmw = v.mm64 ? 8 : 4;
+    if (v.states & ST_MIN) {
+      b = (b + mmw - 1) & ~(mmw - 1);
+      v.b_mn = b;
+      b += mmw;
+      v.w_mn = w++;
+    }
+    if (v.states & ST_MAX) {
+      b = (b + mmw - 1) & ~(mmw - 1);
+      v.b_mx = b;
+      b += mmw;
+      v.w_mx = w++;
+    }
+  }
+  a.rb = (b + 15) & ~15;
+  a.rw = w;
+
+  for (int j = 0; j < nkeys; ++j) hs.wait(keys[j]);
+  // ---- sample: key frequencies (+ the NUNIQUE column's value range) ------------
+  const int64_t ns     = std::min<int64_t>(n, int64_t(1) << 20);
+  const int64_t stride = n / ns;
+  const uint64_t scap  = static_cast<uint64_t>(2 * ns + 64);
+  Buffer<unsigned long long> skeys(al, scap);
+  Buffer<unsigned int> scounts(al, scap);
+  Buffer<unsigned int> shist(al, 4096 + 4 + 2);  // count histogram, {occupied, singletons} (u64), value range
+  LDF_CUDA(cudaMemsetAsync(skeys.get(), 0xff, scap * 8, s));
+  LDF_CUDA(cudaMemsetAsync(scounts.get(), 0, scap * 4, s));
+  LDF_CUDA(cudaMemsetAsync(shist.get(), 0, (4096 + 4) * 4, s));
+  unsigned int* vr = shist.get() + 4096 + 4;
+  const unsigned int vr_init[2] = {0xffffffffu, 0u};
+  LDF_CUDA(cudaMemcpyAsync(vr, vr_init, 8, cudaMemcpyHostToDevice, s));
+  launch("sample", part_sample_kernel, gs_blocks(ns, 256), 256, 0, s, a.key, ns, stride, skeys.get(), scounts.get(),
+         scap);
+  launch("freq_stats", part_sample_stats_kernel, gs_blocks(scap, 256), 256, 0, s,
+         static_cast<const unsigned int*>(scounts.get()), scap, shist.get(),
+         reinterpret_cast<unsigned long long*>(shist.get() + 4096));
+  if (nd >= 0) {
+    a.vflip = (a.c[nd].col.width == 4 && is_signed_int(a.c[nd].col.type)) ? 0x80000000u : 0u;
+    hs.wait(col_of_plan[order[nd]]);
+    const int wd = a.c[nd].col.width;
+    auto vk      = wd == 1 ? value_range_kernel<1> : wd == 2 ? value_range_kernel<2> : value_range_kernel<4>;
+    launch("value_range", vk, static_cast<unsigned>(4 * nsm), 256, 0, s, a.c[nd].col, n, a.vflip, vr);
+  }
+  std::vector<unsigned int> hh(4096 + 4 + 2);
+  LDF_CUDA(cudaMemcpyAsync(hh.data(), shist.get(), hh.size() * 4, cudaMemcpyDeviceToHost, s));
+  ctx.finish();
+  unsigned long long occ_f1[2];
+  std::memcpy(occ_f1, hh.data() + 4096, 16);
+  const double scale       = std::sqrt(static_cast<double>(n) / static_cast<double>(ns));
+  const int64_t est_groups = std::min<int64_t>(
+    n, static_cast<int64_t>(scale * occ_f1[1] + (occ_f1[0] - occ_f1[1])) + 1);
+  // hot set: bounded by shared memory (two routing CTAs per SM) and, with
+  // NUNIQUE, by the value bitmaps' budget
+  const int smem_route_budget = 110 * 1024;
+  int hmax = std::min(kPartHotMax, (smem_route_budget - kPartHotSlots * 12) / a.rb - 1);
+  if (nd >= 0) {
+    if (hh[4096 + 4] > hh[4096 + 5]) {  // no valid value: a one-word range
+      hh[4096 + 4] = 0;
+      hh[4096 + 5] = 0;
+    }
+    a.vbase              = hh[4096 + 4];
+    const uint64_t range = static_cast<uint64_t>(hh[4096 + 5]) - hh[4096 + 4] + 1;
+    a.wpr                = static_cast<uint32_t>((((range + 31) / 32) + 3) / 4 * 4);
+    uint64_t budget      = 96ull << 20;
+    if (const char* e = std::getenv("LDF_B200_ND_BITMAP_MB")) budget = std::max(0ll, std::atoll(e)) << 20;
+    const int64_t hb = static_cast<int64_t>(budget / (4ull * a.wpr)) - 1;
+    if (hb < 16) return false;  // value range too wide for the bitmaps
+    hmax = static_cast<int>(std::min<int64_t>(hmax, hb));
+  }
+  // smallest count threshold (>= 2) whose keys fit the hot set
+  int64_t above = 0;
+  unsigned int thr = 4096;
+  for (int c = 4095; c >= 2; --c) {
+    if (above + hh[c] > hmax) break;
+    above += hh[c];
+    thr = static_cast<unsigned int>(c);
+  }
+  a.H = static_cast<int>(above);
+  Buffer<unsigned long long> hot_keys(al, std::max(a.H, 1));
+  if (a.H > 0) {
+    Buffer<unsigned int> nhot(al, 1);
+    LDF_CUDA(cudaMemsetAsync(nhot.get(), 0, 4, s));
+    launch("hot_select", part_hot_select_kernel, gs_blocks(scap, 256), 256, 0, s,
+           static_cast<const unsigned long long*>(skeys.get()), static_cast<const unsigned int*>(scounts.get()),
+           scap, thr, hot_keys.get(), nhot.get(), a.H);
+  }
+  a.hot_keys = hot_keys.get();
+  // buckets: about 200 groups each
+  int logP = 0;
+  while (logP < 15 && (int64_t(200) << logP) < est_groups) ++logP;
+  a.logP          = logP;
+  const int64_t P = int64_t(1) << logP;
+
+  // ---- counting pre-pass ---------------------------------------------------------
+  Buffer<unsigned int> hist(al, P);
+  LDF_CUDA(cudaMemsetAsync(hist.get(), 0, P * 4, s));
+  a.hist = hist.get();
+  const size_t count_smem = kPartHotSlots * 12 + P * 4;
+  LDF_CUDA(cudaFuncSetAttribute(part_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(count_smem)));
+  int occ = 1;
+  LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, part_count_kernel, kCountThreads, count_smem));
+  launch("part_count", part_count_kernel, static_cast<unsigned>(std::max(occ, 1) * nsm), kCountThreads, count_smem, s,
+         a);
+  std::vector<unsigned int> hist_h(P);
+  LDF_CUDA(cudaMemcpyAsync(hist_h.data(), hist.get(), P * 4, cudaMemcpyDeviceToHost, s));
+  ctx.finish();
+  std::vector<int64_t> bstart_h(P + 1);
+  int64_t cold = 0;
+  for (int64_t q = 0; q < P; ++q) {
+    bstart_h[q] = cold;
+    cold += hist_h[q];
+  }
+  bstart_h[P] = cold;
+  const int64_t small_rows = kBucketRecBytes / 8 / 2 - 64;
+  std::vector<int32_t> large_h;
+  int64_t large_max = 0;
+  for (int64_t q = 0; q < P; ++q)
+    if (hist_h[q] > small_rows) {
+      large_h.push_back(static_cast<int32_t>(q));
+      large_max = std::max<int64_t>(large_max, hist_h[q]);
+    }
+  Buffer<int64_t> bstart(al, P + 1);
+  LDF_CUDA(cudaMemcpyAsync(bstart.get(), bstart_h.data(), (P + 1) * 8, cudaMemcpyHostToDevice, s));
+  a.bstart = bstart.get();
+
+  // ---- routing pass ----------------------------------------------------------------
+  Buffer<unsigned int> bcursor(al, P);
+  Buffer<unsigned long long> recs(al, std::max<int64_t>(3 * cold, 1));
+  Buffer<unsigned long long> hot_rec(al, static_cast<int64_t>(a.H + 1) * a.rw);
+  Buffer<uint32_t> bits;
+  Buffer<int> flag(al, 1);
+  LDF_CUDA(cudaMemsetAsync(bcursor.get(), 0, P * 4, s));
+  LDF_CUDA(cudaMemsetAsync(hot_rec.get(), 0, static_cast<size_t>(a.H + 1) * a.rw * 8, s));
+  LDF_CUDA(cudaMemsetAsync(flag.get(), 0, 4, s));
+  if (nd >= 0) {
+    bits = Buffer<uint32_t>(al, static_cast<int64_t>(a.H + 1) * a.wpr);
+    LDF_CUDA(cudaMemsetAsync(bits.get(), 0, static_cast<size_t>(a.H + 1) * a.wpr * 4, s));
+    a.bits = bits.get();
+  }
+  a.bcursor = bcursor.get();
+  a.recs    = recs.get();
+  a.hot_rec = hot_rec.get();
+  a.flag    = flag.get();
+  for (int q = 0; q < a.ncol; ++q) hs.wait(col_of_plan[order[q]]);
+  const size_t route_smem = kPartHotSlots * 12 + static_cast<size_t>(a.H + 1) * a.rb;
+  LDF_CUDA(cudaFuncSetAttribute(part_route_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(route_smem)));
+  LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, part_route_kernel, kPartThreads, route_smem));
+  launch("part_route", part_route_kernel,
+         static_cast<unsigned>(std::min<int64_t>(std::max(occ, 1) * nsm, ceil_div(n, int64_t(kPartThreads) * kRows))),
+         kPartThreads, route_smem, s, a);
+
+  // ---- outputs, bucket passes, hot groups ---------------------------------------
+  PartOut o{};
+  o.nagg = naggs;
+  int64_t cap_out = std::min<int64_t>(cold + a.H + 1, 2 * est_groups + a.H + 4096);
+  std::vector<ldf_column> big(nkeys + naggs);
+  auto alloc_outputs = [&](int64_t rows) {
+    big[0] = alloc_out_column(al, kc.type, rows, kc.valid != nullptr);
+    o.key  = OCol{big[0].data, big[0].valid, kc.type, type_width(kc.type)};
+    for (int g = 0; g < naggs; ++g) {
+      const ldf_aggregation& ag = aggs[g];
+      const bool nullable       = !(ag.kind == LDF_AGG_COUNT_ALL || ag.kind == LDF_AGG_COUNT_DISTINCT);
+      big[1 + g]                = alloc_out_column(al, ag.out_type, rows, nullable);
+      AggOut& x                 = o.a[g];
+      x.kind                    = ag.kind;
+      x.count_mode              = ag.count_mode;
+      x.col                     = -1;
+      if (agg_col[g] >= 0) x.col = agg_col[g] == order[0] ? 0 : 1;
+      x.in_type = ag.kind == LDF_AGG_COUNT_ALL ? LDF_INT64 : table[ag.in_col].type;
+      x.dst     = OCol{big[1 + g].data, big[1 + g].valid, ag.out_type, type_width(ag.out_type)};
+    }
+  };
+  auto free_outputs = [&]() {
+    for (auto& c : big) free_out_column(al, c);
+  };
+  Buffer<unsigned long long> counters(al, 4);  // out rows, bucket counter, large counter, deferred count
+  Buffer<int32_t> deferred(al, P);
+  BucketArgs B{};
+  B.a          = a;
+  B.out_count  = counters.get();
+  B.small_rows = small_rows;
+  B.err        = ctx.err();
+  B.deferred   = deferred.get();
+  B.ndeferred  = reinterpret_cast<unsigned int*>(counters.get() + 3);
+  Buffer<int32_t> large(al, std::max<int64_t>(static_cast<int64_t>(large_h.size()), 1));
+  if (!large_h.empty())
+    LDF_CUDA(cudaMemcpyAsync(large.get(), large_h.data(), large_h.size() * 4, cudaMemcpyHostToDevice, s));
+  const size_t bucket_smem = kBucketKeySlots * 12 + kBucketRecBytes + kBucketGroupsMax * 5;
+  LDF_CUDA(cudaFuncSetAttribute(part_bucket_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(bucket_smem)));
+  // per-CTA global work memory of the large pass, sized for `rows` rows
+  auto large_pass = [&](const int32_t* list, int64_t nlist, int64_t rows) {
+    if (nlist == 0) return;
+    int ks = 64;
+    while (ks < 2 * rows + 64) ks *= 2;
+    const int64_t gc  = rows;
+    const int64_t ps  = 2 * rows + 64;
+    const int64_t rbytes = std::max<int64_t>(gc * a.rb, ps * 8);
+    const int64_t stride = ((static_cast<int64_t>(ks) * 12 + rbytes + gc * 5) + 255) / 256 * 256;
+    const int64_t grid   = std::min<int64_t>(nlist, nsm);
+    Buffer<unsigned char> scratch(al, grid * stride);
+    BucketArgs L = B;
+    L.list           = list;
+    L.nlist          = nlist;
+    L.next           = counters.get() + 2;
+    L.scratch        = scratch.get();
+    L.scratch_stride = stride;
+    L.ks             = ks;
+    L.gc             = static_cast<int>(gc);
+    L.ps             = ps;
+    LDF_CUDA(cudaMemsetAsync(counters.get() + 2, 0, 8, s));
+    launch("part_bucket_large", part_bucket_large_kernel, static_cast<unsigned>(grid), kBucketThreads, 0, s, L);
+  };
+  for (int attempt = 0;; ++attempt) {
+    alloc_outputs(cap_out);
+    B.o       = o;
+    B.out_cap = cap_out;
+    B.next    = counters.get() + 1;
+    LDF_CUDA(cudaMemsetAsync(counters.get(), 0, 32, s));
+    launch("part_bucket", part_bucket_kernel, static_cast<unsigned>(nsm), kBucketThreads, bucket_smem, s, B);
+    large_pass(large.get(), static_cast<int64_t>(large_h.size()), large_max);
+    launch("part_hot_emit", part_hot_emit_kernel, static_cast<unsigned>(std::min(a.H + 1, 4 * nsm)), 256, 0, s, a,
+           o, counters.get(), cap_out);
+    unsigned long long cnt[4];
+    int fl = 0;
+    LDF_CUDA(cudaMemcpyAsync(cnt, counters.get(), 32, cudaMemcpyDeviceToHost, s));
+    LDF_CUDA(cudaMemcpyAsync(&fl, flag.get(), 4, cudaMemcpyDeviceToHost, s));
+    ctx.finish();
+    if (fl != 0) {  // a float sum value outside the fixed-point range: the general plan
+      free_outputs();
+      return false;
+    }
+    const int64_t ndef = static_cast<int64_t>(cnt[3] & 0xffffffffull);
+    if (ndef > 0) {  // buckets with more groups than the shared records hold
+      std::vector<int32_t> dh(ndef);
+      LDF_CUDA(cudaMemcpyAsync(dh.data(), deferred.get(), ndef * 4, cudaMemcpyDeviceToHost, s));
+      ctx.finish();
+      int64_t rows = 0;
+      for (int32_t q : dh) rows = std::max<int64_t>(rows, hist_h[q]);
+      large_pass(deferred.get(), ndef, rows);
+      LDF_CUDA(cudaMemcpyAsync(cnt, counters.get(), 8, cudaMemcpyDeviceToHost, s));
+      ctx.finish();
+    }
+    const int64_t G = static_cast<int64_t>(cnt[0]);
+    if (G > cap_out) {  // more groups than the estimate allowed for: once more with room for all
+      if (attempt >= 2) fail(LDF_ERR_INTERNAL, "groupby output overflow");
+      free_outputs();
+      cap_out = G;
+      continue;
+    }
+    // outputs of exactly G rows
+    for (int j = 0; j < nkeys + naggs; ++j) {
+      const ldf_column& c = big[j];
+      ldf_column e        = alloc_out_column(al, c.type, G, c.valid != nullptr);
+      const int wdt       = type_width(c.type);
+      if (G > 0) {
+        LDF_CUDA(cudaMemcpyAsync(e.data, c.data, static_cast<size_t>(G) * wdt, cudaMemcpyDeviceToDevice, s));
+        if (c.valid) LDF_CUDA(cudaMemcpyAsync(e.valid, c.valid, static_cast<size_t>(G), cudaMemcpyDeviceToDevice, s));
+      }
+      out[j] = e;
+    }
+    ctx.finish();
+    free_outputs();
+    return true;
+  }
+}
+
 }  // namespace
 
 void groupby_aggregation(const ldf_column* table, int ncols, const int32_t* keys, int nkeys,
@@ -2005,6 +3156,7 @@ void groupby_aggregation(const ldf_column* table, int ncols, const int32_t* keys
     if ((ag.kind == LDF_AGG_MIN || ag.kind == LDF_AGG_MAX) && c.type == LDF_STRING)
       fail(LDF_ERR_UNSUPPORTED, "min/max of a string column is not supported");
   }
+  if (try_partitioned(ctx, p, table, keys, nkeys, aggs, naggs, agg_col, out, hs, col_of_plan)) return;
   switch (key_mode(k)) {
     case KeyMode::K32:
       run_groupby<KeyMode::K32>(ctx, p, table, keys, nkeys, aggs, naggs, agg_col, out, hs, col_of_plan);

@@ -295,3 +295,66 @@ def test_groupby_nunique_with_min_max(vkind, other):
     res = run_groupby(t, ["k"], aggs)
     exp = R.groupby(t, ["k"], aggs)
     assert_tables_equal(res, exp, sort_by=["k"], rtol=RTOL)
+
+
+# ---- partitioned plan (one fixed-width key, <= 2 fixed-width value columns) ----
+PART_AGGS = [
+    ("v", "sum", "s"), ("v", "mean", "m"), ("v", "count", "c"), (None, "count_all", "n"),
+    ("v", "min", "vmin"), ("v", "max", "vmax"),
+    ("v", ("count", pc.CountOptions(mode="all")), "c_all"),
+    ("v", ("count", pc.CountOptions(mode="only_null")), "c_null"),
+    ("i", "min", "mn"), ("i", "max", "mx"), ("i", "count_distinct", "nd"), ("i", "sum", "isum"),
+    ("i", "mean", "imean"), ("i", ("count_distinct", pc.CountOptions(mode="all")), "nd_all"),
+]
+
+
+def _part_table(rng, n, key_kind, ngroups, zipf=None, key_null_p=0.01, i_null_p=0.05, ivals=1000):
+    if zipf:
+        raw = rng.permutation(ngroups)[np.minimum(rng.zipf(zipf, n), ngroups) - 1]
+    else:
+        raw = rng.integers(0, ngroups, n)
+    k = pa.array(raw.astype(key_kind), mask=rng.random(n) < key_null_p if key_null_p else None)
+    v = pa.array(rng.normal(size=n), mask=rng.random(n) < 0.1)
+    i = pa.array(rng.integers(-ivals // 2, ivals, n).astype(np.int32), mask=rng.random(n) < i_null_p)
+    return pa.table({"k": k, "v": v, "i": i})
+
+
+@pytest.mark.parametrize("key_kind,ngroups,zipf,n", [
+    ("int64", 50_000, 1.1, 600_000),     # hot keys in shared memory + cold buckets
+    ("int32", 300_000, None, 500_000),   # mostly cold: many small buckets
+    ("float64", 20_000, 1.3, 400_000),   # float keys by bit pattern
+    ("int8", 200, None, 300_000),        # few groups: large buckets on global scratch
+    ("uint64", 2_000, None, 2_000_000),  # large buckets, hot keys picked among equals
+])
+def test_groupby_partitioned_plan(monkeypatch, key_kind, ngroups, zipf, n):
+    monkeypatch.setenv("LDF_B200_GB_PART_MIN_ROWS", "0")
+    rng = np.random.default_rng(ngroups + n)
+    t = _part_table(rng, n, key_kind, ngroups, zipf=zipf)
+    res = run_groupby(t, ["k"], PART_AGGS)
+    exp = R.groupby(t, ["k"], PART_AGGS)
+    assert_tables_equal(res, exp, sort_by=["k"], rtol=RTOL)
+
+
+def test_groupby_partitioned_single_column_and_edge_keys(monkeypatch):
+    monkeypatch.setenv("LDF_B200_GB_PART_MIN_ROWS", "0")
+    rng = np.random.default_rng(41)
+    n = 400_000
+    raw = rng.integers(0, 5000, n).astype(np.int64)
+    raw[::97] = -1          # all-ones bits (the sample table's empty marker)
+    raw[5::101] = 2**63 - 1
+    t = pa.table({"k": raw, "x": pa.array(rng.integers(-2**40, 2**40, n), mask=rng.random(n) < 0.2)})
+    aggs = [("x", "sum", "s"), ("x", "mean", "m"), ("x", "min", "mn"), ("x", "max", "mx"), (None, "count_all", "n")]
+    assert_tables_equal(run_groupby(t, ["k"], aggs), R.groupby(t, ["k"], aggs), sort_by=["k"], rtol=RTOL)
+
+
+def test_groupby_partitioned_falls_back_on_special_floats(monkeypatch):
+    # NaN / inf / tiny values are outside the exact fixed-point range: the
+    # call re-runs on the general plan, with the same results
+    monkeypatch.setenv("LDF_B200_GB_PART_MIN_ROWS", "0")
+    rng = np.random.default_rng(43)
+    t = _part_table(rng, 200_000, "int64", 3_000, zipf=1.2)
+    v = t.column("v").to_numpy(zero_copy_only=False).copy()
+    v[7], v[11], v[13] = np.nan, np.inf, 1e-300
+    t = t.set_column(1, "v", pa.array(v, mask=np.isnan(v) & (np.arange(len(v)) != 7)))
+    aggs = [("v", "sum", "s"), ("v", "mean", "m"), ("i", "count_distinct", "nd"), (None, "count_all", "n")]
+    assert_tables_equal(run_groupby(t, ["k"], aggs), R.groupby(t, ["k"], aggs), sort_by=["k"], rtol=RTOL)
