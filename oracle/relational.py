@@ -7,6 +7,8 @@ are ``pyarrow`` tables; row order of join / groupby results is unspecified
 
 from __future__ import annotations
 
+import math
+
 import numpy as np
 import pyarrow as pa
 
@@ -153,6 +155,11 @@ def join(lhs: pa.Table, rhs: pa.Table, lhs_keys, rhs_keys, join_type: str, nulls
 # compensated sum per group.
 # ---------------------------------------------------------------------------
 def neumaier(xs) -> float:
+    xs = list(xs)
+    if not all(math.isfinite(x) for x in xs):
+        # inf / NaN: IEEE propagation as in a plain sum (Arrow's sum of
+        # [inf, 1.0] is inf; the compensation term would turn it into NaN)
+        return float(sum(xs))
     s = 0.0
     c = 0.0
     for x in xs:

@@ -174,3 +174,12 @@ def test_oracle_segment_sums_c():
         assert abs(sums[s] - exact) <= 1e-12 * abs(exact) + 1e-300
     s32, c32 = native.segment_sums(x.astype(np.float32), None, off)
     assert abs(s32[0] - math.fsum(x[:off[1]].astype(np.float32).astype(np.float64))) <= 1e-12 * abs(s32[0])
+
+
+def test_oracle_float_sums_with_infinities_vs_arrow():
+    # +inf / -inf / NaN values propagate as in Arrow's hash_sum
+    k = np.array([0, 0, 1, 1, 2, 2, 3, 3, 4], dtype=np.int64)
+    v = np.array([np.inf, 1.0, -np.inf, 2.0, np.inf, -np.inf, np.nan, 1.0, 5.0])
+    t = pa.table({"k": k, "v": v})
+    aggs = [("v", "sum", "s"), ("v", "mean", "m")]
+    assert_tables_equal(R.groupby(t, ["k"], aggs), A.groupby(t, ["k"], aggs), sort_by=["k"])
