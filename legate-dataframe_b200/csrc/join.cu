@@ -93,11 +93,6 @@ struct BuildTable {
   const int32_t* direct;
   int64_t dmin, dmax;
   uint64_t drange;
-  // Keyed: every value of [dmin, dmax] is the key of exactly one build row
-  // (drange == build rows), so a probe key in the range matches without a
-  // lookup and the build side is addressed by key slot u = key - dmin: the
-  // packed build outputs and the FULL join's matched flags are indexed by u.
-  int keyed;
 };
 
 // Slot of key value k in a direct-address table, or drange when k is outside
@@ -234,10 +229,6 @@ __device__ __forceinline__ void for_each_match(const BuildTable& t, const KeyCol
   if (M != KeyMode::GEN && t.direct) {
     const uint64_t u = direct_slot(t, key_value(pk.c[0], r));
     if (u < t.drange) {
-      if (t.keyed) {
-        f(static_cast<int64_t>(u));
-        return;
-      }
       const int32_t br = __ldg(t.direct + u);
       if (br >= 0) f(static_cast<int64_t>(br));
     }
@@ -498,12 +489,7 @@ probe_kernel(ProbeArgs a)
         if (a.t.direct) {
           const uint64_t u = direct_slot(a.t, key_value(a.pk.c[0], r));
           if (u >= a.t.drange) continue;
-          if (a.t.keyed) {
-            if (a.rpack == nullptr) continue;
-            p = a.rpack + u;  // the row's one random access
-          } else {
-            p = a.t.direct + u;
-          }
+          p = a.t.direct + u;
         } else {
           uint64_t lo, hi;
           const uint64_t idx = first_slot(a.t, mix64(key_bits<M>(a.pk, r)), lo, hi);
@@ -612,27 +598,9 @@ __global__ void pack_rows_kernel(DCol c0, DCol c1, int64_t n, ulonglong2* out)
     out[b] = make_ulonglong2(load_w<W0>(c0.data, b), load_w<W1>(c1.data, b));
 }
 
-// The same records at the key slot of each build row (keyed tables).
-template <int W0, int W1>
-__global__ void pack_keyed_kernel(DCol c0, DCol c1, DCol key, int64_t dmin, int64_t n, ulonglong2* out)
-{
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x)
-    out[key_value(key, b) - dmin] = make_ulonglong2(load_w<W0>(c0.data, b), load_w<W1>(c1.data, b));
-}
-
 template <int W0>
-void launch_pack(const DCol& c0, const DCol& c1, int64_t n, ulonglong2* out, cudaStream_t s, unsigned grid,
-                 const DCol* key = nullptr, int64_t dmin = 0)
+void launch_pack(const DCol& c0, const DCol& c1, int64_t n, ulonglong2* out, cudaStream_t s, unsigned grid)
 {
-  if (key) {
-    switch (c1.width) {
-      case 1: launch("pack_rows", pack_keyed_kernel<W0, 1>, grid, 256, 0, s, c0, c1, *key, dmin, n, out); break;
-      case 2: launch("pack_rows", pack_keyed_kernel<W0, 2>, grid, 256, 0, s, c0, c1, *key, dmin, n, out); break;
-      case 4: launch("pack_rows", pack_keyed_kernel<W0, 4>, grid, 256, 0, s, c0, c1, *key, dmin, n, out); break;
-      default: launch("pack_rows", pack_keyed_kernel<W0, 8>, grid, 256, 0, s, c0, c1, *key, dmin, n, out); break;
-    }
-    return;
-  }
   switch (c1.width) {
     case 1: launch("pack_rows", pack_rows_kernel<W0, 1>, grid, 256, 0, s, c0, c1, n, out); break;
     case 2: launch("pack_rows", pack_rows_kernel<W0, 2>, grid, 256, 0, s, c0, c1, n, out); break;
@@ -643,8 +611,7 @@ void launch_pack(const DCol& c0, const DCol& c1, int64_t n, ulonglong2* out, cud
 
 // FULL join tail: rhs rows never matched, appended after the probe rows.
 struct TailArgs {
-  const uint8_t* matched;   // per build row, or per key slot when `rowmap` is set
-  const int32_t* rowmap;    // keyed tables: key slot -> build row
+  const uint8_t* matched;
   int64_t n_build;
   const int64_t* base_pos;  // device: probe output rows
   OutSpec lo, ro;
@@ -680,7 +647,6 @@ __global__ void __launch_bounds__(kProbeThreads) full_tail_kernel(TailArgs a)
   for (int i = 0; i < kProbeItems; ++i) {
     if (!f[i]) continue;
     int64_t r = base + i;
-    if (a.rowmap) r = __ldg(a.rowmap + r);
     write_out_row(a.lo, pos, -1);
     write_out_row(a.ro, pos, r);
     if (a.lmap) a.lmap[pos] = -1;
@@ -1146,22 +1112,15 @@ void run_join(const OpContext& ctx, const KeyCols& pk, int64_t n_probe, const Ke
       const DCol& c1 = ro.src[rest[1]];
       rpack          = Buffer<ulonglong2>(al, n_build);
       const unsigned g = grid_stride_blocks(n_build, 256);
-      // Every key slot of a direct table holding one build row each (and no
-      // null build key): records by key slot, so a matched probe row makes
-      // one random access (the record) instead of two (slot, then record).
-      const bool keyed = t.direct != nullptr && t.drange == static_cast<uint64_t>(n_build) &&
-                         bk.c[0].valid == nullptr;
-      const DCol* kcol = keyed ? &bk.c[0] : nullptr;
       switch (c0.width) {
-        case 1: launch_pack<1>(c0, c1, n_build, rpack.get(), s, g, kcol, t.dmin); break;
-        case 2: launch_pack<2>(c0, c1, n_build, rpack.get(), s, g, kcol, t.dmin); break;
-        case 4: launch_pack<4>(c0, c1, n_build, rpack.get(), s, g, kcol, t.dmin); break;
-        default: launch_pack<8>(c0, c1, n_build, rpack.get(), s, g, kcol, t.dmin); break;
+        case 1: launch_pack<1>(c0, c1, n_build, rpack.get(), s, g); break;
+        case 2: launch_pack<2>(c0, c1, n_build, rpack.get(), s, g); break;
+        case 4: launch_pack<4>(c0, c1, n_build, rpack.get(), s, g); break;
+        default: launch_pack<8>(c0, c1, n_build, rpack.get(), s, g); break;
       }
       a.rpack   = rpack.get();
       a.pcol[0] = rest[0];
       a.pcol[1] = rest[1];
-      a.t.keyed = keyed ? 1 : 0;
     }
   }
 
@@ -1181,7 +1140,6 @@ void run_join(const OpContext& ctx, const KeyCols& pk, int64_t n_probe, const Ke
     const int64_t btiles = ceil_div(n_build, kProbeTile);
     TailArgs ta{};
     ta.matched  = matched.get();
-    ta.rowmap   = a.t.keyed ? t.direct : nullptr;
     ta.n_build  = n_build;
     ta.base_pos = d_total.get();
     ta.lo       = a.lo;

@@ -327,6 +327,7 @@ def _part_table(rng, n, key_kind, ngroups, zipf=None, key_null_p=0.01, i_null_p=
     ("uint64", 2_000, None, 2_000_000),  # large buckets, hot keys picked among equals
 ])
 def test_groupby_partitioned_plan(monkeypatch, key_kind, ngroups, zipf, n):
+    monkeypatch.setenv("LDF_B200_GB_PART", "1")
     monkeypatch.setenv("LDF_B200_GB_PART_MIN_ROWS", "0")
     rng = np.random.default_rng(ngroups + n)
     t = _part_table(rng, n, key_kind, ngroups, zipf=zipf)
@@ -336,6 +337,7 @@ def test_groupby_partitioned_plan(monkeypatch, key_kind, ngroups, zipf, n):
 
 
 def test_groupby_partitioned_single_column_and_edge_keys(monkeypatch):
+    monkeypatch.setenv("LDF_B200_GB_PART", "1")
     monkeypatch.setenv("LDF_B200_GB_PART_MIN_ROWS", "0")
     rng = np.random.default_rng(41)
     n = 400_000
@@ -350,6 +352,7 @@ def test_groupby_partitioned_single_column_and_edge_keys(monkeypatch):
 def test_groupby_partitioned_falls_back_on_special_floats(monkeypatch):
     # NaN / inf / tiny values are outside the exact fixed-point range: the
     # call re-runs on the general plan, with the same results
+    monkeypatch.setenv("LDF_B200_GB_PART", "1")
     monkeypatch.setenv("LDF_B200_GB_PART_MIN_ROWS", "0")
     rng = np.random.default_rng(43)
     t = _part_table(rng, 200_000, "int64", 3_000, zipf=1.2)
