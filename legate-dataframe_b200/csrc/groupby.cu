@@ -1970,10 +1970,10 @@ constexpr int kPartHotMax     = 1024;  // hot keys (the null key takes one more 
 constexpr int kPartHotSlots   = 2048;  // shared hot key table (power of two)
 constexpr uint32_t kPartNoId  = 0xffffffffu;
 constexpr uint32_t kPartBusy  = 0xfffffffeu;
-constexpr int kBucketThreads  = 1024;  // bucket pass
-constexpr int kBucketKeySlots = 2048;  // shared local key table (power of two)
-constexpr int kBucketRecBytes = 128 * 1024;  // shared records, then the pair set
-constexpr int kBucketGroupsMax = 1024;
+constexpr int kBucketThreads  = 512;   // bucket pass (two CTAs per SM)
+constexpr int kBucketKeySlots = 1024;  // shared local key table (power of two)
+constexpr int kBucketRecBytes = 96 * 1024;  // shared records, then the pair set
+constexpr int kBucketGroupsMax = 768;
 
 struct PVal {  // one value column of the partitioned plan
   DCol col;
@@ -2056,35 +2056,62 @@ __device__ __forceinline__ uint64_t part_widen32(uint32_t o32, int type)
   return o32;
 }
 
-__device__ __forceinline__ uint64_t part_load(const DCol& c, int64_t r)
+// Column kinds the routing pass is compiled for: a known kind turns the
+// per-row type dispatch into straight-line code (the generic kind's switches
+// made the kernel outgrow the instruction cache).
+enum : int { PK_GEN = 0, PK_F64 = 1, PK_I32 = 2, PK_NONE = 3 };
+template <int K>
+__device__ __forceinline__ int pk_width(const PVal& c)
 {
-  switch (c.width) {
-    case 1: return __ldg(static_cast<const uint8_t*>(c.data) + r);
-    case 2: return __ldg(static_cast<const uint16_t*>(c.data) + r);
-    case 4: return __ldg(static_cast<const uint32_t*>(c.data) + r);
-    default: return __ldg(static_cast<const unsigned long long*>(c.data) + r);
+  return K == PK_F64 ? 8 : K == PK_I32 ? 4 : c.col.width;
+}
+template <int K>
+__device__ __forceinline__ int pk_type(const PVal& c)
+{
+  return K == PK_F64 ? LDF_FLOAT64 : K == PK_I32 ? LDF_INT32 : c.col.type;
+}
+
+__device__ __forceinline__ uint64_t load_width(const void* data, int w, int64_t r)
+{
+  switch (w) {
+    case 1: return __ldg(static_cast<const uint8_t*>(data) + r);
+    case 2: return __ldg(static_cast<const uint16_t*>(data) + r);
+    case 4: return __ldg(static_cast<const uint32_t*>(data) + r);
+    default: return __ldg(static_cast<const unsigned long long*>(data) + r);
   }
+}
+__device__ __forceinline__ uint64_t part_load(const DCol& c, int64_t r) { return load_width(c.data, c.width, r); }
+template <int K>
+__device__ __forceinline__ uint64_t part_load_k(const PVal& c, int64_t r)
+{
+  return load_width(c.col.data, pk_width<K>(c), r);
 }
 
 // Add one valid value of column `c` into a 32-bit record (shared memory or
 // per-CTA global scratch; generic addresses).  Returns false for a float sum
 // value outside the fixed-point range.
+template <int K = PK_GEN>
 __device__ __forceinline__ bool part_add(const PVal& c, unsigned char* rec, uint64_t raw)
 {
-  bool ok = true;
+  const int W      = pk_width<K>(c);
+  const int T      = pk_type<K>(c);
+  const bool fixed = K == PK_F64 ? true : K == PK_I32 ? false : c.fixed != 0;
+  const bool mm64  = K == PK_F64 ? true : K == PK_I32 ? false : c.mm64 != 0;
+  const int chunks = K == PK_F64 ? kSumChunks : K == PK_I32 ? 2 : c.chunks;
+  bool ok          = true;
   if (c.nullable) atomicAdd(reinterpret_cast<uint32_t*>(rec + c.b_vc), 1u);
   if (c.states & ST_SUM) {
     uint32_t* sum = reinterpret_cast<uint32_t*>(rec + c.b_sum);
-    if (c.fixed) {
-      const double x = c.col.width == 8 ? __longlong_as_double(static_cast<long long>(raw))
-                                        : static_cast<double>(__uint_as_float(static_cast<uint32_t>(raw)));
+    if (fixed) {
+      const double x = W == 8 ? __longlong_as_double(static_cast<long long>(raw))
+                              : static_cast<double>(__uint_as_float(static_cast<uint32_t>(raw)));
       uint64_t m;
       int sh;
       bool neg;
       if (fixed_parts(x, m, sh, neg)) {
         if (m) {
           const int j0 = sh >> 5, b = sh & 31;
-          sh_add_magnitude(sum, c.chunks, j0, m << b, b ? (m >> (64 - b)) : 0, neg);
+          sh_add_magnitude(sum, chunks, j0, m << b, b ? (m >> (64 - b)) : 0, neg);
         }
       } else {
         ok = false;
@@ -2092,22 +2119,22 @@ __device__ __forceinline__ bool part_add(const PVal& c, unsigned char* rec, uint
     } else {
       uint64_t mag = raw;
       bool neg     = false;
-      if (is_signed_int_dev(c.col.type)) {
-        const int64_t v = c.col.width == 1 ? static_cast<int8_t>(raw) : c.col.width == 2 ? static_cast<int16_t>(raw)
-                        : c.col.width == 4 ? static_cast<int32_t>(raw) : static_cast<int64_t>(raw);
+      if (is_signed_int_dev(T)) {
+        const int64_t v = W == 1 ? static_cast<int8_t>(raw) : W == 2 ? static_cast<int16_t>(raw)
+                        : W == 4 ? static_cast<int32_t>(raw) : static_cast<int64_t>(raw);
         neg = v < 0;
         mag = neg ? (0ull - static_cast<uint64_t>(v)) : static_cast<uint64_t>(v);
       }
-      sh_add_magnitude(sum, c.chunks, 0, mag, 0, neg);
+      sh_add_magnitude(sum, chunks, 0, mag, 0, neg);
     }
   }
   if (c.states & (ST_MIN | ST_MAX)) {
-    if (c.mm64) {
-      const uint64_t o = part_ord64(raw, c.col.type);
+    if (mm64) {
+      const uint64_t o = part_ord64(raw, T);
       if (c.states & ST_MIN) atomicMax(reinterpret_cast<unsigned long long*>(rec + c.b_mn), ~o);
       if (c.states & ST_MAX) atomicMax(reinterpret_cast<unsigned long long*>(rec + c.b_mx), o);
     } else {
-      const uint32_t o = part_ord32(raw, c.col.type);
+      const uint32_t o = part_ord32(raw, T);
       if (c.states & ST_MIN) atomicMax(reinterpret_cast<uint32_t*>(rec + c.b_mn), ~o);
       if (c.states & ST_MAX) atomicMax(reinterpret_cast<uint32_t*>(rec + c.b_mx), o);
     }
@@ -2318,8 +2345,11 @@ __global__ void __launch_bounds__(kCountThreads, 1) part_count_kernel(PartArgs a
 }
 
 // ---- routing pass -----------------------------------------------------------
+template <int K0, int K1>
 __global__ void __launch_bounds__(kPartThreads) part_route_kernel(PartArgs a)
 {
+  // the second value column: none, or its kind (generic: decided at run time)
+  const bool two = K1 == PK_NONE ? false : (K1 == PK_GEN ? a.ncol > 1 : true);
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* ids            = reinterpret_cast<uint32_t*>(smem);
   unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem + kPartHotSlots * 4);
@@ -2347,10 +2377,10 @@ __global__ void __launch_bounds__(kPartThreads) part_route_kernel(PartArgs a)
           fl[j] |= 2;
           kb[j] = part_load(a.key, r);
         }
-        v0[j] = part_load(a.c[0].col, r);
+        v0[j] = part_load_k<K0>(a.c[0], r);
         if (dvalid(a.c[0].col, r)) fl[j] |= 4;
-        if (a.ncol > 1) {
-          v1[j] = part_load(a.c[1].col, r);
+        if (two) {
+          v1[j] = part_load_k<K1>(a.c[1], r);
           if (dvalid(a.c[1].col, r)) fl[j] |= 8;
         }
       }
@@ -2363,8 +2393,8 @@ __global__ void __launch_bounds__(kPartThreads) part_route_kernel(PartArgs a)
       if (hid != kPartNoId) {
         unsigned char* rec = recs + static_cast<int64_t>(hid) * a.rb;
         atomicAdd(reinterpret_cast<uint32_t*>(rec + 8), 1u);
-        if (fl[j] & 4) range_ok &= part_add(a.c[0], rec, v0[j]);
-        if (a.ncol > 1 && (fl[j] & 8)) range_ok &= part_add(a.c[1], rec, v1[j]);
+        if (fl[j] & 4) range_ok &= part_add<K0>(a.c[0], rec, v0[j]);
+        if (two && (fl[j] & 8)) range_ok &= part_add<K1 == PK_NONE ? PK_GEN : K1>(a.c[1], rec, v1[j]);
         if (a.nd >= 0 && (fl[j] & (a.nd == 0 ? 4 : 8))) {
           const uint32_t off = (static_cast<uint32_t>(a.nd == 0 ? v0[j] : v1[j]) ^ a.vflip) - a.vbase;
           red_or32(a.bits + static_cast<uint64_t>(hid) * a.wpr + (off >> 5), 1u << (off & 31));
@@ -2372,15 +2402,17 @@ __global__ void __launch_bounds__(kPartThreads) part_route_kernel(PartArgs a)
       } else {
         // a cold row: the validity bits ride in the top of the third word
         // (value 1 is at most 4 bytes)
-        if (a.c[0].fixed && (a.c[0].states & ST_SUM) && (fl[j] & 4)) {
-          const double x = a.c[0].col.width == 8 ? __longlong_as_double(static_cast<long long>(v0[j]))
+        const bool fixed0 = K0 == PK_F64 ? true : K0 == PK_I32 ? false : a.c[0].fixed != 0;
+        const bool fixed1 = K1 == PK_F64 ? true : (K1 == PK_I32 || K1 == PK_NONE) ? false : a.c[1].fixed != 0;
+        if (fixed0 && (a.c[0].states & ST_SUM) && (fl[j] & 4)) {
+          const double x = pk_width<K0>(a.c[0]) == 8 ? __longlong_as_double(static_cast<long long>(v0[j]))
                                                  : static_cast<double>(__uint_as_float(static_cast<uint32_t>(v0[j])));
           uint64_t m;
           int sh;
           bool neg;
           range_ok &= fixed_parts(x, m, sh, neg);
         }
-        if (a.ncol > 1 && a.c[1].fixed && (a.c[1].states & ST_SUM) && (fl[j] & 8)) {
+        if (two && fixed1 && (a.c[1].states & ST_SUM) && (fl[j] & 8)) {
           const double x = static_cast<double>(__uint_as_float(static_cast<uint32_t>(v1[j])));
           uint64_t m;
           int sh;
@@ -2504,6 +2536,7 @@ struct BucketArgs {
   int32_t* deferred;           // shared-memory pass: buckets that did not fit
   unsigned int* ndeferred;
   int64_t small_rows;          // shared-memory pass: buckets above this many rows are skipped
+  int pair32;                  // NUNIQUE pairs as 32-bit words (local id < 4096, value offset < 2^20)
   // large pass: per-CTA global work memory
   unsigned char* scratch;
   int64_t scratch_stride;
@@ -2602,8 +2635,13 @@ __device__ bool process_bucket(const BucketArgs& B, const BucketMem& m, int64_t 
   }
   // NUNIQUE: (local id, value) pairs of the valid rows, counted when new
   __syncthreads();
-  const int64_t ps = m.ps < 2 * rows + 64 ? m.ps : 2 * rows + 64;
-  for (int64_t i = threadIdx.x; i < ps; i += blockDim.x) m.pairs[i] = kEmpty;
+  const int64_t cap = B.pair32 ? 2 * m.ps : m.ps;  // slots of the pair set
+  const int64_t ps  = cap < 2 * rows + 64 ? cap : 2 * rows + 64;
+  uint32_t* pairs32 = reinterpret_cast<uint32_t*>(m.pairs);
+  if (B.pair32)
+    for (int64_t i = threadIdx.x; i < ps; i += blockDim.x) pairs32[i] = kPartNoId;
+  else
+    for (int64_t i = threadIdx.x; i < ps; i += blockDim.x) m.pairs[i] = kEmpty;
   __syncthreads();
   const uint64_t vbit = a.nd == 0 ? (1ull << 32) : (2ull << 32);
   for (int64_t i = threadIdx.x; i < rows; i += blockDim.x) {
@@ -2614,6 +2652,20 @@ __device__ bool process_bucket(const BucketArgs& B, const BucketMem& m, int64_t 
     bool fresh;
     const uint32_t lid = local_id(m, sh_nlocal, kb, mix64(kb), B.err, &fresh);  // present: a pure lookup
     if (lid >= ng) continue;  // only after an expired wait (reported through B.err)
+    if (B.pair32) {
+      const uint32_t e32 = (lid << 20) | ((x ^ a.vflip) - a.vbase);
+      uint64_t idx       = fastrange(mix64(e32), static_cast<uint64_t>(ps));
+      for (int64_t probe = 0; probe < ps; ++probe) {
+        const uint32_t cur = atomicCAS(pairs32 + idx, kPartNoId, e32);
+        if (cur == kPartNoId) {
+          atomicAdd(m.nd + lid, 1u);
+          break;
+        }
+        if (cur == e32) break;
+        idx = idx + 1 == static_cast<uint64_t>(ps) ? 0 : idx + 1;
+      }
+      continue;
+    }
     const uint64_t e   = (static_cast<uint64_t>(lid) << 32) | x;
     uint64_t idx       = fastrange(mix64(e), static_cast<uint64_t>(ps));
     for (int64_t probe = 0; probe < ps; ++probe) {
@@ -2636,7 +2688,7 @@ __device__ bool process_bucket(const BucketArgs& B, const BucketMem& m, int64_t 
 // Shared-memory bucket pass: persistent CTAs take buckets in order; a bucket
 // above `small_rows` rows is left to the large pass, one with more groups
 // than the shared records hold is deferred to it.
-__global__ void __launch_bounds__(kBucketThreads, 1) part_bucket_kernel(BucketArgs B)
+__global__ void __launch_bounds__(kBucketThreads, 2) part_bucket_kernel(BucketArgs B)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint32_t s_nlocal;
@@ -2769,8 +2821,10 @@ bool try_partitioned(const OpContext& ctx, const GbPlan& p, const ldf_column* ta
                      const HostStaging& hs, const std::vector<int>& col_of_plan)
 {
   // Opt-in (LDF_B200_GB_PART=1): on the 200M-row Zipf(1.1) workload this
-  // plan measured slower than the general one (route pass 9.0 ms, bucket
-  // passes 3.6 + 4.8 ms against 14.2 ms for the whole general plan).
+  // plan measured slower than the general one (21.8 ms a call: routing pass
+  // 6.0 ms, bucket passes 4.5 + 1.7 ms, counting pass 1.0 ms, against 13.5 ms
+  // for the whole general plan).  The shared-memory atomics of the hot rows
+  // are the same work as the general plan's column passes.
   const char* on = std::getenv("LDF_B200_GB_PART");
   if (on == nullptr || std::atoi(on) == 0) return false;
   int64_t min_rows = int64_t(1) << 22;
@@ -2919,7 +2973,9 @@ bool try_partitioned(const OpContext& ctx, const GbPlan& p, const ldf_column* ta
   a.hot_keys = hot_keys.get();
   // buckets: about 200 groups each
   int logP = 0;
-  while (logP < 15 && (int64_t(200) << logP) < est_groups) ++logP;
+  // (the sampled estimate undercounts a heavy-tailed key distribution: 2.2M
+  // for the 6.7M groups of Zipf(1.1) over 10M keys at 200M rows)
+  while (logP < 15 && (int64_t(200) << logP) < 3 * est_groups) ++logP;
   a.logP          = logP;
   const int64_t P = int64_t(1) << logP;
 
@@ -2944,7 +3000,10 @@ bool try_partitioned(const OpContext& ctx, const GbPlan& p, const ldf_column* ta
     cold += hist_h[q];
   }
   bstart_h[P] = cold;
-  const int64_t small_rows = kBucketRecBytes / 8 / 2 - 64;
+  // 32-bit NUNIQUE pairs (local id << 20 | value offset) when the values
+  // span at most 2^20: twice the rows fit the shared pair set
+  const bool pair32        = nd >= 0 && a.wpr <= (1u << 20) / 32;
+  const int64_t small_rows = kBucketRecBytes / (pair32 ? 4 : 8) / 2 - 64;
   std::vector<int32_t> large_h;
   int64_t large_max = 0;
   for (int64_t q = 0; q < P; ++q)
@@ -2976,10 +3035,16 @@ bool try_partitioned(const OpContext& ctx, const GbPlan& p, const ldf_column* ta
   a.flag    = flag.get();
   for (int q = 0; q < a.ncol; ++q) hs.wait(col_of_plan[order[q]]);
   const size_t route_smem = kPartHotSlots * 12 + static_cast<size_t>(a.H + 1) * a.rb;
-  LDF_CUDA(cudaFuncSetAttribute(part_route_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(route_smem)));
-  LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, part_route_kernel, kPartThreads, route_smem));
-  launch("part_route", part_route_kernel,
+  auto kind = [&](int q) {
+    return a.c[q].col.type == LDF_FLOAT64 ? PK_F64 : a.c[q].col.type == LDF_INT32 ? PK_I32 : PK_GEN;
+  };
+  const int k0 = kind(0), k1 = a.ncol > 1 ? kind(1) : PK_NONE;
+  auto route = k0 == PK_F64 && k1 == PK_I32    ? part_route_kernel<PK_F64, PK_I32>
+               : k0 == PK_F64 && k1 == PK_NONE ? part_route_kernel<PK_F64, PK_NONE>
+                                               : part_route_kernel<PK_GEN, PK_GEN>;
+  LDF_CUDA(cudaFuncSetAttribute(route, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(route_smem)));
+  LDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, route, kPartThreads, route_smem));
+  launch("part_route", route,
          static_cast<unsigned>(std::min<int64_t>(std::max(occ, 1) * nsm, ceil_div(n, int64_t(kPartThreads) * kRows))),
          kPartThreads, route_smem, s, a);
 
@@ -3013,6 +3078,7 @@ bool try_partitioned(const OpContext& ctx, const GbPlan& p, const ldf_column* ta
   B.a          = a;
   B.out_count  = counters.get();
   B.small_rows = small_rows;
+  B.pair32     = pair32 ? 1 : 0;
   B.err        = ctx.err();
   B.deferred   = deferred.get();
   B.ndeferred  = reinterpret_cast<unsigned int*>(counters.get() + 3);
@@ -3042,6 +3108,7 @@ bool try_partitioned(const OpContext& ctx, const GbPlan& p, const ldf_column* ta
     L.ks             = ks;
     L.gc             = static_cast<int>(gc);
     L.ps             = ps;
+    L.pair32         = 0;  // local ids may pass 4096 here
     LDF_CUDA(cudaMemsetAsync(counters.get() + 2, 0, 8, s));
     launch("part_bucket_large", part_bucket_large_kernel, static_cast<unsigned>(grid), kBucketThreads, 0, s, L);
   };
@@ -3051,7 +3118,7 @@ bool try_partitioned(const OpContext& ctx, const GbPlan& p, const ldf_column* ta
     B.out_cap = cap_out;
     B.next    = counters.get() + 1;
     LDF_CUDA(cudaMemsetAsync(counters.get(), 0, 32, s));
-    launch("part_bucket", part_bucket_kernel, static_cast<unsigned>(nsm), kBucketThreads, bucket_smem, s, B);
+    launch("part_bucket", part_bucket_kernel, static_cast<unsigned>(2 * nsm), kBucketThreads, bucket_smem, s, B);
     large_pass(large.get(), static_cast<int64_t>(large_h.size()), large_max);
     launch("part_hot_emit", part_hot_emit_kernel, static_cast<unsigned>(std::min(a.H + 1, 4 * nsm)), 256, 0, s, a,
            o, counters.get(), cap_out);

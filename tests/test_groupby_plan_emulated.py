@@ -50,10 +50,12 @@ def _section(small: bool) -> str:
     sec = src[start:end]
     sec = sec.replace("extern __shared__ __align__(16) unsigned char smem[];", "unsigned char* smem = emu_smem;")
     sec = re.sub(r"__shared__ ", "static ", sec)
-    if small:  # a bucket pass that holds 64 groups / 448 rows in shared memory
-        sec = sec.replace("kBucketRecBytes = 128 * 1024;", "kBucketRecBytes = 8 * 1024;")
-        sec = sec.replace("kBucketKeySlots = 2048;", "kBucketKeySlots = 128;")
-        sec = sec.replace("kBucketGroupsMax = 1024;", "kBucketGroupsMax = 64;")
+    if small:  # a bucket pass that holds 64 groups / ~1,000 rows in shared memory
+        for old, new in (("kBucketRecBytes = 96 * 1024;", "kBucketRecBytes = 8 * 1024;"),
+                         ("kBucketKeySlots = 1024;", "kBucketKeySlots = 128;"),
+                         ("kBucketGroupsMax = 768;", "kBucketGroupsMax = 64;")):
+            assert old in sec, old
+            sec = sec.replace(old, new)
     return helpers + sec
 
 
