@@ -55,6 +55,8 @@ constexpr int kMaxAggCols = 8;
 constexpr int kMaxAggs    = 32;
 constexpr int kMaxProbe   = 1024;
 constexpr int kGbThreads  = 512;
+// inputs of at most this many rows keep their assign-pass ids as ranks
+constexpr int64_t kSmallPlanRows = int64_t(1) << 18;
 constexpr uint64_t kEmpty = ~0ull;
 // Empty marker of the 8-byte key table; a key equal to it is the group with
 // the reserved id kIdSentinel, a null single key the group kIdNull.
@@ -1200,6 +1202,13 @@ __global__ void fill_kernel(T* p, int64_t n, T v)
     p[i] = v;
 }
 
+// p[i] = i (ranks of a small input: its assign-pass ids)
+__global__ void iota_kernel(int32_t* p, int64_t n)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = static_cast<int32_t>(i);
+}
+
 // ---- frequency ranks --------------------------------------------------------
 // key = ~count: an ascending stable sort puts the most frequent ids first and
 // unused ids (holes, count 0) last.
@@ -1576,6 +1585,14 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
   // per-rank segments for the less frequent ranks (LDF_B200_ND_SEGMENTS=0 keeps them in the pair set)
   bool seg_enabled = true;
   if (const char* e = std::getenv("LDF_B200_ND_SEGMENTS")) seg_enabled = std::atoi(e) != 0;
+  // Small inputs skip the frequency ranking (ranks = assign-pass ids), so
+  // NUNIQUE cannot use the rank-ordered bitmap and segment tiers: every
+  // (group, value) pair goes to the pair set.
+  const bool small = n <= kSmallPlanRows;
+  if (small) {
+    bitmap_budget = 0;
+    seg_enabled   = false;
+  }
 
   for (int attempt = 0;; ++attempt) {
     const uint64_t id_cap = cap + kIdFirst;
@@ -1657,12 +1674,18 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
       // the id counter may pass id_cap (pool refills are clipped to it)
       nid = static_cast<int64_t>(std::min<unsigned long long>(hm[0], id_cap));
 
-      // frequency ranks: sort ids by descending row count (stable radix sort)
-      Buffer<uint32_t> rkey(al, nid);
-      launch("rank_keys", rank_keys_kernel, gs_blocks(nid, 256), 256, 0, s,
-             static_cast<const unsigned long long*>(counts.get()), nid, rkey.get());
+      // frequency ranks: sort ids by descending row count (stable radix
+      // sort).  Small inputs keep the assign-pass ids as ranks: the ranking
+      // only decides which groups get shared-memory records, which matters
+      // for heavy hitters in large inputs, while its passes and read-back
+      // cost more than they save here.
       perm = Buffer<int32_t>(al, nid);
-      {
+      if (small) {
+        launch("iota", iota_kernel, gs_blocks(nid, 256), 256, 0, s, perm.get(), nid);
+      } else {
+        Buffer<uint32_t> rkey(al, nid);
+        launch("rank_keys", rank_keys_kernel, gs_blocks(nid, 256), 256, 0, s,
+               static_cast<const unsigned long long*>(counts.get()), nid, rkey.get());
         DCol kc{};
         kc.data  = rkey.get();
         kc.type  = LDF_UINT32;
@@ -1885,9 +1908,11 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
         for (int ci : pass_order)
           if (p.c[ci].states & ST_NDIST) nunique_pass(ci);
       }
-      LDF_CUDA(cudaMemcpyAsync(hm, misc.get(), 16, cudaMemcpyDeviceToHost, s));
-      ctx.finish();
-      if (static_cast<int>(hm[1]) != 0) {  // the pair set overflowed
+      if (ndist_col >= 0) {  // only pair-set inserts can overflow after the assign pass
+        LDF_CUDA(cudaMemcpyAsync(hm, misc.get(), 16, cudaMemcpyDeviceToHost, s));
+        ctx.finish();
+      }
+      if (ndist_col >= 0 && static_cast<int>(hm[1]) != 0) {  // the pair set overflowed
         if (attempt >= 4) fail(LDF_ERR_INTERNAL, "groupby hash table overflow");
         cap      = cap * 4;
         pair_cap = pair_cap * 4;
