@@ -1,10 +1,11 @@
 // Onesweep LSD radix sort (Adinets & Merrill, "Onesweep", 2022) of row ids by
 // 8-bit digits, stable.  One upfront kernel builds the digit histograms of all
 // passes from the unpermuted columns (histograms do not depend on order); each
-// pass is then ONE kernel: tile load -> warp-level stable ranking with
-// __match_any_sync -> per-digit decoupled look-back across tiles -> tile staged
-// in shared memory in digit order -> coalesced runs written out.  Passes whose
-// digit is constant over all rows are skipped from the histograms.
+// pass is then ONE kernel: tile load -> warp-level stable ranking (peer lanes
+// from one ballot per digit bit) -> per-digit decoupled look-back across
+// tiles -> tile staged in shared memory in digit order -> coalesced runs
+// written out.  Passes whose digit is constant over all rows are skipped from
+// the histograms.
 #include "radix.cuh"
 
 namespace ldf {
@@ -299,10 +300,25 @@ constexpr int kLookback = 8;
 struct OsShared {
   uint32_t whist[RW][256];  // per-warp digit counts, then per-warp digit prefixes
   uint32_t tile_start[256];  // tile-local start of each digit
-  uint64_t gbase[256];       // global position of each digit's first row of the tile
+  int32_t delta[256];        // output position of staged row j of digit d: delta[d] + j
   uint32_t scan[RW + 1];
   int64_t tile[2];
 };
+
+// Lanes of the warp whose digit equals this lane's (d <= 256; 256 marks an
+// item without a row): one ballot per digit bit, each lane keeping the lanes
+// that agree with it on that bit.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d)
+{
+  uint32_t peers = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const uint32_t bit = (d >> b) & 1u;
+    const uint32_t set = __ballot_sync(0xffffffffu, bit);
+    peers &= bit ? set : ~set;
+  }
+  return peers;
+}
 
 // Everything of one pass over one tile after its rows are in registers:
 // key[i] / val[i] / dr[i] (digit, 256 = no row) of item i of this thread,
@@ -322,7 +338,7 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
 #pragma unroll
   for (int i = 0; i < RI; ++i) {
     const uint32_t d     = dr[i];
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t peers = digit_peers(d);
     const uint32_t rank  = __popc(peers & lt_mask);
     uint32_t base        = 0;
     if (d < 256) base = sh.whist[warp][d];
@@ -398,15 +414,15 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
       }
       st_release_u64(&st[tile * 256 + t], kFlagPrefix | (excl + run));
     }
-    sh.gbase[t] = a.digit_base[t] + excl;
+    // positions fit 32 bits (fewer than 2^31 rows)
+    sh.delta[t] = static_cast<int32_t>(a.digit_base[t] + excl) - static_cast<int32_t>(start);
   }
   __syncthreads();
   const int64_t tbase = tile * RTILE;
   const int cnt       = static_cast<int>(a.n - tbase < RTILE ? a.n - tbase : RTILE);
   if constexpr (!MOVE) {
     for (int j = threadIdx.x; j < cnt; j += RT) {
-      const uint32_t d  = s_dig[j];
-      const int64_t pos = static_cast<int64_t>(sh.gbase[d]) + (j - static_cast<int64_t>(sh.tile_start[d]));
+      const int32_t pos = sh.delta[s_dig[j]] + j;
       if (WRITE_KEYS) a.keys_out[pos] = s_keys[j];
       a.vals_out[pos] = s_vals[j];
       if (a.inv_out) a.inv_out[s_vals[j]] = static_cast<int32_t>(pos);
@@ -423,8 +439,7 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
         pos[k]      = -1;
         row[k]      = 0;
         if (j < cnt) {
-          const uint32_t d = s_dig[j];
-          pos[k]           = static_cast<int32_t>(sh.gbase[d] + static_cast<uint32_t>(j) - sh.tile_start[d]);
+          pos[k]           = sh.delta[s_dig[j]] + j;
           row[k]           = s_vals[j];
           a.vals_out[pos[k]] = row[k];
           if (a.inv_out) a.inv_out[row[k]] = pos[k];
@@ -497,7 +512,10 @@ void launch_onesweep(cudaStream_t s, unsigned tiles, const PassArgs& a)
   constexpr size_t smem = onesweep_smem(WRITE_KEYS);
   LDF_CUDA(cudaFuncSetAttribute(onesweep_kernel<GATHER, WRITE_KEYS, MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
-  launch("onesweep", onesweep_kernel<GATHER, WRITE_KEYS, MOVE>, tiles, RT, smem, s, a);
+  // profile names: a pass that loads its word from the columns, one that
+  // moves the payload columns, the others
+  const char* name = MOVE ? "onesweep_move" : (GATHER ? "onesweep_gather" : "onesweep");
+  launch(name, onesweep_kernel<GATHER, WRITE_KEYS, MOVE>, tiles, RT, smem, s, a);
 }
 
 // Identity order: the payload columns copied as they are.

@@ -240,39 +240,47 @@ __device__ __forceinline__ uint64_t warp_lookback(uint64_t* status, int64_t tile
   return excl;
 }
 
+// One tile per block.  The tile is loaded coalesced into shared memory, where
+// thread t then owns kScanItems consecutive elements (runs padded by one word
+// so that neither the coalesced nor the per-thread accesses conflict on
+// banks): a serial sum per thread, one warp scan of the thread sums, the
+// block's warp totals and the look-back in warp 0, then the per-thread runs
+// written back to shared memory and stored coalesced.
 template <typename TIn>
 __global__ void __launch_bounds__(kScanThreads)
   scan_kernel(const TIn* in, int64_t* out, int64_t n, uint64_t* status,
               unsigned long long* counter, int64_t* total, int* err, uint32_t spin_limit)
 {
+  constexpr int kPad = kScanItems + 1;
+  __shared__ int64_t s_x[kScanThreads * kPad];
   __shared__ int64_t s_warp[kScanWarps + 1];
   __shared__ int64_t s_tile;
   __shared__ uint64_t s_prefix;
   const int64_t tile  = next_tile_id(counter, &s_tile);
   const int warp      = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t wbase = tile * kScanTile + static_cast<int64_t>(warp) * (32 * kScanItems);
+  const int64_t tbase = tile * kScanTile;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int e     = i * kScanThreads + threadIdx.x;
+    const int64_t r = tbase + e;
+    s_x[(e / kScanItems) * kPad + e % kScanItems] = r < n ? static_cast<int64_t>(in[r]) : 0;
+  }
+  __syncthreads();
   int64_t v[kScanItems];
+  int64_t sum = 0;
 #pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    const int64_t r = wbase + i * 32 + lane;
-    v[i]            = r < n ? static_cast<int64_t>(in[r]) : 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = s_x[threadIdx.x * kPad + k];
+    sum += v[k];
   }
-  // exclusive scan of the warp's segment, (i, lane) order
-  int64_t carry = 0;
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    const int64_t x   = v[i];
-    const int64_t inc = warp_inclusive_scan(x);
-    v[i]              = carry + inc - x;
-    carry += __shfl_sync(0xffffffffu, inc, 31);
-  }
-  if (lane == 0) s_warp[warp] = carry;
+  const int64_t inc = warp_inclusive_scan(sum);
+  if (lane == 31) s_warp[warp] = inc;
   __syncthreads();
   if (warp == 0) {
-    const int64_t w   = lane < kScanWarps ? s_warp[lane] : 0;
-    const int64_t inc = warp_inclusive_scan(w);
-    if (lane < kScanWarps) s_warp[lane] = inc - w;
-    const int64_t tile_total = __shfl_sync(0xffffffffu, inc, kScanWarps - 1);
+    const int64_t w    = lane < kScanWarps ? s_warp[lane] : 0;
+    const int64_t winc = warp_inclusive_scan(w);
+    if (lane < kScanWarps) s_warp[lane] = winc - w;
+    const int64_t tile_total = __shfl_sync(0xffffffffu, winc, kScanWarps - 1);
     const uint64_t excl = warp_lookback(status, tile, static_cast<uint64_t>(tile_total), err, spin_limit);
     if (lane == 0) {
       s_prefix = excl;
@@ -280,11 +288,18 @@ __global__ void __launch_bounds__(kScanThreads)
     }
   }
   __syncthreads();
-  const int64_t off = static_cast<int64_t>(s_prefix) + s_warp[warp];
+  int64_t run = static_cast<int64_t>(s_prefix) + s_warp[warp] + inc - sum;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    s_x[threadIdx.x * kPad + k] = run;
+    run += v[k];
+  }
+  __syncthreads();
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    const int64_t r = wbase + i * 32 + lane;
-    if (r < n) out[r] = off + v[i];
+    const int e     = i * kScanThreads + threadIdx.x;
+    const int64_t r = tbase + e;
+    if (r < n) out[r] = s_x[(e / kScanItems) * kPad + e % kScanItems];
   }
 }
 

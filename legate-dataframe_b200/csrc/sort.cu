@@ -52,6 +52,9 @@ __global__ void str_find_insert_kernel(DCol col, int64_t n, int64_t stride, unsi
     uint64_t idx         = fastrange(h, cap);
     int64_t found        = -1;
     for (int probe = 0; probe < 4096; ++probe) {
+      // a long probe sequence means a full table: stop once any row has
+      // reported the overflow (the pass is redone with a larger table)
+      if ((probe & 31) == 31 && *static_cast<volatile int*>(overflow)) break;
       uint64_t v = slots[idx];
       if (v == kEmpty) {
         v = atomicCAS(&slots[idx], kEmpty, entry);
@@ -243,9 +246,11 @@ void string_ranks(const OpContext& ctx, const DCol& col, int64_t n, uint32_t* ou
   cudaStream_t s      = ctx.stream();
   if (n == 0) return;
   // Dedupe table size from a strided sample of 2^20 rows: distinct strings
-  // estimated by GEE (Charikar et al. 2000), taken x8 because it
-  // underestimates heavy tails; a table too small for the real count
-  // overflows and the pass is redone with room for every row.
+  // estimated by GEE (Charikar et al. 2000), room for twice the estimate at
+  // a load of one half (a table that stays in L2 for a dictionary of a few
+  // million strings).  GEE can underestimate heavy tails; a table too small
+  // for the real count overflows (inserts stop at the first full probe
+  // window) and the pass is redone with room for every row.
   uint64_t cap          = static_cast<uint64_t>(2 * n + 64);
   const int64_t kSample = int64_t(1) << 20;
   if (n > 4 * kSample) {
@@ -270,7 +275,7 @@ void string_ranks(const OpContext& ctx, const DCol& col, int64_t n, uint32_t* ou
     if (h[2] == 0) {
       const double est = std::sqrt(static_cast<double>(n) / kSample) * static_cast<double>(h[1]) +
                          static_cast<double>(h[0] - h[1]);
-      const int64_t groups = std::min<int64_t>(n, static_cast<int64_t>(8 * est) + 1024);
+      const int64_t groups = std::min<int64_t>(n, static_cast<int64_t>(2 * est) + 1024);
       cap                  = static_cast<uint64_t>(2 * groups + 64);
     }
   }

@@ -134,6 +134,24 @@ def test_sort_strings_sampled_dictionary():
     assert np.all(rows[1:][same] > rows[:-1][same])
 
 
+def test_sort_strings_dictionary_overflow_redo():
+    """20M distinct strings: every string of the sample is seen once, so the
+    sampled estimate (about 4.6M) is too low, the first dedupe table
+    overflows (inserts stop early) and the ranking is redone with room for
+    every row."""
+    n = 20_000_000
+    perm = np.random.default_rng(13).permutation(n)
+    digits = np.stack([(perm // 10 ** (7 - d)) % 10 + 48 for d in range(8)], axis=1).astype(np.uint8)
+    offsets = np.arange(0, 8 * n + 1, 8, dtype=np.int32)
+    keys = pa.StringArray.from_buffers(n, pa.py_buffer(offsets), pa.py_buffer(digits.tobytes()))
+    t = pa.table({"k": keys, "row": np.arange(n)})
+    res = run_sort(t, ["k"])
+    assert np.array_equal(res.column("row").to_numpy(), np.argsort(perm))
+    out = res.column("k").combine_chunks()
+    assert out.slice(0, 3).to_pylist() == ["00000000", "00000001", "00000002"]
+    assert out[n - 1].as_py() == f"{n - 1:08d}"
+
+
 def test_sort_wide_table_moved_and_gathered_columns():
     """A whole-table sort moves the first four columns inside its last radix
     pass (fixed widths straight into the outputs, a string column's ranges
