@@ -73,6 +73,26 @@ __device__ __forceinline__ void store_w(void* data, int64_t i, uint64_t v)
   else static_cast<unsigned long long*>(data)[i] = v;
 }
 
+// Streaming (evict-first) forms for the probe side and the output rows, which
+// are touched once: they then leave L2 before the build-side table and
+// payload records that the probe rows hit repeatedly.
+template <int W>
+__device__ __forceinline__ uint64_t load_w_stream(const void* data, int64_t r)
+{
+  if (W == 1) return __ldcs(static_cast<const unsigned char*>(data) + r);
+  if (W == 2) return __ldcs(static_cast<const unsigned short*>(data) + r);
+  if (W == 4) return __ldcs(static_cast<const unsigned int*>(data) + r);
+  return __ldcs(static_cast<const unsigned long long*>(data) + r);
+}
+template <int W>
+__device__ __forceinline__ void store_w_stream(void* data, int64_t i, uint64_t v)
+{
+  if (W == 1) __stcs(static_cast<unsigned char*>(data) + i, static_cast<unsigned char>(v));
+  else if (W == 2) __stcs(static_cast<unsigned short*>(data) + i, static_cast<unsigned short>(v));
+  else if (W == 4) __stcs(static_cast<unsigned int*>(data) + i, static_cast<unsigned int>(v));
+  else __stcs(static_cast<unsigned long long*>(data) + i, static_cast<unsigned long long>(v));
+}
+
 // Device-side view of the build table.
 struct BuildTable {
   KeyCols bk;             // build keys (rhs)
@@ -359,8 +379,10 @@ __device__ __forceinline__ void emit(const ProbeArgs& a, int64_t pos, int64_t lr
 
 // Write output column set `o` for the kProbeItems rows of a thread at once:
 // for each column, the items' source values are loaded together, then
-// stored (row[i] < 0 -> null / zero; pos[i] < 0 -> no output row).
-template <int W>
+// stored (row[i] < 0 -> null / zero; pos[i] < 0 -> no output row).  STREAM:
+// the source is the probe side (rows in order, read once); otherwise the
+// build side (random rows, kept in L2).
+template <int W, bool STREAM>
 __device__ __forceinline__ void emit_column_batch(const DCol& src, const OCol& d, const int64_t* pos,
                                                   const int64_t* row)
 {
@@ -369,25 +391,28 @@ __device__ __forceinline__ void emit_column_batch(const DCol& src, const OCol& d
 #pragma unroll
   for (int i = 0; i < kProbeItems; ++i) {
     ok[i] = row[i] >= 0;
-    v[i]  = (pos[i] >= 0 && ok[i]) ? load_w<W>(src.data, row[i]) : 0;
-    if (d.valid && pos[i] >= 0 && ok[i] && src.valid) ok[i] = __ldg(src.valid + row[i]) != 0;
+    v[i]  = 0;
+    if (pos[i] >= 0 && ok[i]) v[i] = STREAM ? load_w_stream<W>(src.data, row[i]) : load_w<W>(src.data, row[i]);
+    if (d.valid && pos[i] >= 0 && ok[i] && src.valid)
+      ok[i] = (STREAM ? __ldcs(src.valid + row[i]) : __ldg(src.valid + row[i])) != 0;
   }
 #pragma unroll
   for (int i = 0; i < kProbeItems; ++i) {
     if (pos[i] < 0) continue;
-    store_w<W>(d.data, pos[i], v[i]);
-    if (d.valid) d.valid[pos[i]] = ok[i] ? 1 : 0;
+    store_w_stream<W>(d.data, pos[i], v[i]);
+    if (d.valid) __stcs(d.valid + pos[i], static_cast<uint8_t>(ok[i] ? 1 : 0));
   }
 }
 
 // One output column of `o` from source rows row[i] (see emit_column_batch).
+template <bool STREAM>
 __device__ __forceinline__ void emit_one(const DCol& src, const OCol& d, const int64_t* pos, const int64_t* row)
 {
   switch (d.width) {
-    case 1: emit_column_batch<1>(src, d, pos, row); break;
-    case 2: emit_column_batch<2>(src, d, pos, row); break;
-    case 4: emit_column_batch<4>(src, d, pos, row); break;
-    default: emit_column_batch<8>(src, d, pos, row); break;
+    case 1: emit_column_batch<1, STREAM>(src, d, pos, row); break;
+    case 2: emit_column_batch<2, STREAM>(src, d, pos, row); break;
+    case 4: emit_column_batch<4, STREAM>(src, d, pos, row); break;
+    default: emit_column_batch<8, STREAM>(src, d, pos, row); break;
   }
 }
 
@@ -409,12 +434,12 @@ __device__ __forceinline__ void emit_build_batch(const ProbeArgs& a, const int64
         if (pos[i] < 0) continue;
         const uint64_t v = q == 0 ? w[i].x : w[i].y;
         switch (d.width) {
-          case 1: store_w<1>(d.data, pos[i], v); break;
-          case 2: store_w<2>(d.data, pos[i], v); break;
-          case 4: store_w<4>(d.data, pos[i], v); break;
-          default: store_w<8>(d.data, pos[i], v); break;
+          case 1: store_w_stream<1>(d.data, pos[i], v); break;
+          case 2: store_w_stream<2>(d.data, pos[i], v); break;
+          case 4: store_w_stream<4>(d.data, pos[i], v); break;
+          default: store_w_stream<8>(d.data, pos[i], v); break;
         }
-        if (d.valid) d.valid[pos[i]] = brow[i] >= 0 ? 1 : 0;
+        if (d.valid) __stcs(d.valid + pos[i], static_cast<uint8_t>(brow[i] >= 0 ? 1 : 0));
       }
     }
   }
@@ -426,23 +451,17 @@ __device__ __forceinline__ void emit_build_batch(const ProbeArgs& a, const int64
       int64_t krow[kProbeItems];
 #pragma unroll
       for (int i = 0; i < kProbeItems; ++i) krow[i] = brow[i] >= 0 ? lrow[i] : -1;
-      emit_one(a.pk.c[0], o.dst[j], pos, krow);
+      emit_one<true>(a.pk.c[0], o.dst[j], pos, krow);
     } else {
-      emit_one(o.src[j], o.dst[j], pos, brow);
+      emit_one<false>(o.src[j], o.dst[j], pos, brow);
     }
   }
 }
 
+// The probe-side output columns (rows in order, streamed).
 __device__ __forceinline__ void emit_batch(const OutSpec& o, const int64_t* pos, const int64_t* row)
 {
-  for (int j = 0; j < o.n; ++j) {
-    switch (o.dst[j].width) {
-      case 1: emit_column_batch<1>(o.src[j], o.dst[j], pos, row); break;
-      case 2: emit_column_batch<2>(o.src[j], o.dst[j], pos, row); break;
-      case 4: emit_column_batch<4>(o.src[j], o.dst[j], pos, row); break;
-      default: emit_column_batch<8>(o.src[j], o.dst[j], pos, row); break;
-    }
-  }
+  for (int j = 0; j < o.n; ++j) emit_one<true>(o.src[j], o.dst[j], pos, row);
 }
 
 // COUNT: per-tile output counts.  WRITE: probe again (or use the single match

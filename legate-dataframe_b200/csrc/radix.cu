@@ -452,15 +452,33 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
 
 // Rows of a tile straight from global memory (GATHER: the word is loaded from
 // the columns at the row, the first pass of a word; otherwise the carried key).
+// In a pass on the carried word, all row ids and then all words are loaded
+// before any digit is taken, so that the thread's loads are in flight together.
 template <bool GATHER>
 __device__ __forceinline__ void load_tile_rows(const PassArgs& a, int64_t tile, uint64_t (&key)[RI],
                                                int32_t (&val)[RI], uint32_t (&dr)[RI])
 {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t tbase = tile * RTILE;
+  const int64_t wbase = tile * RTILE + warp * (32 * RI) + lane;
+  if (!GATHER && a.p.src != DigitSrc::CLASS) {
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+      const int64_t idx = wbase + i * 32;
+      val[i] = idx < a.n ? (a.vals_in ? __ldg(a.vals_in + idx) : static_cast<int32_t>(idx)) : 0;
+    }
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+      const int64_t idx = wbase + i * 32;
+      key[i] = idx < a.n ? __ldg(reinterpret_cast<const unsigned long long*>(a.keys_in) + idx) : 0ull;
+    }
+#pragma unroll
+    for (int i = 0; i < RI; ++i)
+      dr[i] = wbase + i * 32 < a.n ? static_cast<uint32_t>(key[i] >> a.p.shift) & 0xffu : 256u;
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < RI; ++i) {
-    const int64_t idx = tbase + warp * (32 * RI) + i * 32 + lane;
+    const int64_t idx = wbase + i * 32;
     key[i]            = 0;
     val[i]            = 0;
     dr[i]             = 256;
