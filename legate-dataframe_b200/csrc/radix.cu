@@ -85,12 +85,37 @@ __device__ __forceinline__ uint64_t pass_word(const RadixPass& p, int64_t row)
   return sort_word(p.key, row);
 }
 
+// Adds a fused-word component v placed at bit `off` of W to C = W >> 8 and
+// to W's low byte (components do not overlap, so OR adds them).  Since W has
+// at most 72 bits, v << (off - 8) fits C.
+__device__ __forceinline__ void fused_add(uint64_t v, int off, uint64_t& c, uint32_t& low)
+{
+  if (v == 0) return;  // also every component of no bits, whose `off` may reach 72
+  if (off >= 8) {
+    c |= v << (off - 8);
+  } else {
+    c |= v >> (8 - off);
+    low |= static_cast<uint32_t>(v << off) & 0xffu;
+  }
+}
+
+// C = W >> 8 of the fused word W of a row (FusedKey); *low = W's low byte.
+__device__ __forceinline__ uint64_t fused_word(const FusedKey& f, int64_t row, uint32_t& low)
+{
+  uint64_t c = 0;
+  low        = 0;
+#pragma unroll
+  for (int k = 0; k < kFuseMax; ++k)
+    if (k < f.n) fused_add(sort_word(f.key[k], row) - f.min[k], f.off[k], c, low);
+  return c;
+}
 
 constexpr int kHistPassesPerLaunch = 16;
 struct HistArgs {
   int npasses;
   uint32_t reuse;  // bit q: pass q reads the same key word as pass q - 1
   RadixPass p[kHistPassesPerLaunch];
+  FusedKey fused;
   int64_t n;
   uint32_t* hist;  // [npasses][256]
 };
@@ -117,6 +142,7 @@ __device__ __forceinline__ void load_raw_rows(const DCol& c, const int64_t (&r)[
 // All digit histograms of up to kHistPassesPerLaunch passes in one read of the
 // columns: kHR rows per thread, each key word loaded once for all the passes
 // over it (their loads in flight together), shared-memory counts.
+template <bool FUSED>
 __global__ void __launch_bounds__(RT) histogram_kernel(HistArgs a)
 {
   __shared__ uint32_t sh[kHistPassesPerLaunch * 256];
@@ -128,8 +154,9 @@ __global__ void __launch_bounds__(RT) histogram_kernel(HistArgs a)
 #pragma unroll
     for (int j = 0; j < kHR; ++j) r[j] = base + j * RT + threadIdx.x;
     uint64_t w[kHR];
+    uint32_t low[kHR];
 #pragma unroll
-    for (int j = 0; j < kHR; ++j) w[j] = 0;
+    for (int j = 0; j < kHR; ++j) w[j] = 0, low[j] = 0;
     for (int q = 0; q < a.npasses; ++q) {
       const RadixPass& p = a.p[q];
       uint32_t d[kHR];
@@ -141,6 +168,9 @@ __global__ void __launch_bounds__(RT) histogram_kernel(HistArgs a)
           if (p.src == DigitSrc::BUCKET) {
 #pragma unroll
             for (int j = 0; j < kHR; ++j) w[j] = r[j] < a.n ? bucket_word(p, r[j]) : 0;
+          } else if (FUSED && p.src == DigitSrc::FUSED) {
+#pragma unroll
+            for (int j = 0; j < kHR; ++j) w[j] = r[j] < a.n ? fused_word(a.fused, r[j], low[j]) : 0;
           } else {
             uint64_t raw[kHR];
             bool ok[kHR];
@@ -155,7 +185,9 @@ __global__ void __launch_bounds__(RT) histogram_kernel(HistArgs a)
           }
         }
 #pragma unroll
-        for (int j = 0; j < kHR; ++j) d[j] = r[j] < a.n ? static_cast<uint32_t>(w[j] >> p.shift) & 0xffu : 256u;
+        for (int j = 0; j < kHR; ++j)
+          d[j] = r[j] < a.n ? ((FUSED && p.fused_low) ? low[j] : static_cast<uint32_t>(w[j] >> p.shift) & 0xffu)
+                            : 256u;
       }
 #pragma unroll
       for (int j = 0; j < kHR; ++j)
@@ -179,6 +211,7 @@ struct PassArgs {
   unsigned long long* counter;
   int32_t* inv_out;  // != null: inv_out[row] = the row's output position
   RadixPayload pay;  // columns moved by this pass (payload_empty: none)
+  FusedKey fused;    // FUSED passes
   int* err;
 };
 
@@ -454,7 +487,7 @@ __device__ __forceinline__ void rank_and_scatter(const PassArgs& a, int64_t tile
 // the columns at the row, the first pass of a word; otherwise the carried key).
 // In a pass on the carried word, all row ids and then all words are loaded
 // before any digit is taken, so that the thread's loads are in flight together.
-template <bool GATHER>
+template <bool GATHER, bool FUSEDG = false>
 __device__ __forceinline__ void load_tile_rows(const PassArgs& a, int64_t tile, uint64_t (&key)[RI],
                                                int32_t (&val)[RI], uint32_t (&dr)[RI])
 {
@@ -474,6 +507,45 @@ __device__ __forceinline__ void load_tile_rows(const PassArgs& a, int64_t tile, 
 #pragma unroll
     for (int i = 0; i < RI; ++i)
       dr[i] = wbase + i * 32 < a.n ? static_cast<uint32_t>(key[i] >> a.p.shift) & 0xffu : 256u;
+    return;
+  }
+  if (FUSEDG) {
+    // the fused word from its key columns, one column at a time with the
+    // items' loads in flight together; dr[i] gathers W's low byte
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+      const int64_t idx = wbase + i * 32;
+      val[i] = idx < a.n ? (a.vals_in ? __ldg(a.vals_in + idx) : static_cast<int32_t>(idx)) : -1;
+      key[i] = 0;
+      dr[i]  = 0;
+    }
+    for (int k = 0; k < a.fused.n; ++k) {
+      const SortKeyDesc& kk = a.fused.key[k];
+      uint64_t raw[RI];
+#pragma unroll
+      for (int i = 0; i < RI; ++i) {
+        raw[i] = 0;
+        if (val[i] < 0) continue;
+        switch (kk.col.width) {
+          case 1: raw[i] = __ldg(static_cast<const uint8_t*>(kk.col.data) + val[i]); break;
+          case 2: raw[i] = __ldg(static_cast<const uint16_t*>(kk.col.data) + val[i]); break;
+          case 4: raw[i] = __ldg(static_cast<const uint32_t*>(kk.col.data) + val[i]); break;
+          default: raw[i] = __ldg(static_cast<const unsigned long long*>(kk.col.data) + val[i]); break;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < RI; ++i)
+        if (val[i] >= 0) fused_add(sort_word_of(kk, raw[i], true) - a.fused.min[k], a.fused.off[k], key[i], dr[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+      if (val[i] < 0) {
+        val[i] = 0;
+        dr[i]  = 256;
+      } else if (!a.p.fused_low) {
+        dr[i] = static_cast<uint32_t>(key[i] >> a.p.shift) & 0xffu;
+      }
+    }
     return;
   }
 #pragma unroll
@@ -498,7 +570,7 @@ __device__ __forceinline__ void load_tile_rows(const PassArgs& a, int64_t tile, 
 // One tile per CTA.  WRITE_KEYS: later passes of the same word follow, so
 // carry the word along.  MOVE: the pass also moves a.pay's columns (the last
 // pass only, which carries no word).
-template <bool GATHER, bool WRITE_KEYS, bool MOVE = false>
+template <bool GATHER, bool WRITE_KEYS, bool MOVE = false, bool FUSEDG = false>
 __global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs a)
 {
   __shared__ OsShared sh;
@@ -514,7 +586,7 @@ __global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs 
   uint64_t key[RI];
   int32_t val[RI];
   uint32_t dr[RI];
-  load_tile_rows<GATHER>(a, tile, key, val, dr);
+  load_tile_rows<GATHER, FUSEDG>(a, tile, key, val, dr);
   rank_and_scatter<WRITE_KEYS, MOVE>(a, tile, key, val, dr, sh, s_keys, s_vals, s_dig);
 }
 
@@ -523,17 +595,17 @@ constexpr size_t onesweep_smem(bool write_keys)
   return (write_keys ? RTILE * sizeof(uint64_t) : 0) + RTILE * (sizeof(int32_t) + 1);
 }
 
-template <bool GATHER, bool WRITE_KEYS, bool MOVE = false>
+template <bool GATHER, bool WRITE_KEYS, bool MOVE = false, bool FUSEDG = false>
 void launch_onesweep(cudaStream_t s, unsigned tiles, const PassArgs& a)
 {
   static_assert(!(MOVE && WRITE_KEYS), "the pass that moves columns is the last one");
   constexpr size_t smem = onesweep_smem(WRITE_KEYS);
-  LDF_CUDA(cudaFuncSetAttribute(onesweep_kernel<GATHER, WRITE_KEYS, MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  LDF_CUDA(cudaFuncSetAttribute(onesweep_kernel<GATHER, WRITE_KEYS, MOVE, FUSEDG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
   // profile names: a pass that loads its word from the columns, one that
   // moves the payload columns, the others
   const char* name = MOVE ? "onesweep_move" : (GATHER ? "onesweep_gather" : "onesweep");
-  launch(name, onesweep_kernel<GATHER, WRITE_KEYS, MOVE>, tiles, RT, smem, s, a);
+  launch(name, onesweep_kernel<GATHER, WRITE_KEYS, MOVE, FUSEDG>, tiles, RT, smem, s, a);
 }
 
 // Identity order: the payload columns copied as they are.
@@ -569,14 +641,92 @@ unsigned hist_blocks(int64_t n)
 bool same_word(const RadixPass& a, const RadixPass& b)
 {
   if (a.src != b.src || a.src == DigitSrc::CLASS) return false;
-  if (a.src == DigitSrc::BUCKET) return true;
+  if (a.src == DigitSrc::BUCKET || a.src == DigitSrc::FUSED) return true;
   return a.key.col.data == b.key.col.data && a.key.descending == b.key.descending;
+}
+
+struct WordRangeArgs {
+  int n;
+  SortKeyDesc key[kFuseMax];
+};
+
+// mm[2k] = min, mm[2k + 1] = max of key k's words (init ~0 and 0).  Eight
+// rows per thread, one key column at a time, loads in flight together.
+constexpr int kRangeRows = 8;
+__global__ void __launch_bounds__(256) word_range_kernel(WordRangeArgs a, int64_t n, unsigned long long* mm)
+{
+  unsigned long long lo[kFuseMax], hi[kFuseMax];
+#pragma unroll
+  for (int k = 0; k < kFuseMax; ++k) lo[k] = ~0ull, hi[k] = 0;
+  const int64_t per_iter = static_cast<int64_t>(blockDim.x) * kRangeRows;
+  for (int64_t base = blockIdx.x * per_iter; base < n; base += static_cast<int64_t>(gridDim.x) * per_iter) {
+#pragma unroll
+    for (int k = 0; k < kFuseMax; ++k) {
+      if (k >= a.n) continue;
+      const DCol& c = a.key[k].col;
+      uint64_t raw[kRangeRows];
+#pragma unroll
+      for (int j = 0; j < kRangeRows; ++j) {
+        const int64_t r = base + j * blockDim.x + threadIdx.x;
+        raw[j]          = 0;
+        if (r >= n) continue;
+        switch (c.width) {
+          case 1: raw[j] = __ldg(static_cast<const uint8_t*>(c.data) + r); break;
+          case 2: raw[j] = __ldg(static_cast<const uint16_t*>(c.data) + r); break;
+          case 4: raw[j] = __ldg(static_cast<const uint32_t*>(c.data) + r); break;
+          default: raw[j] = __ldg(static_cast<const unsigned long long*>(c.data) + r); break;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kRangeRows; ++j) {
+        if (base + j * blockDim.x + threadIdx.x >= n) continue;
+        const unsigned long long w = sort_word_of(a.key[k], raw[j], true);
+        lo[k]                      = w < lo[k] ? w : lo[k];
+        hi[k]                      = w > hi[k] ? w : hi[k];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kFuseMax; ++k) {
+    if (k >= a.n) continue;
+    for (int d = 16; d > 0; d >>= 1) {
+      const unsigned long long l = __shfl_xor_sync(0xffffffffu, lo[k], d);
+      const unsigned long long h = __shfl_xor_sync(0xffffffffu, hi[k], d);
+      lo[k]                      = l < lo[k] ? l : lo[k];
+      hi[k]                      = h > hi[k] ? h : hi[k];
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(mm + 2 * k, lo[k]);
+      atomicMax(mm + 2 * k + 1, hi[k]);
+    }
+  }
 }
 
 }  // namespace
 
+void sort_word_ranges(const OpContext& ctx, const SortKeyDesc* keys, int nkeys, int64_t n, uint64_t* mn,
+                      uint64_t* mx)
+{
+  LDF_REQUIRE(nkeys >= 1 && nkeys <= kFuseMax, "sort_word_ranges: too many keys");
+  cudaStream_t s = ctx.stream();
+  Buffer<unsigned long long> mm(ctx.alloc(), 2 * kFuseMax);
+  std::vector<unsigned long long> h(2 * kFuseMax);
+  for (int k = 0; k < kFuseMax; ++k) h[2 * k] = ~0ull, h[2 * k + 1] = 0;
+  LDF_CUDA(cudaMemcpyAsync(mm.get(), h.data(), h.size() * 8, cudaMemcpyHostToDevice, s));
+  WordRangeArgs a{};
+  a.n = nkeys;
+  for (int k = 0; k < nkeys; ++k) a.key[k] = keys[k];
+  if (n > 0) launch("word_range", word_range_kernel, hblocks(n), 256, 0, s, a, n, mm.get());
+  LDF_CUDA(cudaMemcpyAsync(h.data(), mm.get(), h.size() * 8, cudaMemcpyDeviceToHost, s));
+  ctx.finish();
+  for (int k = 0; k < nkeys; ++k) {
+    mn[k] = h[2 * k];
+    mx[k] = h[2 * k + 1];
+  }
+}
+
 void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
-                      uint32_t* d_hist)
+                      uint32_t* d_hist, const FusedKey* fused)
 {
   cudaStream_t s = ctx.stream();
   LDF_CUDA(cudaMemsetAsync(d_hist, 0, passes.size() * 256 * sizeof(uint32_t), s));
@@ -587,15 +737,18 @@ void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes
       h.p[q] = passes[b + q];
       if (q > 0 && same_word(passes[b + q - 1], passes[b + q])) h.reuse |= 1u << q;
     }
+    if (fused) h.fused = *fused;
     h.n    = n;
     h.hist = d_hist + b * 256;
-    if (n > 0) launch("histogram", histogram_kernel, hist_blocks(n), RT, 0, s, h);
+    if (n > 0 && fused) launch("histogram", histogram_kernel<true>, hist_blocks(n), RT, 0, s, h);
+    else if (n > 0) launch("histogram", histogram_kernel<false>, hist_blocks(n), RT, 0, s, h);
     LDF_CHECK_LAUNCH();
   }
 }
 
 void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
-                     int32_t* perm, std::vector<uint32_t>* hist_out, int32_t* inv, const RadixPayload* payload)
+                     int32_t* perm, std::vector<uint32_t>* hist_out, int32_t* inv, const RadixPayload* payload,
+                     const FusedKey* fused)
 {
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
@@ -603,7 +756,7 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
   std::vector<uint32_t> hist(P * 256, 0);
   if (P > 0 && n > 0) {
     Buffer<uint32_t> d_hist(al, P * 256);
-    radix_histograms(ctx, passes, n, d_hist.get());
+    radix_histograms(ctx, passes, n, d_hist.get(), fused);
     LDF_CUDA(cudaMemcpyAsync(hist.data(), d_hist.get(), P * 256 * sizeof(uint32_t),
                              cudaMemcpyDeviceToHost, s));
     ctx.finish();
@@ -665,10 +818,15 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
     a.counter    = reinterpret_cast<unsigned long long*>(status.get() + tiles * 256);
     a.inv_out    = k + 1 == run.size() ? inv : nullptr;
     if (k + 1 == run.size() && payload) a.pay = *payload;
+    if (fused) a.fused = *fused;
     a.err        = ctx.err();
     const unsigned g = static_cast<unsigned>(tiles);
     const bool move = !payload_empty(a.pay);
-    if (move && gather) launch_onesweep<true, false, true>(s, g, a);
+    if (gather && p.src == DigitSrc::FUSED) {  // the fused word's first pass
+      if (move) launch_onesweep<true, false, true, true>(s, g, a);
+      else if (write_keys) launch_onesweep<true, true, false, true>(s, g, a);
+      else launch_onesweep<true, false, false, true>(s, g, a);
+    } else if (move && gather) launch_onesweep<true, false, true>(s, g, a);
     else if (move) launch_onesweep<false, false, true>(s, g, a);
     else if (gather && write_keys) launch_onesweep<true, true>(s, g, a);
     else if (gather) launch_onesweep<true, false>(s, g, a);
@@ -694,7 +852,7 @@ void radix_histogram_raw(cudaStream_t s, const RadixPass& p, int64_t n, uint32_t
   h.p[0]    = p;
   h.n       = n;
   h.hist    = d_hist;
-  launch("histogram", histogram_kernel, hist_blocks(n), RT, 0, s, h);
+  launch("histogram", histogram_kernel<false>, hist_blocks(n), RT, 0, s, h);
 }
 
 int64_t radix_status_words(int64_t n) { return ceil_div(n, RTILE) * 256 + 2; }

@@ -18,7 +18,8 @@ enum class DigitSrc : int {
   CARRIED = 0,  // byte `shift/8` of the carried key word
   COLUMN  = 1,  // load the key column at the row, transform, then byte
   CLASS   = 2,  // 0/1/2 class of the row: value / NaN / null, ordered by nulls_at_end
-  BUCKET  = 3   // hash of the key columns % nparts (then byte)
+  BUCKET  = 3,  // hash of the key columns % nparts (then byte)
+  FUSED   = 4   // byte of the fused word of several keys (FusedKey)
 };
 
 // Value transform of one sort key column into an order-preserving unsigned
@@ -33,11 +34,33 @@ struct SortKeyDesc {
 
 struct RadixPass {
   DigitSrc src;
-  int shift;  // bit offset of the digit in the key word
+  int shift;      // bit offset of the digit in the key word (FUSED: in C)
+  int fused_low;  // FUSED: the pass of the fused word's low byte
   SortKeyDesc key;
   KeyCols hash_keys;  // BUCKET
   uint32_t nparts;    // BUCKET
 };
+
+// Several sort keys without nulls or floating-point values packed into one
+// word, least significant key first: W = sum_k (word_k - min_k) << off_k,
+// word_k the key's order-preserving word (inverted when descending) and
+// min_k its minimum over the rows, at most kFusedMaxBits bits in all.  The
+// pass of W's low byte loads every key at the row and carries C = W >> 8
+// (64 bits); the later passes take byte shift / 8 of C.  One word for all
+// the keys means that no pass gathers a key column through the permutation.
+constexpr int kFuseMax      = 4;
+constexpr int kFusedMaxBits = 72;
+struct FusedKey {
+  int n;
+  SortKeyDesc key[kFuseMax];
+  uint64_t min[kFuseMax];
+  int off[kFuseMax];
+};
+
+// Minimum and maximum of the order-preserving words of `keys` (no nulls)
+// over n rows, one read of each column.
+void sort_word_ranges(const OpContext& ctx, const SortKeyDesc* keys, int nkeys, int64_t n, uint64_t* mn,
+                      uint64_t* mx);
 
 // Stable sort of rows by a list of passes (least significant first).
 // Returns the permutation (row ids) in `perm` (n entries, caller allocated).
@@ -48,7 +71,7 @@ struct RadixPlan {
 
 // Upfront digit histograms of every candidate pass: hist[p * 256 + d].
 void radix_histograms(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
-                      uint32_t* d_hist);
+                      uint32_t* d_hist, const FusedKey* fused = nullptr);
 
 // Run the passes; `perm` receives the row order.  Passes whose histogram has a
 // single bucket holding every row are skipped.
@@ -77,9 +100,9 @@ inline bool payload_empty(const RadixPayload& p) { return p.n == 0 && p.nparts =
 
 // `inv` (optional, n entries): inv[row] = the row's position in the sorted
 // order, written by the last pass.  `payload` (optional): columns the last
-// pass writes in sorted order.
+// pass writes in sorted order.  `fused`: the FusedKey of FUSED passes.
 void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes, int64_t n,
                      int32_t* perm, std::vector<uint32_t>* hist_out = nullptr, int32_t* inv = nullptr,
-                     const RadixPayload* payload = nullptr);
+                     const RadixPayload* payload = nullptr, const FusedKey* fused = nullptr);
 
 }  // namespace ldf

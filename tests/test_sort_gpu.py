@@ -69,6 +69,36 @@ def test_sort_string_and_timestamp(asc):
         assert_tables_equal(res, exp, sort_by=None)
 
 
+@pytest.mark.parametrize("case", ["fits64", "fits72", "too_wide", "limit", "string_ts"])
+def test_sort_fused_key_word(case):
+    """Keys without nulls or floats whose value ranges fit 72 bits are sorted
+    on one fused word (every key loaded in input order by the first pass,
+    carried through the others): mixed directions, negative values, ties on
+    every key, a word over 64 bits (its low byte sorted on its own), one over
+    72 bits (per-key passes), a limit, and a string key with a timestamp."""
+    rng = np.random.default_rng(31)
+    n = 1_000_003
+    a = rng.integers(-50, 51, n).astype(np.int8)
+    b = rng.integers(0, 1_000, n).astype(np.int32)
+    if case == "fits64":
+        c = rng.integers(-(2**30), 2**30, n)
+    elif case == "too_wide":
+        c = rng.integers(-(2**62), 2**62, n)
+    else:
+        c = 1_700_000_000_000_000 + rng.integers(0, 2**50, n)
+    t = pa.table({"a": a, "b": b, "c": c, "row": np.arange(n)})
+    if case == "string_ts":
+        words = np.array([f"w{i * 7919 % 10007:05d}{'x' * (i % 5)}" for i in range(20_000)], dtype=object)
+        t = pa.table({"s": pa.array(words[rng.integers(0, 20_000, n)]),
+                      "ts": pa.array(c, type=pa.timestamp("us")), "row": np.arange(n)})
+        res = run_sort(t, ["s", "ts"], [True, False])
+        assert_tables_equal(res, R.sort(t, ["s", "ts"], [True, False]), sort_by=None)
+        return
+    limit = 1000 if case == "limit" else None
+    res = run_sort(t, ["a", "b", "c"], [False, True, False], limit=limit)
+    assert_tables_equal(res, R.sort(t, ["a", "b", "c"], [False, True, False], limit=limit), sort_by=None)
+
+
 def test_sort_stability_many_ties():
     rng = np.random.default_rng(2)
     n = 300_000
