@@ -196,6 +196,29 @@ int ldf_b200_arrow_bits_to_bytes(const uint8_t* bits, int64_t bit_offset, int64_
 int ldf_b200_arrow_offsets_to_ranges(const void* offsets, int32_t offset_bytes, int64_t n,
                                      ldf_range* ranges, void* stream);
 
+/* ---- CSV text -> columns, parsed on the device --------------------------- */
+/* Replaces cudf::io::read_csv in CSVRead::gpu_variant (csv.cu:53-139) with
+ * the conversions of the reference's Arrow reader (CSVRead::cpu_variant,
+ * csv.cpp:58-130).  `text` (device) holds one file's `nbytes` bytes.
+ * Records end at '\n', "\r\n" or a lone '\r' outside quotes; empty records
+ * are skipped; `skip_first` skips the first record (the header).  A field
+ * that starts with '"' is quoted up to the next lone '"' ("" is one quote;
+ * terminators inside quotes belong to the field; characters after the
+ * closing quote are kept).  Every record must have as many fields as the
+ * first.  Output column j is field `fields[j]` converted to `types[j]`:
+ * LDF_BOOL8 ("1/True/TRUE/true", "0/False/FALSE/false"), the integer types
+ * (decimal, or 0x-hex bit patterns; spaces and tabs trimmed), LDF_FLOAT32/64
+ * (correctly rounded; "inf"/"infinity" any case), LDF_STRING (valid UTF-8).
+ * Fields equal to one of the `n_nulls` spellings in `nulls` (NUL-separated,
+ * `nulls_bytes` bytes in all; host memory) are nulls, and then every output
+ * column has a null mask; with no spellings no column has one.  A value that
+ * does not convert fails with LDF_ERR_INVALID_ARGUMENT and the record's line.
+ * At most 64 output columns and 1024 fields per record. */
+int ldf_b200_csv_read(const uint8_t* text, int64_t nbytes, char delimiter, int32_t skip_first,
+                      const int32_t* fields, const int32_t* types, int32_t ncols,
+                      const char* nulls, int32_t nulls_bytes, int32_t n_nulls,
+                      ldf_column* out, int64_t* nrows, const ldf_allocator* alloc, void* stream);
+
 /* ---- test hook: a bounded wait that runs out ------------------------------ */
 /* No counterpart in the reference (its waits are inside libcudf).  Runs the
  * library's look-back scan kernel as one block that takes the second tile of

@@ -33,6 +33,7 @@ SOURCES = [
     "batch.cu",
     "distinct.cu",
     "ingest.cu",
+    "csv.cu",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -44,11 +45,12 @@ CFLAGS = [
     "-Xcompiler",
     "-fPIC,-O3",
     f"-I{INCLUDE}",
+    f"-I{BUILD_DIR}",  # generated tables (pow5_table.inc)
 ]
 
 
 def _newest_input_mtime() -> float:
-    files = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    files = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.py")) + list(INCLUDE.glob("*.h"))
     files.append(Path(__file__))
     return max(f.stat().st_mtime for f in files)
 
@@ -71,6 +73,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if LIB.exists() and not force and LIB.stat().st_mtime >= _newest_input_mtime():
         return LIB
     BUILD_DIR.mkdir(parents=True, exist_ok=True)
+    subprocess.run([sys.executable, str(CSRC / "pow5_table.py"), str(BUILD_DIR / "pow5_table.inc")], check=True)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
     tmp = LIB.with_suffix(".so.tmp")

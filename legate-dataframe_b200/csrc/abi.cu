@@ -17,6 +17,9 @@ void distinct(const ldf_column* table, int ncols, const int32_t* keys, int nkeys
               const OpContext& ctx);
 void arrow_bits_to_bytes(const uint8_t* bits, int64_t bit_offset, int64_t n, uint8_t* out, cudaStream_t s);
 void arrow_offsets_to_ranges(const void* offsets, int offset_bytes, int64_t n, ldf_range* out, cudaStream_t s);
+void csv_read(const uint8_t* text, int64_t n, char delimiter, int skip_first, const int32_t* fields,
+              const int32_t* types, int ncols, const char* nulls, int nulls_bytes, int n_nulls, ldf_column* out,
+              int64_t* nrows, const OpContext& ctx);
 }  // namespace ldf
 
 namespace {
@@ -137,6 +140,17 @@ int ldf_b200_arrow_offsets_to_ranges(const void* offsets, int32_t offset_bytes, 
 {
   return guarded([&] {
     ldf::arrow_offsets_to_ranges(offsets, offset_bytes, n, ranges, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int ldf_b200_csv_read(const uint8_t* text, int64_t nbytes, char delimiter, int32_t skip_first, const int32_t* fields,
+                      const int32_t* types, int32_t ncols, const char* nulls, int32_t nulls_bytes, int32_t n_nulls,
+                      ldf_column* out, int64_t* nrows, const ldf_allocator* alloc, void* stream)
+{
+  return guarded([&] {
+    ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
+    ldf::csv_read(text, nbytes, delimiter, skip_first != 0, fields, types, ncols, nulls, nulls_bytes, n_nulls, out,
+                  nrows, ctx);
   });
 }
 

@@ -149,6 +149,12 @@ def lib():
             ]
             L.ldf_b200_test_stalled_lookback.argtypes = [ctypes.c_uint32, P(ldf_allocator), ctypes.c_void_p]
             L.ldf_b200_test_stalled_lookback.restype = ctypes.c_int
+            L.ldf_b200_csv_read.argtypes = [
+                ctypes.c_void_p, ctypes.c_int64, ctypes.c_char, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
+                P(ldf_column), ctypes.POINTER(ctypes.c_int64), P(ldf_allocator), ctypes.c_void_p,
+            ]
+            L.ldf_b200_csv_read.restype = ctypes.c_int
             L.ldf_b200_arrow_bits_to_bytes.restype = ctypes.c_int
             L.ldf_b200_arrow_offsets_to_ranges.restype = ctypes.c_int
             L.ldf_b200_launch_count.restype = ctypes.c_ulonglong
