@@ -594,11 +594,12 @@ struct CsvOut {
 
 constexpr int64_t kQuotedBit = int64_t(1) << 62;
 
-// Converts field [b, e) of record `line` into output column k, row `row`.
-__device__ void convert_field(const CsvParams& P, const CsvOut& O, int64_t line, int64_t row, int k, int64_t b,
-                              int64_t e, unsigned long long* err)
+// Converts field t[b, e) of record `line` into output column k, row `row`;
+// `off` turns positions in t into positions in the text (t may be a staged
+// copy of part of it).
+__device__ void convert_field(const CsvParams& P, const CsvOut& O, const uint8_t* t, int64_t off, int64_t line,
+                              int64_t row, int k, int64_t b, int64_t e, unsigned long long* err)
 {
-  const uint8_t* t  = P.text;
   const bool quoted = e > b && t[b] == '"';
   const int type    = P.types[k];
   uint8_t buf[kCsvNumBuf];
@@ -620,7 +621,7 @@ __device__ void convert_field(const CsvParams& P, const CsvOut& O, int64_t line,
       }
       if (!u8.ok()) csv_error(err, line, k, kErrUtf8);
     }
-    O.str_src[k][row] = b | (quoted ? kQuotedBit : 0);
+    O.str_src[k][row] = (b + off) | (quoted ? kQuotedBit : 0);
     O.str_len[k][row] = n;
     return;
   }
@@ -633,7 +634,7 @@ __device__ void convert_field(const CsvParams& P, const CsvOut& O, int64_t line,
         csv_error(err, line, k, kErrConvert);
       } else if (r == 2) {
         const unsigned int d = atomicAdd(O.ndeferred, 1u);
-        if (d < kCsvMaxDeferred) O.deferred[d] = DeferredFloat{line, row, b, e, k};
+        if (d < kCsvMaxDeferred) O.deferred[d] = DeferredFloat{line, row, b + off, e + off, k};
         else csv_error(err, line, k, kErrUnsupported);
       }
     } else if (len < 0) {
@@ -942,21 +943,70 @@ __global__ void csv_first_fields_kernel(CsvParams P, const int64_t* lstart, cons
 }
 
 // One thread per record: output row, field walk, conversions, field count.
-__global__ void __launch_bounds__(128) csv_parse_kernel(CsvParams P, CsvOut O, const int64_t* lstart,
-                                                        const int64_t* lend, const int64_t* rowidx, int64_t nrec,
-                                                        int64_t first, int skip_first, int nfields,
-                                                        unsigned long long* err)
+// A block takes kParseRecords consecutive records at a time; their bytes
+// (contiguous in the text) are first staged in shared memory with 16-byte
+// loads (a group longer than the stage is read from global memory).  Each
+// thread then walks its record once per batch of kColBatch output columns,
+// noting the bounds of those columns' fields, and the batch's columns are
+// converted one after another by all threads together: the conversion code
+// of one type runs in lockstep across the warp instead of each thread being
+// at a different field of its record.
+constexpr int kParseRecords = 128;
+constexpr int kParseStage   = 24 * 1024;
+constexpr int kColBatch     = 16;
+__global__ void __launch_bounds__(kParseRecords) csv_parse_kernel(CsvParams P, CsvOut O, const int64_t* lstart,
+                                                                  const int64_t* lend, const int64_t* rowidx,
+                                                                  int64_t nrec, int64_t first, int skip_first,
+                                                                  int nfields, unsigned long long* err)
 {
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrec; r += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t s = lstart[r], e = lend[r];
-    if (e <= s || (skip_first && r == first)) continue;
-    const int64_t row = rowidx[r] - (skip_first && r > first ? 1 : 0);
-    const int got     = walk_fields(P.text, s, e, static_cast<uint8_t>(P.delim), [&](int f, int64_t b, int64_t fe) {
-      if (f >= P.nfield_map) return;
-      const int k = P.col_of_field[f];
-      if (k >= 0) convert_field(P, O, r, row, k, b, fe, err);
-    });
-    if (got != nfields) csv_error(err, r, 0, kErrFields);
+  __shared__ __align__(16) uint8_t stage[kParseStage];
+  __shared__ int32_t s_fb[kColBatch][kParseRecords];  // field bounds relative to the record's start
+  __shared__ int32_t s_fe[kColBatch][kParseRecords];
+  const uint8_t delim = static_cast<uint8_t>(P.delim);
+  const int tid       = threadIdx.x;
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * kParseRecords; g < nrec;
+       g += static_cast<int64_t>(gridDim.x) * kParseRecords) {
+    const int64_t last = g + kParseRecords < nrec ? g + kParseRecords - 1 : nrec - 1;
+    const int64_t gs   = lstart[g] & ~int64_t(15);
+    const int64_t ge   = lend[last];
+    const bool staged  = ge - gs <= kParseStage;
+    if (staged) {
+      const int64_t full = (ge - gs) >> 4;  // 16-byte blocks inside [gs, ge)
+      for (int64_t q = tid; q < full; q += blockDim.x)
+        reinterpret_cast<uint4*>(stage)[q] = *reinterpret_cast<const uint4*>(P.text + gs + 16 * q);
+      for (int64_t i = gs + 16 * full + tid; i < ge; i += blockDim.x) stage[i - gs] = P.text[i];
+    }
+    __syncthreads();
+    const uint8_t* t = staged ? stage : P.text;
+    const int64_t off = staged ? gs : 0;
+    const int64_t r   = g + tid;
+    bool active       = false;
+    int64_t s = 0, e = 0, row = 0;
+    if (r < nrec) {
+      s      = lstart[r] - off;
+      e      = lend[r] - off;
+      active = e > s && !(skip_first && r == first);
+      if (active) row = rowidx[r] - (skip_first && r > first ? 1 : 0);
+    }
+    for (int k0 = 0; k0 < P.ncols; k0 += kColBatch) {
+      const int k1 = k0 + kColBatch < P.ncols ? k0 + kColBatch : P.ncols;
+      bool ok      = false;
+      if (active) {
+        const int got = walk_fields(t, s, e, delim, [&](int f, int64_t b, int64_t fe) {
+          if (f >= P.nfield_map) return;
+          const int k = P.col_of_field[f];
+          if (k >= k0 && k < k1) {
+            s_fb[k - k0][tid] = static_cast<int32_t>(b - s);
+            s_fe[k - k0][tid] = static_cast<int32_t>(fe - s);
+          }
+        });
+        ok = got == nfields;  // otherwise some fields were never found: reported, not converted
+        if (!ok && k0 == 0) csv_error(err, r, 0, kErrFields);
+      }
+      for (int k = k0; k < k1; ++k)
+        if (ok) convert_field(P, O, t, off, r, row, k, s + s_fb[k - k0][tid], s + s_fe[k - k0][tid], err);
+    }
+    __syncthreads();
   }
 }
 
@@ -1097,7 +1147,7 @@ void csv_read(const uint8_t* text, int64_t n, char delimiter, int skip_first, co
       }
     }
     if (rows > 0) {
-      launch("csv_parse", csv_parse_kernel, csv_blocks(nrec, 128), 128, 0, s, P, O,
+      launch("csv_parse", csv_parse_kernel, csv_blocks(nrec, kParseRecords), kParseRecords, 0, s, P, O,
              static_cast<const int64_t*>(lstart.get()), static_cast<const int64_t*>(lend.get()),
              static_cast<const int64_t*>(rowidx.get()), nrec, static_cast<int64_t>(h_first), skip_first ? 1 : 0,
              h_nfields, first.get() + 1);

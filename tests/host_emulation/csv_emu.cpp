@@ -152,7 +152,7 @@ int main()
     const int got     = walk_fields(P.text, rec[i].first, rec[i].second, (uint8_t)delim, [&](int f, int64_t b, int64_t e) {
       if (f >= P.nfield_map) return;
       const int k = P.col_of_field[f];
-      if (k >= 0) convert_field(P, O, i, row, k, b, e, &err);
+      if (k >= 0) convert_field(P, O, P.text, 0, i, row, k, b, e, &err);
     });
     if (got != nfields) csv_error(&err, i, 0, kErrFields);
   }
