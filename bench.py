@@ -13,10 +13,12 @@ At N=1 the same JSON line also carries
     (int32 keys, 5% null probe keys, Zipf(0.9) hits);
   * `strings`: 100M string-key rows: groupby SUM/COUNT(*), stable sort
     (key asc, ts desc), hash_partition into 256 buckets;
+  * `csv`: csv_read of a 4M-row CSV file of the string workload's shape on
+    the device reader, against Arrow's CSV reader on the host;
   * `served`: the batched/served mix (8,192 small joins and groupbys arriving
     at 2,000 req/s) through the continuous-batching server and, for
     comparison, the same requests issued one op per launch.
-(--no-joins / --no-strings / --no-served skip them.)
+(--no-joins / --no-strings / --no-csv / --no-served skip them.)
 
 `--workload join|strings|sort|ingest` instead prints one line per op.
 
@@ -547,6 +549,83 @@ def run_sort_workload(args):
     return 0
 
 
+def _string_workload_table(n: int, seed: int = 9):
+    """n rows shaped like the 100M-row string workload, on the host: string
+    key from a 2M-entry dictionary (Zipf), 10% null int64 ts, float32 value."""
+    import numpy as np
+    import pyarrow as pa
+
+    nd = 2_000_000
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(8, 25, nd)
+    alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz0123456789", dtype=np.uint8)
+    chars = alphabet[rng.integers(0, 36, int(lens.sum()))]
+    doff = np.zeros(nd + 1, np.int32)
+    np.cumsum(lens, out=doff[1:])
+    dictionary = pa.StringArray.from_buffers(nd, pa.py_buffer(doff), pa.py_buffer(chars.tobytes()))
+    ranks = np.minimum(rng.zipf(1.5, n), nd) - 1
+    key = pa.DictionaryArray.from_arrays(pa.array(ranks.astype(np.int32)), dictionary).cast(pa.string())
+    ts = pa.array(rng.integers(0, 365 * 86400 * 10**6, n), mask=rng.random(n) < 0.10)
+    val = pa.array(rng.lognormal(size=n).astype(np.float32))
+    return pa.table({"k": key, "ts": ts, "v": val})
+
+
+def csv_record(n: int, steps: int = 3) -> dict:
+    """csv_read of an n-row CSV file of the string workload's shape (local
+    file, page cache warm): the device reader end to end (file -> pinned
+    memory -> device -> parsed columns), its kernels, and the reference's
+    CPU reader on the same file (Arrow read_csv, use_threads=False as in
+    CSVRead::cpu_variant, and with all host threads); parity against Arrow."""
+    import pyarrow as pa
+    import pyarrow.csv as pacsv
+    import torch
+
+    from legate_dataframe import _native as N
+    from legate_dataframe.lib.csv import csv_read
+
+    t = _string_workload_table(n)
+    names, dtypes = t.column_names, [pa.string(), pa.int64(), pa.float32()]
+    conv = pacsv.ConvertOptions(column_types=dict(zip(names, dtypes)), strings_can_be_null=True,
+                                quoted_strings_can_be_null=True)
+
+    def wall(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+            del r
+        return statistics.median(ts)
+
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "t.csv")
+        pacsv.write_csv(t, path)
+        size = os.path.getsize(path)
+        dev_s = wall(lambda: csv_read(path, dtypes=dtypes, names=names))
+        N.profile_enable(True)
+        N.profile_report(reset=True)
+        got = csv_read(path, dtypes=dtypes, names=names)
+        torch.cuda.synchronize()
+        prof = N.profile_report(reset=True)
+        N.profile_enable(False)
+        one = wall(lambda: pacsv.read_csv(path, read_options=pacsv.ReadOptions(use_threads=False),
+                                          convert_options=conv))
+        allt = wall(lambda: pacsv.read_csv(path, convert_options=conv))
+        exp = pacsv.read_csv(path, parse_options=pacsv.ParseOptions(newlines_in_values=True), convert_options=conv)
+        parity = "ok" if got.to_arrow().equals(exp.select(names)) else "MISMATCH"
+    kernel_ms = sum(v[1] for v in prof.values())
+    return {"op": f"csv_read: {n} rows, {size} bytes (string key, nullable int64, float32)",
+            "ms": round(dev_s * 1e3, 3), "GBps_text": size / dev_s / 1e9, "rows_per_s": n / dev_s,
+            "kernel_ms": round(kernel_ms, 3), "kernel_GBps_text": size / (kernel_ms / 1e3) / 1e9,
+            "kernels_ms": {k: [c, round(ms, 4)] for k, (c, ms) in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "arrow_1_thread_ms": round(one * 1e3, 3), "arrow_all_threads_ms": round(allt * 1e3, 3),
+            "host_threads": host_cores(), "vs_arrow_1_thread": one / dev_s, "vs_arrow_all_threads": allt / dev_s,
+            "parity": parity, "timing": "host wall clock, median, device synchronized; file in the page cache"}
+
+
 def run_ingest_workload(args):
     """--rows (default 20M) rows as a host Arrow table shaped like the string
     workload (string key from a 2M-entry dictionary, 10% null int64 ts,
@@ -564,19 +643,8 @@ def run_ingest_workload(args):
     from legate_dataframe.lib.parquet import parquet_read
 
     dev = torch.device("cuda", 0)
-    n, nd = args.rows, 2_000_000
-    rng = np.random.default_rng(9)
-    lens = rng.integers(8, 25, nd)
-    alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz0123456789", dtype=np.uint8)
-    chars = alphabet[rng.integers(0, 36, int(lens.sum()))]
-    doff = np.zeros(nd + 1, np.int32)
-    np.cumsum(lens, out=doff[1:])
-    dictionary = pa.StringArray.from_buffers(nd, pa.py_buffer(doff), pa.py_buffer(chars.tobytes()))
-    ranks = np.minimum(rng.zipf(1.5, n), nd) - 1
-    key = pa.DictionaryArray.from_arrays(pa.array(ranks.astype(np.int32)), dictionary).cast(pa.string())
-    ts = pa.array(rng.integers(0, 365 * 86400 * 10**6, n), mask=rng.random(n) < 0.10)
-    val = pa.array(rng.lognormal(size=n).astype(np.float32))
-    t = pa.table({"k": key, "ts": ts, "v": val})
+    n = args.rows
+    t = _string_workload_table(n)
     arrow_bytes = sum(b.size for c in t.columns for ch in c.chunks for b in ch.buffers() if b is not None)
 
     def host_then_copy():
@@ -614,6 +682,7 @@ def run_ingest_workload(args):
         print(json.dumps({"workload": f"ingest {name}: {n} rows", "ms": round(ms, 3), "rows_per_s": n / (ms / 1e3),
                           "arrow_GBps": arrow_bytes / (ms / 1e3) / 1e9, "arrow_bytes": arrow_bytes,
                           "timing": "host wall clock, median, device synchronized"}), flush=True)
+    print(json.dumps(csv_record(n, steps)), flush=True)
     return 0
 
 
@@ -630,6 +699,7 @@ def main():
     ap.add_argument("--served-requests", type=int, default=8192)
     ap.add_argument("--no-joins", action="store_true")
     ap.add_argument("--no-strings", action="store_true")
+    ap.add_argument("--no-csv", action="store_true")
     ap.add_argument("--sub-steps", type=int, default=5, help="timed steps of each join / string op record")
     ap.add_argument("--ops", default="", help="--workload strings: comma list of groupby,sort,partition (default all)")
     ap.add_argument("--workload", default="groupby", choices=["groupby", "join", "strings", "sort", "ingest"],
@@ -796,6 +866,11 @@ def main():
     if joins is not None:
         parity["joins"] = "ok" if all(r.get("parity") == "ok" for r in joins) else "MISMATCH"
 
+    csv = None
+    if rank == 0 and world == 1 and not args.no_csv:
+        csv = csv_record(4_000_000)
+        parity["csv"] = csv["parity"]
+
     # ---- served mix (rank 0, N=1 only) --------------------------------------
     served = None
     if rank == 0 and world == 1 and not args.no_served:
@@ -833,6 +908,7 @@ def main():
         "cpu_baseline": cpu,
         "joins": joins,
         "strings": strings,
+        "csv": csv,
         "served": served,
     }
     print(json.dumps(line))
