@@ -14,6 +14,7 @@
 #include <memory>
 #include <optional>
 #include <string>
+#include <utility>
 #include <vector>
 
 // ---- Arrow (the types the task arguments carry; utils.cpp:30-139) ---------
@@ -179,6 +180,10 @@ template <typename T>
 T get_next_scalar(TaskContext& ctx);  // task_argument.hpp:126
 template <typename T>
 std::vector<T> get_next_scalar_vector(TaskContext& ctx);  // task_argument.hpp:148
+void get_parallel_launch_task(TaskContext& ctx);         // task_argument.hpp:281
 }  // namespace argument
+
+[[nodiscard]] std::pair<size_t, size_t> evenly_partition_work(size_t work_size, size_t rank,
+                                                              size_t nranks);  // utils.hpp:156
 
 }  // namespace legate::dataframe

@@ -1,12 +1,14 @@
-// The GPU task bodies of legate-dataframe's join, groupby_aggregation, sort
-// and the local step of repartition_by_hash, rewritten over the C ABI of
-// libldf_b200.so.  INTEGRATION.md shows this code; the test suite type-checks
+// The GPU task bodies of legate-dataframe's join, groupby_aggregation, sort,
+// the local step of repartition_by_hash and CSV read, rewritten over the C ABI
+// of libldf_b200.so.  INTEGRATION.md shows this code; the test suite type-checks
 // it against include/ldf_b200.h and the stand-in declarations of the
 // reference's task-side API (reference_api.hpp).
 #include "reference_api.hpp"
 
 #include <ldf_b200.h>
 
+#include <fstream>
+#include <iterator>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -271,6 +273,56 @@ std::vector<ldf_column> hash_partition_local(TaskContext& ctx, std::vector<Physi
                                     static_cast<int32_t>(keys.size()), ctx.nranks, res.data(), offsets.data(),
                                     &alloc, ctx.stream()));
   return res;
+}
+
+// ---- CSVRead::gpu_variant (csv.cu:53-139) --------------------------------------
+// Each rank parses whole files (as the CPU variant splits the files,
+// csv.cpp:87-88): the bytes go to a device buffer from the task's resource
+// and ldf_b200_csv_read parses them there.  This sketch binds one file per
+// rank; several files per rank would concatenate the columns.
+void csv_read_gpu_body(TaskContext& ctx)
+{
+  const auto file_paths   = argument::get_next_scalar_vector<std::string>(ctx);
+  const auto column_names = argument::get_next_scalar_vector<std::string>(ctx);
+  const auto use_cols     = argument::get_next_scalar_vector<int>(ctx);
+  const bool na_filter    = argument::get_next_scalar<bool>(ctx);
+  const auto delimiter    = static_cast<char>(argument::get_next_scalar<int32_t>(ctx));
+  const auto nbytes       = argument::get_next_scalar_vector<size_t>(ctx);
+  const auto nbytes_total = argument::get_next_scalar<size_t>(ctx);
+  const bool read_header  = argument::get_next_scalar<bool>(ctx);
+  auto output             = argument::get_next_output<PhysicalTable>(ctx);
+  argument::get_parallel_launch_task(ctx);
+  (void)nbytes;
+  (void)nbytes_total;
+  (void)column_names;
+
+  auto ocols = output.release();
+  auto [first_file, nfiles] =
+    legate::dataframe::evenly_partition_work(file_paths.size(), static_cast<size_t>(ctx.rank),
+                                             static_cast<size_t>(ctx.nranks));
+  if (nfiles == 0) {
+    for (auto& c : ocols) c.bind_empty_data();
+    return;
+  }
+  std::ifstream in(file_paths[first_file], std::ios::binary);
+  const std::vector<char> bytes((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+  TaskMemoryResource& mr = *ctx.mr();
+  void* text             = mr.allocate(bytes.size() + 16, ctx.stream());  // 16-byte aligned legate buffer
+  cudaMemcpyAsync(text, bytes.data(), bytes.size(), cudaMemcpyHostToDevice, ctx.stream());
+  // Arrow's default null spellings (ConvertOptions::null_values), NUL-separated
+  static const char kNulls[] =
+    "\0#N/A\0#N/A N/A\0#NA\0-1.#IND\0-1.#QNAN\0-NaN\0-nan\0001.#IND\0001.#QNAN\0N/A\0NA\0NULL\0NaN\0n/a\0nan\0null";
+  std::vector<int32_t> types;
+  for (auto& c : ocols) types.push_back(ldf_type_of(c));
+  std::vector<ldf_column> res(ocols.size());
+  int64_t nrows       = 0;
+  ldf_allocator alloc = task_allocator(ctx);
+  ldf_check(ldf_b200_csv_read(static_cast<const uint8_t*>(text), static_cast<int64_t>(bytes.size()), delimiter,
+                              read_header ? 1 : 0, use_cols.data(), types.data(), static_cast<int32_t>(types.size()),
+                              kNulls, na_filter ? static_cast<int32_t>(sizeof(kNulls)) : 0, na_filter ? 17 : 0,
+                              res.data(), &nrows, &alloc, ctx.stream()));
+  mr.deallocate(text, bytes.size() + 16, ctx.stream());
+  bind_outputs(ocols, res, ctx);
 }
 
 }  // namespace ldf_integration
