@@ -219,6 +219,40 @@ int ldf_b200_csv_read(const uint8_t* text, int64_t nbytes, char delimiter, int32
                       const char* nulls, int32_t nulls_bytes, int32_t n_nulls,
                       ldf_column* out, int64_t* nrows, const ldf_allocator* alloc, void* stream);
 
+/* ---- Parquet pages -> columns, decoded on the device ------------------------ */
+/* Replaces cudf::io::read_parquet in ParquetRead::gpu_variant
+ * (parquet.cu:48-101).  The caller walks the file's metadata and page headers
+ * (Thrift, small) and passes one entry per page; the pages' bytes are decoded
+ * on the device from `file` (the whole file, in device memory).  Flat columns
+ * only (max repetition level 0, max definition level 0 or 1). */
+enum { LDF_PQ_DICT_PAGE = 0, LDF_PQ_DATA_V1 = 1, LDF_PQ_DATA_V2 = 2 };
+enum { LDF_PQ_UNCOMPRESSED = 0, LDF_PQ_SNAPPY = 1 };
+/* Parquet physical types used */
+enum { LDF_PQ_BOOLEAN = 0, LDF_PQ_INT32 = 1, LDF_PQ_INT64 = 2, LDF_PQ_FLOAT = 4, LDF_PQ_DOUBLE = 5,
+       LDF_PQ_BYTE_ARRAY = 6 };
+typedef struct {
+  int64_t offset;       /* first byte of the page's payload in `file` (after its header) */
+  int64_t compressed;   /* payload bytes in the file */
+  int64_t uncompressed; /* payload bytes once decompressed */
+  int64_t row0;         /* data pages: first row of the page in its column */
+  int32_t num_values;   /* values in the page, nulls included */
+  int32_t kind;         /* LDF_PQ_* page kind */
+  int32_t encoding;     /* Parquet Encoding of the values (0 PLAIN, 2/8 dictionary indices) */
+  int32_t codec;        /* LDF_PQ_UNCOMPRESSED / LDF_PQ_SNAPPY */
+  int32_t levels_bytes; /* v2 data pages: definition-level bytes at the payload's start, never compressed */
+  int32_t dict;         /* data pages: index of the chunk's dictionary page in `pages`, -1 none */
+  int32_t column;       /* output column */
+  int32_t reserved;
+} ldf_parquet_page;
+/* Columns: `physical[j]` (LDF_PQ_*), output type `types[j]` (the integer
+ * types narrow INT32/INT64 values), `nullable[j]` (max definition level 1),
+ * `nrows` rows each.  Outputs are nullable exactly when `nullable[j]`. */
+int ldf_b200_parquet_decode(const uint8_t* file, int64_t file_bytes,
+                            const ldf_parquet_page* pages, int32_t npages,
+                            const int32_t* physical, const int32_t* types, const int32_t* nullable,
+                            int32_t ncols, int64_t nrows,
+                            ldf_column* out, const ldf_allocator* alloc, void* stream);
+
 /* ---- test hook: a bounded wait that runs out ------------------------------ */
 /* No counterpart in the reference (its waits are inside libcudf).  Runs the
  * library's look-back scan kernel as one block that takes the second tile of

@@ -34,6 +34,7 @@ SOURCES = [
     "distinct.cu",
     "ingest.cu",
     "csv.cu",
+    "parquet.cu",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

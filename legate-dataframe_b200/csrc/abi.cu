@@ -20,6 +20,9 @@ void arrow_offsets_to_ranges(const void* offsets, int offset_bytes, int64_t n, l
 void csv_read(const uint8_t* text, int64_t n, char delimiter, int skip_first, const int32_t* fields,
               const int32_t* types, int ncols, const char* nulls, int nulls_bytes, int n_nulls, ldf_column* out,
               int64_t* nrows, const OpContext& ctx);
+void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_page* pages, int npages,
+                    const int32_t* physical, const int32_t* types, const int32_t* nullable, int ncols, int64_t nrows,
+                    ldf_column* out, const OpContext& ctx);
 }  // namespace ldf
 
 namespace {
@@ -151,6 +154,18 @@ int ldf_b200_csv_read(const uint8_t* text, int64_t nbytes, char delimiter, int32
     ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
     ldf::csv_read(text, nbytes, delimiter, skip_first != 0, fields, types, ncols, nulls, nulls_bytes, n_nulls, out,
                   nrows, ctx);
+  });
+}
+
+int ldf_b200_parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_page* pages, int32_t npages,
+                            const int32_t* physical, const int32_t* types, const int32_t* nullable, int32_t ncols,
+                            int64_t nrows, ldf_column* out, const ldf_allocator* alloc, void* stream)
+{
+  return guarded([&] {
+    LDF_REQUIRE(physical != nullptr && types != nullptr && nullable != nullptr && out != nullptr,
+                "parquet_decode: null argument");
+    ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
+    ldf::parquet_decode(file, file_bytes, pages, npages, physical, types, nullable, ncols, nrows, out, ctx);
   });
 }
 

@@ -82,6 +82,19 @@ class ldf_allocator(ctypes.Structure):
     _fields_ = [("ctx", ctypes.c_void_p), ("allocate", ALLOC_FN), ("deallocate", DEALLOC_FN)]
 
 
+# Parquet page table (ldf_b200_parquet_decode)
+LDF_PQ_DICT_PAGE, LDF_PQ_DATA_V1, LDF_PQ_DATA_V2 = 0, 1, 2
+LDF_PQ_UNCOMPRESSED, LDF_PQ_SNAPPY = 0, 1
+LDF_PQ_BOOLEAN, LDF_PQ_INT32, LDF_PQ_INT64, LDF_PQ_FLOAT, LDF_PQ_DOUBLE, LDF_PQ_BYTE_ARRAY = 0, 1, 2, 4, 5, 6
+
+
+class ldf_parquet_page(ctypes.Structure):
+    _fields_ = [("offset", ctypes.c_int64), ("compressed", ctypes.c_int64), ("uncompressed", ctypes.c_int64),
+                ("row0", ctypes.c_int64), ("num_values", ctypes.c_int32), ("kind", ctypes.c_int32),
+                ("encoding", ctypes.c_int32), ("codec", ctypes.c_int32), ("levels_bytes", ctypes.c_int32),
+                ("dict", ctypes.c_int32), ("column", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 class ldf_aggregation(ctypes.Structure):
     _fields_ = [
         ("in_col", ctypes.c_int32),
@@ -155,6 +168,12 @@ def lib():
                 P(ldf_column), ctypes.POINTER(ctypes.c_int64), P(ldf_allocator), ctypes.c_void_p,
             ]
             L.ldf_b200_csv_read.restype = ctypes.c_int
+            L.ldf_b200_parquet_decode.argtypes = [
+                ctypes.c_void_p, ctypes.c_int64, P(ldf_parquet_page), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.c_int64,
+                P(ldf_column), P(ldf_allocator), ctypes.c_void_p,
+            ]
+            L.ldf_b200_parquet_decode.restype = ctypes.c_int
             L.ldf_b200_arrow_bits_to_bytes.restype = ctypes.c_int
             L.ldf_b200_arrow_offsets_to_ranges.restype = ctypes.c_int
             L.ldf_b200_launch_count.restype = ctypes.c_ulonglong

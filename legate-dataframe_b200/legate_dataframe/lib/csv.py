@@ -19,7 +19,6 @@ import ctypes
 import io
 import os
 import pathlib
-from concurrent.futures import ThreadPoolExecutor, as_completed
 
 import numpy as np
 import pyarrow as pa
@@ -29,7 +28,7 @@ import torch
 from legate_dataframe import _native as N
 from legate_dataframe.lib.core.column import LogicalColumn, ldf_type_of
 from legate_dataframe.lib.core.table import LogicalTable
-from legate_dataframe.lib.parquet import _file_list
+from legate_dataframe.lib.parquet import _file_list, _file_to_device
 
 
 def _parsed_on_device(t: pa.DataType) -> bool:
@@ -86,45 +85,10 @@ def _header_names(path, delimiter: str) -> list[str]:
     return pacsv.read_csv(io.BytesIO(rec + b"\n"), parse_options=pacsv.ParseOptions(delimiter=delimiter)).schema.names
 
 
-_READ_PIECE = 64 << 20  # bytes per read (and per host-to-device copy) of a large file
-
-
-def _file_to_device(path, dev) -> tuple[torch.Tensor, int]:
-    """The file's bytes on the device.  Large files are read in 64 MB pieces
-    by a few threads into pinned memory, each piece copied to the device as
-    soon as it has been read, so the reads and the copies overlap."""
-    size = os.path.getsize(path)
-    host = torch.empty(max(size, 16), dtype=torch.uint8, pin_memory=True)
-    text = torch.empty(max(size, 16), dtype=torch.uint8, device=dev)
-    if size == 0:
-        return text, 0
-    mv = memoryview(host.numpy())
-    pieces = [(a, min(a + _READ_PIECE, size)) for a in range(0, size, _READ_PIECE)]
-
-    def read(piece):
-        a, b = piece
-        with open(path, "rb") as f:
-            f.seek(a)
-            got = f.readinto(mv[a:b])
-        if got != b - a:
-            raise OSError(f"short read of {path}")
-        return piece
-
-    if len(pieces) == 1:
-        read(pieces[0])
-        text[:size].copy_(host[:size], non_blocking=True)
-    else:
-        with ThreadPoolExecutor(max_workers=min(8, len(pieces))) as ex:
-            for fut in as_completed([ex.submit(read, pc) for pc in pieces]):
-                a, b = fut.result()
-                text[a:b].copy_(host[a:b], non_blocking=True)
-    return text, size
-
-
 def _read_file_device(path, fields, types, header: bool, na_filter: bool, delimiter: str) -> list[LogicalColumn]:
     dev = N.require_cuda()
     L = N.lib()
-    text, size = _file_to_device(path, dev)
+    _, text, size = _file_to_device(path, dev)
     nulls = _NULL_SPELLINGS if na_filter else []
     blob = b"".join(s.encode() + b"\0" for s in nulls)
     ldf_types = [ldf_type_of(t) for t in types]
