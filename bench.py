@@ -13,12 +13,13 @@ At N=1 the same JSON line also carries
     (int32 keys, 5% null probe keys, Zipf(0.9) hits);
   * `strings`: 100M string-key rows: groupby SUM/COUNT(*), stable sort
     (key asc, ts desc), hash_partition into 256 buckets;
-  * `csv`: csv_read of a 4M-row CSV file of the string workload's shape on
-    the device reader, against Arrow's CSV reader on the host;
+  * `csv` / `parquet`: csv_read / parquet_read of a 4M-row file of the
+    string workload's shape on the device readers, against Arrow's readers on
+    the host;
   * `served`: the batched/served mix (8,192 small joins and groupbys arriving
     at 2,000 req/s) through the continuous-batching server and, for
     comparison, the same requests issued one op per launch.
-(--no-joins / --no-strings / --no-csv / --no-served skip them.)
+(--no-joins / --no-strings / --no-csv (both files) / --no-served skip them.)
 
 `--workload join|strings|sort|ingest` instead prints one line per op.
 
@@ -626,6 +627,60 @@ def csv_record(n: int, steps: int = 3) -> dict:
             "parity": parity, "timing": "host wall clock, median, device synchronized; file in the page cache"}
 
 
+def parquet_record(n: int, steps: int = 3) -> dict:
+    """parquet_read of an n-row Parquet file of the string workload's shape
+    (Arrow's writer defaults: Snappy, dictionary pages, page cache warm): the
+    device decoder end to end (file -> pinned memory -> device -> decoded
+    columns), its kernels, and the reference's CPU reader on the same file
+    (Arrow read_table with one thread, and with all host threads); parity
+    against Arrow."""
+    import pyarrow.parquet as pq
+    import torch
+
+    from legate_dataframe import _native as N
+    from legate_dataframe.lib.parquet import parquet_read
+
+    t = _string_workload_table(n)
+
+    def wall(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+            del r
+        return statistics.median(ts)
+
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "t.parquet")
+        pq.write_table(t, path)
+        size = os.path.getsize(path)
+        dev_s = wall(lambda: parquet_read(path))
+        N.profile_enable(True)
+        N.profile_report(reset=True)
+        got = parquet_read(path)
+        torch.cuda.synchronize()
+        prof = N.profile_report(reset=True)
+        N.profile_enable(False)
+        one = wall(lambda: pq.read_table(path, use_threads=False))
+        allt = wall(lambda: pq.read_table(path))
+        parity = "ok" if got.to_arrow().equals(pq.read_table(path)) else "MISMATCH"
+    kernel_ms = sum(v[1] for v in prof.values())
+    out_bytes = sum(c.size * N.TYPE_WIDTH[c.ldf_type] + (c.size if c.valid is not None else 0) + (c.num_chars or 0)
+                    for c in got.get_columns())
+    return {"op": f"parquet_read: {n} rows, {size} bytes of Parquet (Snappy, dictionary pages; string key, "
+                  "nullable int64, float32)",
+            "ms": round(dev_s * 1e3, 3), "rows_per_s": n / dev_s, "file_GBps": size / dev_s / 1e9,
+            "kernel_ms": round(kernel_ms, 3), "output_bytes": out_bytes,
+            "kernels_ms": {k: [c, round(ms, 4)] for k, (c, ms) in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "arrow_1_thread_ms": round(one * 1e3, 3), "arrow_all_threads_ms": round(allt * 1e3, 3),
+            "host_threads": host_cores(), "vs_arrow_1_thread": one / dev_s, "vs_arrow_all_threads": allt / dev_s,
+            "parity": parity, "timing": "host wall clock, median, device synchronized; file in the page cache"}
+
+
 def run_ingest_workload(args):
     """--rows (default 20M) rows as a host Arrow table shaped like the string
     workload (string key from a 2M-entry dictionary, 10% null int64 ts,
@@ -683,6 +738,7 @@ def run_ingest_workload(args):
                           "arrow_GBps": arrow_bytes / (ms / 1e3) / 1e9, "arrow_bytes": arrow_bytes,
                           "timing": "host wall clock, median, device synchronized"}), flush=True)
     print(json.dumps(csv_record(n, steps)), flush=True)
+    print(json.dumps(parquet_record(n, steps)), flush=True)
     return 0
 
 
@@ -866,10 +922,12 @@ def main():
     if joins is not None:
         parity["joins"] = "ok" if all(r.get("parity") == "ok" for r in joins) else "MISMATCH"
 
-    csv = None
+    csv = parquet = None
     if rank == 0 and world == 1 and not args.no_csv:
         csv = csv_record(4_000_000)
         parity["csv"] = csv["parity"]
+        parquet = parquet_record(4_000_000)
+        parity["parquet"] = parquet["parity"]
 
     # ---- served mix (rank 0, N=1 only) --------------------------------------
     served = None
@@ -909,6 +967,7 @@ def main():
         "joins": joins,
         "strings": strings,
         "csv": csv,
+        "parquet": parquet,
         "served": served,
     }
     print(json.dumps(line))

@@ -247,6 +247,19 @@ typedef struct {
 /* Columns: `physical[j]` (LDF_PQ_*), output type `types[j]` (the integer
  * types narrow INT32/INT64 values), `nullable[j]` (max definition level 1),
  * `nrows` rows each.  Outputs are nullable exactly when `nullable[j]`. */
+/* The page table of column chunks, from their page headers (Thrift compact
+ * protocol) in host memory: chunk k spans `chunk_bytes[k]` bytes of
+ * `file_host` from `chunk_start[k]` (its dictionary page, else its first data
+ * page), holds rows from `chunk_row0[k]` of output column
+ * `chunk_column[k]`, with codec `chunk_codec[k]` (LDF_PQ_*) and physical type
+ * `chunk_physical[k]`.  With `pages` NULL only *npages is set (the count);
+ * otherwise at most `max_pages` entries are written.  Pages the decoder
+ * cannot take (another encoding, repetition levels) fail with
+ * LDF_ERR_UNSUPPORTED.  Host memory only; no device work. */
+int ldf_b200_parquet_pages(const uint8_t* file_host, int64_t file_bytes, const int64_t* chunk_start,
+                           const int64_t* chunk_bytes, const int64_t* chunk_row0, const int32_t* chunk_column,
+                           const int32_t* chunk_codec, const int32_t* chunk_physical, int32_t nchunks,
+                           ldf_parquet_page* pages, int32_t max_pages, int32_t* npages);
 int ldf_b200_parquet_decode(const uint8_t* file, int64_t file_bytes,
                             const ldf_parquet_page* pages, int32_t npages,
                             const int32_t* physical, const int32_t* types, const int32_t* nullable,

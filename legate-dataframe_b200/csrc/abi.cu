@@ -20,6 +20,9 @@ void arrow_offsets_to_ranges(const void* offsets, int offset_bytes, int64_t n, l
 void csv_read(const uint8_t* text, int64_t n, char delimiter, int skip_first, const int32_t* fields,
               const int32_t* types, int ncols, const char* nulls, int nulls_bytes, int n_nulls, ldf_column* out,
               int64_t* nrows, const OpContext& ctx);
+void parquet_pages(const uint8_t* file, int64_t file_bytes, const int64_t* chunk_start, const int64_t* chunk_bytes,
+                   const int64_t* chunk_row0, const int32_t* chunk_column, const int32_t* chunk_codec,
+                   const int32_t* chunk_physical, int nchunks, ldf_parquet_page* pages, int max_pages, int* npages);
 void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_page* pages, int npages,
                     const int32_t* physical, const int32_t* types, const int32_t* nullable, int ncols, int64_t nrows,
                     ldf_column* out, const OpContext& ctx);
@@ -154,6 +157,19 @@ int ldf_b200_csv_read(const uint8_t* text, int64_t nbytes, char delimiter, int32
     ldf::OpContext ctx(alloc, static_cast<cudaStream_t>(stream));
     ldf::csv_read(text, nbytes, delimiter, skip_first != 0, fields, types, ncols, nulls, nulls_bytes, n_nulls, out,
                   nrows, ctx);
+  });
+}
+
+int ldf_b200_parquet_pages(const uint8_t* file_host, int64_t file_bytes, const int64_t* chunk_start,
+                           const int64_t* chunk_bytes, const int64_t* chunk_row0, const int32_t* chunk_column,
+                           const int32_t* chunk_codec, const int32_t* chunk_physical, int32_t nchunks,
+                           ldf_parquet_page* pages, int32_t max_pages, int32_t* npages)
+{
+  return guarded([&] {
+    int n = 0;
+    ldf::parquet_pages(file_host, file_bytes, chunk_start, chunk_bytes, chunk_row0, chunk_column, chunk_codec,
+                       chunk_physical, nchunks, pages, max_pages, &n);
+    *npages = n;
   });
 }
 

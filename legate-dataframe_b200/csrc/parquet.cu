@@ -5,11 +5,12 @@
 // The caller walks the footer and the page headers (Thrift, a few bytes per
 // page) and hands over one entry per page; the whole file is in device
 // memory.  Then:
-// 1. Snappy pages are decompressed, one warp per page: every lane parses the
-//    same element tags (broadcast loads), the warp copies the element's bytes
-//    together (a back-reference of offset d repeats its last d bytes, so
-//    byte k of it is dst[o - d + k % d] and all of it copies at once).
-// 2. Dictionary pages of byte arrays get an entry table (offset, length).
+// 1. Snappy pages are decompressed, one warp per page, with the compressed
+//    stream staged and the recent output kept in shared memory; every lane
+//    parses the same element tags and the warp copies each element's bytes
+//    together.
+// 2. Dictionary pages of byte arrays get an entry table (offset, length),
+//    one block per page walking the length prefixes from shared memory.
 // 3. One block per data page decodes its rows in tiles of kPqTile: thread 0
 //    cuts the next tile out of the RLE / bit-packed hybrid streams (the
 //    definition levels, the dictionary indices) as a list of run segments,
@@ -18,6 +19,8 @@
 //    index; PLAIN values are read at that index, dictionary values through
 //    the decoded index, and byte arrays by a walk of their length prefixes.
 // 4. String columns: lengths -> offsets (scan) -> characters copied.
+#include <algorithm>
+
 #include "scan.cuh"
 #include "table_ops.cuh"
 
@@ -51,59 +54,378 @@ __device__ __forceinline__ uint32_t le_bytes(const uint8_t* p, int n)
 }
 
 // ---- 1. Snappy ------------------------------------------------------------------
-// src[0, n) -> dst (at most cap bytes) by the calling warp; false when the
-// stream is malformed.  Every lane parses the same tags.
-__device__ bool snappy_warp(const uint8_t* src, int64_t n, uint8_t* dst, int64_t cap, int64_t& produced)
+// One warp per page.  The compressed stream is staged kSnapIn bytes at a time
+// in shared memory (16-byte granules loaded by all lanes), and the last
+// kSnapWin output bytes are kept in a shared ring, so tag parsing and most
+// back-references run at shared-memory latency; the output goes to global
+// memory as it is produced.
+// One warp per block: the 32 KB ring covers all but a few back-references
+// (Snappy's offsets stay below 64 KB) and six such blocks fit an SM.
+constexpr int kSnapIn    = 2048;   // staged compressed bytes per warp
+constexpr int kSnapWin   = 32768;  // output ring per warp (a power of two, a multiple of 32)
+
+constexpr int kSnapBatch      = 32;    // short elements decoded together
+constexpr int kSnapBatchBytes = 1024;  // output bytes of a batch at most
+constexpr int kSnapShort      = 64;    // longer literals are copied on their own
+constexpr int kSnapPerLane    = 4;     // output bytes per lane per window of a batch
+
+struct alignas(16) SnapShared {
+  uint8_t in[kSnapIn];
+  uint8_t win[kSnapWin];
+  uint16_t size[kSnapIn];         // input bytes of an element whose tag is at in[x] (0xffff: unknown)
+  uint8_t elem[kSnapBatchBytes];  // batch element of each output byte
+  int64_t off[kSnapBatch];        // copy: offset
+  int32_t epos[kSnapBatch];       // staged index of the element's tag
+  int32_t rstart[kSnapBatch];     // first output byte in the batch
+  int32_t len[kSnapBatch];        // output bytes (kSnapBatchBytes + 1 for longer literals)
+  int32_t src[kSnapBatch];        // literal: staged index of its first byte; copy: -1
+  int32_t flags[kSnapBatch];      // 1: malformed on its own, 2: short enough for a batch
+  int32_t cut, bad;
+};
+
+struct SnapStage {
+  const uint8_t* src;
+  int64_t n;
+  int64_t ib;  // stream index of in[0] (negative before a misaligned start)
+  bool sized;  // size[] describes the staged bytes
+};
+
+__device__ __forceinline__ void copy16(uint8_t* dst, const uint8_t* src)
+{
+#ifdef __CUDA_ARCH__
+  *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(src);
+#else
+  for (int k = 0; k < 16; ++k) dst[k] = src[k];
+#endif
+}
+
+// One element's tag: t and the four bytes after it (x).
+struct SnapElem {
+  int hdr;      // tag bytes
+  int64_t l;    // output bytes
+  int64_t off;  // copy: offset
+  bool literal;
+};
+
+__device__ __forceinline__ SnapElem snap_decode(uint32_t t, uint32_t x)
+{
+  SnapElem e{1, 0, 0, (t & 3) == 0};
+  if (e.literal) {
+    e.l = t >> 2;
+    if (e.l >= 60) {
+      const int nbytes = static_cast<int>(e.l) - 59;
+      e.hdr += nbytes;
+      e.l = nbytes == 4 ? x : (x & ((1u << (8 * nbytes)) - 1));
+    }
+    e.l += 1;
+  } else if ((t & 3) == 1) {
+    e.hdr = 2;
+    e.l   = 4 + ((t >> 2) & 7);
+    e.off = (static_cast<int64_t>(t >> 5) << 8) | (x & 0xff);
+  } else {
+    const bool two = (t & 3) == 2;
+    e.hdr = two ? 3 : 5;
+    e.l   = (t >> 2) + 1;
+    e.off = two ? (x & 0xffff) : x;
+  }
+  return e;
+}
+
+// The tag at staged index r and the four bytes after it (r + 5 <= kSnapIn).
+__device__ __forceinline__ SnapElem snap_at(const SnapShared& sh, int r)
+{
+  const uint8_t* q = sh.in + r;
+  const uint32_t x = static_cast<uint32_t>(q[1]) | static_cast<uint32_t>(q[2]) << 8 |
+                     static_cast<uint32_t>(q[3]) << 16 | static_cast<uint32_t>(q[4]) << 24;
+  return snap_decode(q[0], x);
+}
+
+__device__ __forceinline__ uint32_t load_u32(const uint8_t* p)  // p 4-byte aligned
+{
+#ifdef __CUDA_ARCH__
+  return *reinterpret_cast<const uint32_t*>(p);
+#else
+  uint32_t v;
+  memcpy(&v, p, 4);
+  return v;
+#endif
+}
+
+// Input bytes of an element whose tag is t, followed by the bytes x (capped at 0xffff).
+// Branch-free: every lane of the warp takes the same path.
+__device__ __forceinline__ uint32_t snap_size(uint32_t t, uint32_t x)
+{
+  const uint32_t type = t & 3, L = t >> 2;
+  const uint32_t copy = (0x05030200u >> (8 * type)) & 0xff;  // 2, 3, 5 bytes of tag
+  const uint32_t nbytes = L >= 60 ? L - 59 : 1;               // extra length bytes (1..4)
+  const uint32_t mask   = nbytes == 4 ? 0xffffffffu : (1u << (8 * nbytes)) - 1;
+  const uint32_t big    = (x & mask) >= 0xfff0u ? 0xffffu : 2 + nbytes + (x & mask);  // 1 + nbytes + (len + 1)
+  const uint32_t lit    = L < 60 ? L + 2 : big;
+  return type != 0 ? copy : lit;
+}
+
+// size[] of the staged bytes: every position read as a tag, in parallel,
+// four positions from two aligned words at a time.
+__device__ void snap_sizes(SnapStage& st, SnapShared& sh)
 {
   const int lane = threadIdx.x % kLanes;
-  int64_t i      = 0;
-  uint64_t len   = 0;
-  for (int sh = 0;; sh += 7) {  // preamble: the uncompressed length as a varint
-    if (i >= n || sh > 35) return false;
-    const uint8_t b = src[i++];
-    len |= static_cast<uint64_t>(b & 0x7f) << sh;
+#pragma unroll 2
+  for (int w = lane; w < kSnapIn / 4; w += kLanes) {
+    const uint32_t lo = load_u32(sh.in + 4 * w);
+    const uint32_t hi = w + 1 < kSnapIn / 4 ? load_u32(sh.in + 4 * w + 4) : 0;
+    const uint64_t v  = static_cast<uint64_t>(hi) << 32 | lo;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int r = 4 * w + k;
+      const uint32_t t = static_cast<uint32_t>(v >> (8 * k)) & 0xff;
+      const uint32_t x = static_cast<uint32_t>(v >> (8 * k + 8));
+      sh.size[r] = static_cast<uint16_t>(r + 5 <= kSnapIn ? snap_size(t, x) : 0xffff);
+    }
+  }
+  st.sized = true;
+  __syncwarp();
+}
+
+// Stages the stream from the 16-byte boundary at or below stream index i:
+// in[k] = src[ib + k] for the indices inside [0, n); with `sizes`, size[]
+// too.
+__device__ void snap_stage(SnapStage& st, SnapShared& sh, int64_t i, bool sizes)
+{
+  const int lane = threadIdx.x % kLanes;
+  const int64_t ib = i - static_cast<int64_t>(reinterpret_cast<uintptr_t>(st.src + i) & 15);
+  constexpr int kPer = kSnapIn / 16 / kLanes;  // granules per lane
+  struct alignas(16) Granule {
+    uint8_t b[16];
+  } reg[kPer];
+  for (int r = 0; r < kPer; ++r) {  // all loads first, then the stores
+    const int64_t b = ib + 16 * (lane + r * kLanes);
+    if (b >= 0 && b + 16 <= st.n) {
+      copy16(reg[r].b, st.src + b);
+    } else {
+      for (int k = 0; k < 16; ++k) reg[r].b[k] = b + k >= 0 && b + k < st.n ? st.src[b + k] : 0;
+    }
+  }
+  __syncwarp();  // every lane is done with the previous contents
+  st.ib    = ib;
+  st.sized = false;
+  for (int r = 0; r < kPer; ++r) copy16(sh.in + 16 * (lane + r * kLanes), reg[r].b);
+  __syncwarp();
+  if (sizes) snap_sizes(st, sh);
+}
+
+// src[0, n) -> dst (at most cap bytes) by the calling warp; false when the
+// stream is malformed.  The stream is a chain of elements (literals and
+// back-references) whose boundaries are known only by parsing them in turn.
+// Per batch of up to kSnapBatch short elements: the warp walks the chain
+// through size[] (one shared load per element; the sizes of every staged
+// position were tabulated in parallel), each lane decodes one element, and
+// the batch's output bytes are produced all at once: byte r of the batch is
+// a literal's input byte, or a back-reference's source byte -- at
+// out[o - d + k % d] for byte k of a copy of offset d -- followed back
+// through the batch until it reaches a literal or output written before the
+// batch (ring or global).  Long literals are copied on their own.
+__device__ bool snappy_warp(const uint8_t* src, int64_t n, uint8_t* dst, int64_t cap, int64_t& produced,
+                            SnapShared& sh)
+{
+  const int lane = threadIdx.x % kLanes;
+  SnapStage st{src, n, 0, false};
+  snap_stage(st, sh, 0, false);
+  int64_t i    = 0;
+  uint64_t len = 0;
+  for (int sh_ = 0;; sh_ += 7) {  // preamble: the uncompressed length as a varint
+    if (i >= n || sh_ > 35) return false;
+    const uint8_t b = sh.in[i++ - st.ib];
+    len |= static_cast<uint64_t>(b & 0x7f) << sh_;
     if (!(b & 0x80)) break;
   }
   if (len > static_cast<uint64_t>(cap)) return false;
+  const int64_t total = static_cast<int64_t>(len);
+  constexpr int64_t kMask = kSnapWin - 1;
   int64_t o = 0;
-  while (o < static_cast<int64_t>(len)) {
+  while (o < total) {
     if (i >= n) return false;
-    const uint32_t t = src[i++];
-    int64_t l;
-    if ((t & 3) == 0) {  // literal
-      l = t >> 2;
-      if (l >= 60) {
-        const int nb = static_cast<int>(l) - 59;
-        if (i + nb > n) return false;
-        l = le_bytes(src + i, nb);
-        i += nb;
-      }
-      l += 1;
-      if (i + l > n || o + l > static_cast<int64_t>(len)) return false;
-      for (int64_t k = lane; k < l; k += kLanes) dst[o + k] = src[i + k];
-      i += l;
-    } else {  // back-reference
-      int64_t off;
-      if ((t & 3) == 1) {
-        if (i >= n) return false;
-        l   = 4 + ((t >> 2) & 7);
-        off = (static_cast<int64_t>(t >> 5) << 8) | src[i++];
-      } else {
-        const int nb = (t & 3) == 2 ? 2 : 4;
-        if (i + nb > n) return false;
-        l   = (t >> 2) + 1;
-        off = le_bytes(src + i, nb);
-        i += nb;
-      }
-      if (off == 0 || off > o || o + l > static_cast<int64_t>(len)) return false;
-      for (int64_t k = lane; k < l; k += kLanes) dst[o + k] = dst[o - off + k % off];
+    if (i + 5 > st.ib + kSnapIn) snap_stage(st, sh, i, true);  // a tag and its extra bytes
+    else if (!st.sized) snap_sizes(st, sh);
+    // walk the chain (every lane the same)
+    int nb = 0, r = static_cast<int>(i - st.ib);
+    while (nb < kSnapBatch && st.ib + r < n && r + 5 <= kSnapIn) {
+      if (lane == 0) sh.epos[nb] = r;
+      ++nb;
+      r += sh.size[r];
     }
-    o += l;
-    __syncwarp();  // the next element may read these bytes
+    const int walk_end = r;
+    if (lane == 0) {
+      sh.cut = nb;
+      sh.bad = kSnapBatch;
+    }
+    __syncwarp();
+    // decode, one element per lane
+    for (int j = lane; j < nb; j += kLanes) {
+      const int er      = sh.epos[j];
+      const SnapElem e  = snap_at(sh, er);
+      const int64_t body = st.ib + er + e.hdr;  // stream index
+      bool alone_bad = body > n;
+      bool is_short  = true;
+      if (e.literal) {
+        alone_bad = alone_bad || body + e.l > n;
+        is_short  = e.l <= kSnapShort && body + e.l <= st.ib + kSnapIn;
+      } else {
+        alone_bad = alone_bad || e.off == 0;
+      }
+      sh.len[j]   = static_cast<int32_t>(e.l > kSnapBatchBytes ? kSnapBatchBytes + 1 : e.l);
+      sh.src[j]   = e.literal ? er + e.hdr : -1;
+      sh.off[j]   = e.off;
+      sh.flags[j] = (alone_bad ? 1 : 0) | (is_short ? 2 : 0);
+    }
+    __syncwarp();
+    // output positions; the batch ends before the first element that is past
+    // the end, long, or does not fit
+    int cut, first_bad;
+    if (kLanes == 32) {  // one element per lane: a shuffle scan and ballots
+      const int lj = lane < nb ? sh.len[lane] : 0;
+      int incl     = lj;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += u;
+      }
+      const int rs     = incl - lj;
+      const int64_t at = o + rs;
+      bool stop = false, bad = false;
+      if (lane < nb) {
+        sh.rstart[lane] = rs;
+        const int fl    = sh.flags[lane];
+        const bool end  = at >= total;
+        stop            = end || !(fl & 2) || rs + lj > kSnapBatchBytes;
+        bad             = !end && ((fl & 1) || at + lj > total || (sh.src[lane] < 0 && sh.off[lane] > at));
+      }
+      const unsigned sm = __ballot_sync(0xffffffffu, stop), bm = __ballot_sync(0xffffffffu, bad);
+      cut       = sm ? __ffs(sm) - 1 : nb;
+      first_bad = bm ? __ffs(bm) - 1 : kSnapBatch;
+    } else {
+      for (int j = lane; j < nb; j += kLanes) {
+        int rs = 0;
+        for (int k = 0; k < j; ++k) rs += sh.len[k];
+        sh.rstart[j]     = rs;
+        const int64_t at = o + rs;
+        const int lj     = sh.len[j];
+        const int fl     = sh.flags[j];
+        const bool end   = at >= total;
+        const bool stop  = end || !(fl & 2) || rs + lj > kSnapBatchBytes;
+        const bool bad   = !end && ((fl & 1) || at + lj > total || (sh.src[j] < 0 && sh.off[j] > at));
+        if (stop) atomicMin(&sh.cut, j);
+        if (bad) atomicMin(&sh.bad, j);
+      }
+      __syncwarp();
+      cut       = sh.cut;
+      first_bad = sh.bad;
+    }
+    __syncwarp();
+    if (first_bad < cut) return false;
+    if (cut == 0) {  // a long literal (or one past the staged bytes), straight from the input
+      const SnapElem e   = snap_at(sh, static_cast<int>(i - st.ib));
+      const int64_t body = i + e.hdr;
+      if (body > n || body + e.l > n || o + e.l > total) return false;
+      int64_t from_i = body;
+      for (int64_t done = 0; done < e.l;) {
+        if (from_i >= st.ib + kSnapIn) snap_stage(st, sh, from_i, false);
+        const int64_t piece = e.l - done < st.ib + kSnapIn - from_i ? e.l - done : st.ib + kSnapIn - from_i;
+        const uint8_t* from = sh.in + (from_i - st.ib);
+        const int64_t at    = o + done;
+#pragma unroll 4
+        for (int64_t k = lane; k < piece; k += kLanes) {
+          const uint8_t b          = from[k];
+          dst[at + k]              = b;
+          sh.win[(at + k) & kMask] = b;
+        }
+        done += piece;
+        from_i += piece;
+      }
+      o += e.l;
+      i = from_i;
+      __syncwarp();
+      continue;
+    }
+    const int B = sh.rstart[cut - 1] + sh.len[cut - 1];
+    for (int j = lane; j < cut; j += kLanes) {
+      const int r0 = sh.rstart[j], lj = sh.len[j];
+      for (int k = 0; k < lj; ++k) sh.elem[r0 + k] = static_cast<uint8_t>(j);
+    }
+    __syncwarp();
+    // The batch is written a window of kSnapPerLane * kLanes bytes at a time,
+    // ring included, so a source inside the batch but before the window is
+    // read from the ring and only sources inside the window are followed
+    // back.  A batch writes ring slots of [o, o + B), B <= kSnapBatchBytes;
+    // the slots of positions from o + kSnapBatchBytes - kSnapWin on are not
+    // among them, so those are read from the ring and older ones from dst.
+    for (int base = 0; base < B; base += kSnapPerLane * kLanes) {
+      uint8_t bv[kSnapPerLane];
+      int64_t nrq[kSnapPerLane];
+      bool chase[kSnapPerLane];
+#pragma unroll
+      for (int q = 0; q < kSnapPerLane; ++q) {  // first hop of every byte, side by side
+        const int rb = base + q * kLanes + lane;
+        const int rr = rb < B ? rb : 0;
+        const int e  = sh.elem[rr];
+        const int r0 = sh.rstart[e];
+        const int si = sh.src[e];
+        const int64_t d = sh.off[e];
+        int k = rr - r0;
+        if (si < 0 && d < sh.len[e]) k %= static_cast<int>(d);  // an overlapping copy: d < len <= 64
+        const int64_t nr = si >= 0 ? 0 : r0 - d + k;
+        const bool far   = si < 0 && nr < base;
+        const int64_t at = o + nr;
+        bv[q]    = si >= 0 ? sh.in[si + k] : (far ? (nr >= kSnapBatchBytes - kSnapWin ? sh.win[at & kMask] : dst[at]) : 0);
+        chase[q] = rb < B && si < 0 && !far;
+        nrq[q]   = nr;
+      }
+#pragma unroll
+      for (int q = 0; q < kSnapPerLane; ++q) {
+        if (!chase[q]) continue;
+        int64_t rr = nrq[q];  // a source inside this window: follow it back
+        while (true) {
+          const int e  = sh.elem[rr];
+          const int r0 = sh.rstart[e];
+          const int si = sh.src[e];
+          if (si >= 0) {
+            bv[q] = sh.in[si + (rr - r0)];
+            break;
+          }
+          const int64_t d = sh.off[e];
+          int64_t nr;
+          if (d >= sh.len[e]) nr = rr - d;  // no overlap
+          else nr = r0 - d + static_cast<int>(rr - r0) % static_cast<int>(d);  // d < len <= 64
+          if (nr < base) {
+            const int64_t at = o + nr;
+            bv[q] = nr >= kSnapBatchBytes - kSnapWin ? sh.win[at & kMask] : dst[at];
+            break;
+          }
+          rr = nr;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kSnapPerLane; ++q) {
+        const int rb = base + q * kLanes + lane;
+        if (rb < B) {
+          dst[o + rb]              = bv[q];
+          sh.win[(o + rb) & kMask] = bv[q];
+        }
+      }
+      __syncwarp();  // the next window may read these bytes from the ring
+    }
+    o += B;
+    i = st.ib + (cut < nb ? sh.epos[cut] : walk_end);
+    __syncwarp();  // the next batch reads these bytes and rewrites the descriptors
   }
   produced = o;
   return true;
 }
+
+// ---- 2. byte-array dictionary pages ---------------------------------------------------
+constexpr int kDictStage = 8192;  // staged page bytes per round
+struct alignas(16) DictStage {
+  uint8_t b[kDictStage];
+};
 
 // ---- 3. RLE / bit-packed hybrid streams ----------------------------------------------
 // Streaming state of one hybrid stream of `bw`-bit values in [pos, end).
@@ -204,11 +526,12 @@ __device__ __forceinline__ uint32_t rle_value(const RleStream& s, const RleSeg* 
 // ---- kernels ------------------------------------------------------------------------
 // Compressed pages, one warp each: payload -> scratch (a v2 page's levels are
 // stored uncompressed in front of its values and copied as they are).
-__global__ void __launch_bounds__(kPqThreads) pq_snappy_kernel(const uint8_t* file, PqPage* pages,
-                                                               const int* list, int nlist, uint8_t* scratch,
-                                                               const int64_t* soff, unsigned long long* err)
+__global__ void __launch_bounds__(kLanes) pq_snappy_kernel(const uint8_t* file, PqPage* pages, const int* list,
+                                                          int nlist, uint8_t* scratch, const int64_t* soff,
+                                                          unsigned long long* err)
 {
-  const int w = blockIdx.x * (kPqThreads / kLanes) + threadIdx.x / kLanes;
+  __shared__ SnapShared sm;
+  const int w = blockIdx.x;
   if (w >= nlist) return;
   const int p           = list[w];
   const PqPage& pg      = pages[p];
@@ -218,32 +541,67 @@ __global__ void __launch_bounds__(kPqThreads) pq_snappy_kernel(const uint8_t* fi
   const int lane        = threadIdx.x % kLanes;
   for (int64_t k = lane; k < lv; k += kLanes) dst[k] = src[k];
   int64_t got = 0;
-  const bool ok = snappy_warp(src + lv, pg.h.compressed - lv, dst + lv, pg.h.uncompressed - lv, got);
+  const bool ok = snappy_warp(src + lv, pg.h.compressed - lv, dst + lv, pg.h.uncompressed - lv, got, sm);
   if (lane == 0 && (!ok || got != pg.h.uncompressed - lv)) pq_error(err, p, kPqErrSnappy);
 }
 
-// Byte-array dictionary pages, one thread each: entry (offset in the page's
-// data, length) of every value.
-__global__ void pq_dict_strings_kernel(const PqPage* pages, const int* list, int nlist, int64_t* entry_off,
-                                       int32_t* entry_len, unsigned long long* err)
+// Byte-array dictionary pages, one block each: the entry table (offset in
+// the page's data, length) of every value.  The page is staged kDictStage
+// bytes at a time by the block and thread 0 walks the length prefixes.
+__global__ void __launch_bounds__(kPqThreads) pq_dict_strings_kernel(const PqPage* pages, const int* list,
+                                                                     int nlist, int64_t* entry_off,
+                                                                     int32_t* entry_len, unsigned long long* err)
 {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nlist; q += gridDim.x * blockDim.x) {
-    const int p      = list[q];
-    const PqPage& pg = pages[p];
-    int64_t pos      = 0;
-    for (int v = 0; v < pg.h.num_values; ++v) {
-      int64_t len = -1;
-      if (pos + 4 <= pg.data_bytes) len = le_bytes(pg.data + pos, 4);
-      if (len < 0 || pos + 4 + len > pg.data_bytes) {
-        pq_error(err, p, kPqErrValues);
-        len = 0;
-        pos = pg.data_bytes;
-      } else {
-        pos += 4;
+  __shared__ DictStage stage;
+  __shared__ int64_t s_pos;
+  __shared__ int s_v;
+  for (int q = blockIdx.x; q < nlist; q += gridDim.x) {
+    const int p         = list[q];
+    const PqPage& pg    = pages[p];
+    const uint8_t* data = pg.data;
+    const int64_t bytes = pg.data_bytes;
+    const int nv        = pg.h.num_values;
+    int64_t pos         = 0;
+    int v               = 0;
+    uint8_t* buf        = stage.b;
+    while (v < nv) {
+      const int64_t base = pos - static_cast<int64_t>(reinterpret_cast<uintptr_t>(data + pos) & 15);
+      for (int g = threadIdx.x; g < kDictStage / 16; g += blockDim.x) {
+        const int64_t b = base + 16 * g;
+        if (b >= 0 && b + 16 <= bytes) {
+          copy16(buf + 16 * g, data + b);
+        } else {
+          for (int k = 0; k < 16; ++k)
+            if (b + k >= 0 && b + k < bytes) buf[16 * g + k] = data[b + k];
+        }
       }
-      entry_off[pg.dict_entry0 + v] = pos;
-      entry_len[pg.dict_entry0 + v] = static_cast<int32_t>(len);
-      pos += len;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        while (v < nv) {
+          int64_t len = -1;
+          if (pos + 4 <= bytes) {
+            if (pos + 4 > base + kDictStage) break;  // the next prefix is past the staged bytes
+            len = le_bytes(buf + (pos - base), 4);
+          }
+          if (len < 0 || pos + 4 + len > bytes) {
+            pq_error(err, p, kPqErrValues);
+            len = 0;
+            pos = bytes;
+          } else {
+            pos += 4;
+          }
+          entry_off[pg.dict_entry0 + v] = pos;
+          entry_len[pg.dict_entry0 + v] = static_cast<int32_t>(len);
+          pos += len;
+          ++v;
+        }
+        s_pos = pos;
+        s_v   = v;
+      }
+      __syncthreads();
+      pos = s_pos;
+      v   = s_v;
+      __syncthreads();  // s_pos / s_v and buf are rewritten next round
     }
   }
 }
@@ -539,6 +897,21 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
   }
   for (int j = 0; j < ncols; ++j)
     LDF_REQUIRE(covered[j] == nrows, "parquet_decode: the data pages do not cover every row of a column");
+  {  // decompress the largest pages first: a page is one warp's sequential work
+    std::vector<int> order(snappy.size());
+    for (size_t q = 0; q < order.size(); ++q) order[q] = static_cast<int>(q);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      return pages[snappy[a]].uncompressed > pages[snappy[b]].uncompressed;
+    });
+    std::vector<int> sp(order.size());
+    std::vector<int64_t> so(order.size());
+    for (size_t q = 0; q < order.size(); ++q) {
+      sp[q] = snappy[order[q]];
+      so[q] = soff[order[q]];
+    }
+    snappy.swap(sp);
+    soff.swap(so);
+  }
   const Allocator& al = ctx.alloc();
   cudaStream_t s      = ctx.stream();
   Buffer<uint8_t> scratch(al, std::max<int64_t>(scratch_bytes, 16));
@@ -576,11 +949,11 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
   const int nsn = static_cast<int>(snappy.size()), nds = static_cast<int>(dict_strings.size()),
             ndp = static_cast<int>(data_pages.size());
   if (nsn > 0)
-    launch("pq_snappy", pq_snappy_kernel, static_cast<unsigned>(ceil_div(nsn, kPqThreads / kLanes)), kPqThreads, 0, s,
+    launch("pq_snappy", pq_snappy_kernel, static_cast<unsigned>(nsn), kLanes, 0, s,
            file, d_pages.get(), static_cast<const int*>(d_lists.get()), nsn, scratch.get(),
            static_cast<const int64_t*>(d_soff.get()), d_err.get());
   if (nds > 0)
-    launch("pq_dict_strings", pq_dict_strings_kernel, pq_blocks(nds, 128), 128, 0, s,
+    launch("pq_dict_strings", pq_dict_strings_kernel, static_cast<unsigned>(nds), kPqThreads, 0, s,
            static_cast<const PqPage*>(d_pages.get()), static_cast<const int*>(d_lists.get()) + nsn, nds,
            entry_off.get(), entry_len.get(), d_err.get());
   if (ndp > 0)
@@ -615,6 +988,178 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
              static_cast<ldf_range*>(out[j].data));
   }
   ctx.finish();
+}
+
+}  // namespace ldf
+
+// ---- page headers on the host (Thrift compact protocol) -----------------------------
+namespace ldf {
+namespace {
+
+struct ThriftReader {
+  const uint8_t* b;
+  int64_t pos, end;
+  uint8_t byte()
+  {
+    if (pos >= end) fail(LDF_ERR_INVALID_ARGUMENT, "truncated Parquet page header");
+    return b[pos++];
+  }
+  uint64_t varint()
+  {
+    uint64_t v = 0;
+    for (int sh = 0;; sh += 7) {
+      if (sh > 63) fail(LDF_ERR_INVALID_ARGUMENT, "bad varint in a Parquet page header");
+      const uint8_t c = byte();
+      v |= static_cast<uint64_t>(c & 0x7f) << sh;
+      if (!(c & 0x80)) return v;
+    }
+  }
+  int64_t zigzag()
+  {
+    const uint64_t v = varint();
+    return static_cast<int64_t>(v >> 1) ^ -static_cast<int64_t>(v & 1);
+  }
+  // Skips a value of Thrift compact type t.
+  void skip(int t)
+  {
+    switch (t) {
+      case 1:
+      case 2: return;
+      case 3: byte(); return;
+      case 4:
+      case 5:
+      case 6: varint(); return;
+      case 7: pos += 8; return;
+      case 8: pos += static_cast<int64_t>(varint()); return;
+      case 9:
+      case 10: {
+        const uint8_t h = byte();
+        uint64_t n      = h >> 4;
+        if (n == 15) n = varint();
+        for (uint64_t k = 0; k < n; ++k) skip((h & 15) == 1 || (h & 15) == 2 ? 3 : (h & 15));
+        return;
+      }
+      case 11: {
+        const uint64_t n = varint();
+        if (n) {
+          const uint8_t kv = byte();
+          for (uint64_t k = 0; k < n; ++k) {
+            skip(kv >> 4);
+            skip(kv & 15);
+          }
+        }
+        return;
+      }
+      case 12: struct_fields([](int, int, ThriftReader&) { return false; }); return;
+      default: fail(LDF_ERR_INVALID_ARGUMENT, "unknown Thrift type in a Parquet page header");
+    }
+  }
+  // Calls f(field id, type, *this) for each field; f reads the value and
+  // returns true, or returns false to have it skipped.
+  template <typename F>
+  void struct_fields(F&& f)
+  {
+    int last = 0;
+    while (true) {
+      const uint8_t h = byte();
+      if (h == 0) return;
+      const int t   = h & 15;
+      const int fid = (h >> 4) ? last + (h >> 4) : static_cast<int>(zigzag());
+      if (!f(fid, t, *this)) skip(t);
+      last = fid;
+    }
+  }
+  int64_t int_value(int t) { return t == 1 ? 1 : (t == 2 ? 0 : zigzag()); }
+};
+
+}  // namespace
+
+void parquet_pages(const uint8_t* file, int64_t file_bytes, const int64_t* chunk_start, const int64_t* chunk_bytes,
+                   const int64_t* chunk_row0, const int32_t* chunk_column, const int32_t* chunk_codec,
+                   const int32_t* chunk_physical, int nchunks, ldf_parquet_page* pages, int max_pages, int* npages)
+{
+  LDF_REQUIRE(nchunks >= 0 && file != nullptr && npages != nullptr, "parquet_pages: null argument");
+  int count = 0;
+  for (int k = 0; k < nchunks; ++k) {
+    LDF_REQUIRE(chunk_start[k] >= 0 && chunk_bytes[k] >= 0 && chunk_start[k] + chunk_bytes[k] <= file_bytes,
+                "parquet_pages: column chunk outside the file");
+    const int64_t end = chunk_start[k] + chunk_bytes[k];
+    int64_t pos = chunk_start[k], row = chunk_row0[k];
+    int dict    = -1;
+    while (pos < end) {
+      ThriftReader rd{file, pos, end};
+      int64_t type = -1, usize = 0, csize = 0;
+      int64_t nvals = 0, enc = 0, lv = 0, rep = 0, compressed = 1;
+      rd.struct_fields([&](int fid, int t, ThriftReader& r) {
+        switch (fid) {
+          case 1: type = r.int_value(t); return true;
+          case 2: usize = r.int_value(t); return true;
+          case 3: csize = r.int_value(t); return true;
+          case 5:  // DataPageHeader
+          case 7:  // DictionaryPageHeader
+          case 8:  // DataPageHeaderV2
+            if (t != 12) return false;
+            r.struct_fields([&](int g, int tt, ThriftReader& q) {
+              if (fid == 8) {
+                switch (g) {
+                  case 1: nvals = q.int_value(tt); return true;
+                  case 4: enc = q.int_value(tt); return true;
+                  case 5: lv = q.int_value(tt); return true;
+                  case 6: rep = q.int_value(tt); return true;
+                  case 7: compressed = q.int_value(tt); return true;
+                  default: return false;
+                }
+              }
+              if (g == 1) nvals = q.int_value(tt);
+              else if (g == 2) enc = q.int_value(tt);
+              else return false;
+              return true;
+            });
+            return true;
+          default: return false;
+        }
+      });
+      const int64_t payload = rd.pos;
+      LDF_REQUIRE(csize >= 0 && payload + csize <= end, "parquet_pages: page outside its column chunk");
+      if (type == 0 || type == 2 || type == 3) {
+        if (type != 2) {
+          const bool rle_bool = enc == 3 && chunk_physical[k] == LDF_PQ_BOOLEAN;
+          if (!(enc == 0 || enc == 2 || enc == 8 || rle_bool))
+            fail(LDF_ERR_UNSUPPORTED, "parquet_pages: page encoding " + std::to_string(enc));
+          if (rep != 0) fail(LDF_ERR_UNSUPPORTED, "parquet_pages: repetition levels");
+        }
+        if (pages != nullptr) {
+          LDF_REQUIRE(count < max_pages, "parquet_pages: more pages than max_pages");
+          ldf_parquet_page& e = pages[count];
+          e                   = ldf_parquet_page{};
+          e.offset            = payload;
+          e.compressed        = csize;
+          e.uncompressed      = usize;
+          e.num_values        = static_cast<int32_t>(nvals);
+          e.encoding          = static_cast<int32_t>(enc);
+          e.codec             = chunk_codec[k];
+          e.column            = chunk_column[k];
+          e.dict              = -1;
+          if (type == 2) {
+            e.kind = LDF_PQ_DICT_PAGE;
+          } else {
+            e.kind = type == 0 ? LDF_PQ_DATA_V1 : LDF_PQ_DATA_V2;
+            e.row0 = row;
+            e.dict = (enc == 2 || enc == 8) ? dict : -1;
+            if (type == 3) {
+              e.levels_bytes = static_cast<int32_t>(lv);
+              if (!compressed) e.codec = LDF_PQ_UNCOMPRESSED;
+            }
+          }
+        }
+        if (type == 2) dict = count;
+        else row += nvals;
+        ++count;
+      }
+      pos = payload + csize;
+    }
+  }
+  *npages = count;
 }
 
 }  // namespace ldf

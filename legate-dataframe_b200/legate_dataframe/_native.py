@@ -174,6 +174,12 @@ def lib():
                 P(ldf_column), P(ldf_allocator), ctypes.c_void_p,
             ]
             L.ldf_b200_parquet_decode.restype = ctypes.c_int
+            i64p = P(ctypes.c_int64)
+            L.ldf_b200_parquet_pages.argtypes = [
+                ctypes.c_void_p, ctypes.c_int64, i64p, i64p, i64p, i32p, i32p, i32p, ctypes.c_int32,
+                P(ldf_parquet_page), ctypes.c_int32, i32p,
+            ]
+            L.ldf_b200_parquet_pages.restype = ctypes.c_int
             L.ldf_b200_arrow_bits_to_bytes.restype = ctypes.c_int
             L.ldf_b200_arrow_offsets_to_ranges.restype = ctypes.c_int
             L.ldf_b200_launch_count.restype = ctypes.c_ulonglong

@@ -73,86 +73,9 @@ def _file_to_device(path, dev) -> tuple[torch.Tensor, torch.Tensor, int]:
     return host, text, size
 
 
-# ---- page headers: Thrift compact protocol --------------------------------------
-class _Thrift:
-    """Reads Thrift compact-protocol structs (the Parquet page headers) as
-    {field id: value} dicts; nested structs become dicts, lists are read and
-    kept, binaries kept as bytes."""
-
-    def __init__(self, buf, pos: int, end: int):
-        self.b, self.pos, self.end = buf, pos, end
-
-    def byte(self) -> int:
-        if self.pos >= self.end:
-            raise ValueError("truncated Parquet page header")
-        v = int(self.b[self.pos])
-        self.pos += 1
-        return v
-
-    def varint(self) -> int:
-        v, sh = 0, 0
-        while True:
-            c = self.byte()
-            v |= (c & 0x7F) << sh
-            if not c & 0x80:
-                return v
-            sh += 7
-            if sh > 70:
-                raise ValueError("bad varint in a Parquet page header")
-
-    def zigzag(self) -> int:
-        v = self.varint()
-        return (v >> 1) ^ -(v & 1)
-
-    def value(self, t: int):
-        if t in (1, 2):  # booleans inside a struct: the type carries the value
-            return t == 1
-        if t == 3:
-            return self.byte()
-        if t in (4, 5, 6):
-            return self.zigzag()
-        if t == 7:
-            self.pos += 8
-            return None
-        if t == 8:
-            n = self.varint()
-            v = bytes(self.b[self.pos:self.pos + n])
-            self.pos += n
-            return v
-        if t in (9, 10):
-            h = self.byte()
-            n, et = h >> 4, h & 0x0F
-            if n == 15:
-                n = self.varint()
-            return [self.byte() == 1 if et in (1, 2) else self.value(et) for _ in range(n)]
-        if t == 11:
-            n = self.varint()
-            if n:
-                kv = self.byte()
-                for _ in range(n):
-                    self.value(kv >> 4)
-                    self.value(kv & 0x0F)
-            return None
-        if t == 12:
-            return self.struct()
-        raise ValueError(f"unknown Thrift type {t} in a Parquet page header")
-
-    def struct(self) -> dict:
-        out, last = {}, 0
-        while True:
-            h = self.byte()
-            if h == 0:
-                return out
-            delta, t = h >> 4, h & 0x0F
-            fid = last + delta if delta else self.zigzag()
-            out[fid] = self.value(t)
-            last = fid
-
-
 _PHYSICAL = {"BOOLEAN": N.LDF_PQ_BOOLEAN, "INT32": N.LDF_PQ_INT32, "INT64": N.LDF_PQ_INT64,
              "FLOAT": N.LDF_PQ_FLOAT, "DOUBLE": N.LDF_PQ_DOUBLE, "BYTE_ARRAY": N.LDF_PQ_BYTE_ARRAY}
 _CODECS = {"UNCOMPRESSED": N.LDF_PQ_UNCOMPRESSED, "SNAPPY": N.LDF_PQ_SNAPPY}
-_VALUE_ENCODINGS = {0, 2, 8}  # PLAIN, PLAIN_DICTIONARY, RLE_DICTIONARY
 
 
 class _NotOnDevice(Exception):
@@ -172,56 +95,41 @@ def _ldf_output_type(arrow_type: pa.DataType, physical: int) -> int:
         raise _NotOnDevice(str(e))
 
 
-def _page_table(host, md, col_indices, physical=None):
-    """One ldf_parquet_page per page of the selected column chunks, from the
-    footer (via Arrow's metadata reader) and the page headers in `host`."""
-    pages = []
-    row_base = 0
+def _page_table(host, md, col_indices, physical):
+    """One ldf_parquet_page per page of the selected column chunks: the
+    chunks' extents come from the footer (Arrow's metadata reader), their page
+    headers are walked by the library on the host (ldf_b200_parquet_pages)."""
+    nchunks = md.num_row_groups * len(col_indices)
+    i64, i32 = ctypes.c_int64 * max(nchunks, 1), ctypes.c_int32 * max(nchunks, 1)
+    start, nbytes, row0 = i64(), i64(), i64()
+    column, codec, phys = i32(), i32(), i32()
+    k, row_base = 0, 0
     for g in range(md.num_row_groups):
         rg = md.row_group(g)
         for j, ci in enumerate(col_indices):
             cc = rg.column(ci)
             if cc.compression not in _CODECS:
                 raise _NotOnDevice(f"codec {cc.compression}")
-            codec = _CODECS[cc.compression]
-            start = cc.dictionary_page_offset if cc.dictionary_page_offset else cc.data_page_offset
-            end = start + cc.total_compressed_size
-            pos, row, dict_index = start, row_base, -1
-            while pos < end:
-                rd = _Thrift(host, pos, end)
-                h = rd.struct()
-                payload = rd.pos
-                kind, csize, usize = h.get(1), h.get(3, 0), h.get(2, 0)
-                e = {"offset": payload, "compressed": csize, "uncompressed": usize, "row0": 0, "num_values": 0,
-                     "kind": 0, "encoding": 0, "codec": codec, "levels_bytes": 0, "dict": -1, "column": j}
-                if kind == 2:  # dictionary page
-                    dh = h.get(7, {})
-                    e.update(kind=N.LDF_PQ_DICT_PAGE, num_values=dh.get(1, 0), encoding=dh.get(2, 0))
-                    dict_index = len(pages)
-                    pages.append(e)
-                elif kind in (0, 3):
-                    dh = h.get(5 if kind == 0 else 8, {})
-                    enc = dh.get(2 if kind == 0 else 4, 0)
-                    rle_bool = enc == 3 and physical is not None and physical[j] == N.LDF_PQ_BOOLEAN
-                    if enc not in _VALUE_ENCODINGS and not rle_bool:
-                        raise _NotOnDevice(f"page encoding {enc}")
-                    e.update(kind=N.LDF_PQ_DATA_V1 if kind == 0 else N.LDF_PQ_DATA_V2, num_values=dh.get(1, 0),
-                             encoding=enc, row0=row, dict=dict_index if enc in (2, 8) else -1)
-                    if kind == 3:
-                        if dh.get(6, 0):
-                            raise _NotOnDevice("repetition levels")
-                        e["levels_bytes"] = dh.get(5, 0)
-                        if dh.get(7, True) is False:
-                            e["codec"] = N.LDF_PQ_UNCOMPRESSED
-                    row += e["num_values"]
-                    pages.append(e)
-                pos = payload + csize
+            start[k] = cc.dictionary_page_offset if cc.dictionary_page_offset else cc.data_page_offset
+            nbytes[k] = cc.total_compressed_size
+            row0[k], column[k], codec[k], phys[k] = row_base, j, _CODECS[cc.compression], physical[j]
+            k += 1
         row_base += rg.num_rows
-    table = (N.ldf_parquet_page * max(len(pages), 1))()
-    for k, e in enumerate(pages):
-        for name, v in e.items():
-            setattr(table[k], name, v)
-    return table, len(pages)
+    L = N.lib()
+    buf = np.ascontiguousarray(host, dtype=np.uint8)
+    args = (buf.ctypes.data, buf.size, start, nbytes, row0, column, codec, phys, nchunks)
+    count = ctypes.c_int32(0)
+
+    def walk(table, cap):
+        status = L.ldf_b200_parquet_pages(*args, table, cap, ctypes.byref(count))
+        if status == N.LDF_ERR_UNSUPPORTED:
+            raise _NotOnDevice(L.ldf_b200_last_error().decode("utf-8", "replace"))
+        N.check(status)
+
+    walk(None, 0)  # the page count
+    table = (N.ldf_parquet_page * max(count.value, 1))()
+    walk(table, count.value)
+    return table, count.value
 
 
 def _column_specs(pf, columns):

@@ -33,6 +33,10 @@ static inline void __syncthreads() {}
 static inline void __syncwarp() {}
 template <typename T> static inline T atomicMin(T* p, T v) { T o = *p; if (v < o) *p = v; return o; }
 template <typename T, int NT> static inline T block_exclusive_scan(T v, T*, T* total) { *total = v; return 0; }
+// warp intrinsics of the 32-lane paths, which a one-lane build never takes
+static inline int __shfl_up_sync(unsigned, int v, int) { abort(); return v; }
+static inline unsigned __ballot_sync(unsigned, bool) { abort(); return 0; }
+static inline int __ffs(unsigned) { abort(); return 0; }
 
 namespace ldf {
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }

@@ -3,7 +3,9 @@
 The Snappy decoder, the RLE / bit-packed hybrid cutter, the dictionary entry
 table and the data-page kernel of legate-dataframe_b200/csrc/parquet.cu are
 compiled as host C++ with tests/host_emulation/parquet_emu.cpp (one thread
-per block, tiles of 8 rows, so every tile boundary and run split is
+per block, tiles of 8 rows, 48-byte Snappy input stages, a 256-byte output
+ring, 64-byte Snappy batches and 32-byte dictionary stages, so every tile
+boundary, run split, restage, chain through a batch and ring miss is
 exercised) under AddressSanitizer.  The page table comes from the library's
 own footer and page-header reader (lib/parquet.py); every column's values
 and nulls are compared with the reference's CPU reader, Arrow
@@ -35,7 +37,13 @@ def _section() -> str:
     sec = src[src.index("constexpr int kLanes"):src.index("unsigned pq_blocks(")]
     for a, b in (("constexpr int kLanes     = 32;", "constexpr int kLanes     = 1;"),
                  ("constexpr int kPqThreads = 128;", "constexpr int kPqThreads = 1;"),
-                 ("constexpr int kPqTile    = 1024;", "constexpr int kPqTile    = 8;")):
+                 ("constexpr int kPqTile    = 1024;", "constexpr int kPqTile    = 8;"),
+                 # small stages and ring: restaging, long literals and far back-references are frequent
+                 ("constexpr int kSnapIn    = 2048;", "constexpr int kSnapIn    = 48;"),
+                 ("constexpr int kSnapWin   = 32768;", "constexpr int kSnapWin   = 256;"),
+                 ("constexpr int kSnapBatchBytes = 1024;", "constexpr int kSnapBatchBytes = 64;"),
+                 ("constexpr int kSnapShort      = 64;", "constexpr int kSnapShort      = 16;"),
+                 ("constexpr int kDictStage = 8192;", "constexpr int kDictStage = 32;")):
         assert a in sec, a
         sec = sec.replace(a, b)
     return sec
@@ -183,4 +191,52 @@ def test_long_runs_and_all_null_pages(emu, tmp_path):
                   "h": pa.array(np.where(np.arange(n) % 1000 == 0, None, 7), pa.int64())})
     path = tmp_path / "l.parquet"
     pq.write_table(t, path, data_page_size=4096)
+    same(decode(emu, path, tmp_path), expected(path))
+
+
+def test_page_walk_rejects_what_the_decoder_lacks(tmp_path):
+    """ldf_b200_parquet_pages (the host page-header walk) refuses pages in
+    other encodings, which sends parquet_read to Arrow, and reports headers
+    cut short by the file's end as invalid input."""
+    import sys
+
+    sys.path.insert(0, str(ROOT / "legate-dataframe_b200"))
+    from legate_dataframe.lib import parquet as P
+
+    t = pa.table({"x": pa.array(np.arange(5000), pa.int64())})
+    path = tmp_path / "delta.parquet"
+    pq.write_table(t, path, use_dictionary=False, column_encoding={"x": "DELTA_BINARY_PACKED"})
+    pf = pq.ParquetFile(path)
+    _, idx, physical, _, _, _ = P._column_specs(pf, None)
+    data = np.fromfile(path, dtype=np.uint8)
+    with pytest.raises(P._NotOnDevice, match="encoding"):
+        P._page_table(data, pf.metadata, idx, physical)
+
+    path = tmp_path / "plain.parquet"
+    pq.write_table(t, path, use_dictionary=False, data_page_size=1024)
+    pf = pq.ParquetFile(path)
+    data = np.fromfile(path, dtype=np.uint8)
+    pages, n = P._page_table(data, pf.metadata, idx, physical)
+    assert n > 1 and sum(pages[k].num_values for k in range(n)) == 5000
+    cut = data[: pages[1].offset - 3]  # the second page's header runs past the end
+    with pytest.raises(ValueError):
+        P._page_table(cut, pf.metadata, idx, physical)
+
+
+def test_snappy_overlapping_and_far_copies(emu, tmp_path):
+    """PLAIN pages that Snappy turns into overlapping back-references (runs
+    of one value, short periodic strings) and references further back than
+    the output ring, mixed with literals of every length class."""
+    rng = np.random.default_rng(5)
+    n = 30_000
+    period = np.array(["ab" * (i % 5 + 1) for i in range(n)], dtype=object)
+    far = rng.integers(0, 2**62, 64)  # a block of values repeated every 512 bytes
+    t = pa.table({"zeros": pa.array(np.zeros(n, np.int64)),
+                  "runs": pa.array(np.repeat(rng.integers(0, 2**40, n // 100), 100)),
+                  "period": pa.array(period),
+                  "far": pa.array(np.tile(far, n // 64 + 1)[:n]),
+                  "noise": pa.array(rng.integers(0, 2**63, n)),
+                  "mixed": pa.array(np.where(rng.random(n) < 0.5, 7, rng.integers(0, 2**31, n)))})
+    path = tmp_path / "s.parquet"
+    pq.write_table(t, path, use_dictionary=False, compression="snappy", data_page_size=64 * 1024)
     same(decode(emu, path, tmp_path), expected(path))
