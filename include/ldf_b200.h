@@ -227,7 +227,7 @@ int ldf_b200_csv_read(const uint8_t* text, int64_t nbytes, char delimiter, int32
  * only (max repetition level 0, max definition level 0 or 1). */
 enum { LDF_PQ_DICT_PAGE = 0, LDF_PQ_DATA_V1 = 1, LDF_PQ_DATA_V2 = 2 };
 enum { LDF_PQ_UNCOMPRESSED = 0, LDF_PQ_SNAPPY = 1 };
-/* Parquet physical types used */
+/* Parquet physical types used (the values of the format's Type enum) */
 enum { LDF_PQ_BOOLEAN = 0, LDF_PQ_INT32 = 1, LDF_PQ_INT64 = 2, LDF_PQ_FLOAT = 4, LDF_PQ_DOUBLE = 5,
        LDF_PQ_BYTE_ARRAY = 6 };
 typedef struct {

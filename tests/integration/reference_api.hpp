@@ -54,6 +54,47 @@ class CountOptions : public FunctionOptions {  // groupby_aggregation.cpp:58-71 
 }  // namespace compute
 }  // namespace arrow
 
+// ---- Arrow's Parquet metadata reader (parquet.cpp:459-468 opens files with
+// it; the column-chunk members are those of Arrow's parquet/metadata.h) -----
+namespace arrow::io {
+class ReadableFile {
+ public:
+  static std::shared_ptr<ReadableFile> Open(const std::string& path);  // through ARROW_RESULT at parquet.cpp:459
+};
+}  // namespace arrow::io
+namespace parquet {
+struct Type {  // the Parquet physical types (Thrift enum Type): the values of LDF_PQ_*
+  enum type { BOOLEAN = 0, INT32 = 1, INT64 = 2, INT96 = 3, FLOAT = 4, DOUBLE = 5, BYTE_ARRAY = 6, FIXED_LEN_BYTE_ARRAY = 7 };
+};
+struct Compression {
+  enum type { UNCOMPRESSED, SNAPPY, GZIP, BROTLI, ZSTD, LZ4, LZ4_FRAME, LZO, BZ2 };
+};
+class ColumnChunkMetaData {
+ public:
+  bool has_dictionary_page() const;
+  int64_t dictionary_page_offset() const;
+  int64_t data_page_offset() const;
+  int64_t total_compressed_size() const;
+  Compression::type compression() const;
+  Type::type type() const;
+};
+class RowGroupMetaData {
+ public:
+  int64_t num_rows() const;  // parquet.cpp:468
+  std::unique_ptr<ColumnChunkMetaData> ColumnChunk(int i) const;
+};
+class FileMetaData {
+ public:
+  int num_row_groups() const;  // parquet.cpp:463
+  std::unique_ptr<RowGroupMetaData> RowGroup(int i) const;
+};
+class ParquetFileReader {
+ public:
+  static std::unique_ptr<ParquetFileReader> Open(std::shared_ptr<arrow::io::ReadableFile> source);  // parquet.cpp:460
+  std::shared_ptr<FileMetaData> metadata() const;  // parquet.cpp:461
+};
+}  // namespace parquet
+
 // ---- rmm (TaskMemoryResource is an rmm device_memory_resource) -------------
 namespace rmm {
 class cuda_stream_view {
@@ -185,5 +226,12 @@ void get_parallel_launch_task(TaskContext& ctx);         // task_argument.hpp:28
 
 [[nodiscard]] std::pair<size_t, size_t> evenly_partition_work(size_t work_size, size_t rank,
                                                               size_t nranks);  // utils.hpp:156
+
+namespace task {
+// The rank's files and their row groups (parquet.cpp:60-93)
+std::pair<std::vector<std::string>, std::vector<std::vector<int>>> find_files_and_row_groups(
+  const std::vector<std::string>& file_paths, const std::vector<size_t>& ngroups_per_file, size_t from_row_group,
+  size_t num_row_groups);
+}  // namespace task
 
 }  // namespace legate::dataframe

@@ -325,4 +325,81 @@ void csv_read_gpu_body(TaskContext& ctx)
   bind_outputs(ocols, res, ctx);
 }
 
+// ---- ParquetRead::gpu_variant (parquet.cu:48-101) ----------------------------------
+// The rank's row groups (find_files_and_row_groups, parquet.cpp:60-93) are
+// decoded on the device: Arrow's metadata reader gives the column chunks'
+// extents, ldf_b200_parquet_pages walks their page headers on the host and
+// ldf_b200_parquet_decode decodes the pages from a device copy of the file.
+// This sketch binds one file per rank; several files per rank would
+// concatenate the columns, and a chunk in another codec would take the CPU
+// reader's path.
+void parquet_read_gpu_body(TaskContext& ctx)
+{
+  const auto file_paths        = argument::get_next_scalar_vector<std::string>(ctx);
+  const auto columns           = argument::get_next_scalar_vector<std::string>(ctx);
+  const auto column_indices    = argument::get_next_scalar_vector<int>(ctx);
+  const auto ngroups_per_file  = argument::get_next_scalar_vector<size_t>(ctx);
+  const auto nrow_groups_total = argument::get_next_scalar<size_t>(ctx);
+  auto output                  = argument::get_next_output<PhysicalTable>(ctx);
+  argument::get_parallel_launch_task(ctx);
+  (void)columns;
+
+  auto ocols = output.release();
+  auto [first_group, ngroups] = legate::dataframe::evenly_partition_work(
+    nrow_groups_total, static_cast<size_t>(ctx.rank), static_cast<size_t>(ctx.nranks));
+  if (ngroups == 0) {
+    for (auto& c : ocols) c.bind_empty_data();
+    return;
+  }
+  auto [files, row_groups] =
+    legate::dataframe::task::find_files_and_row_groups(file_paths, ngroups_per_file, first_group, ngroups);
+  auto metadata = parquet::ParquetFileReader::Open(arrow::io::ReadableFile::Open(files.at(0)))->metadata();
+  std::vector<int64_t> start, bytes, row0;
+  std::vector<int32_t> column, codec, physical;
+  int64_t nrows = 0;
+  for (int g : row_groups.at(0)) {
+    auto rg = metadata->RowGroup(g);
+    for (size_t j = 0; j < column_indices.size(); ++j) {
+      auto cc = rg->ColumnChunk(column_indices[j]);
+      if (cc->compression() != parquet::Compression::SNAPPY && cc->compression() != parquet::Compression::UNCOMPRESSED)
+        throw std::invalid_argument("codec not decoded on the device");
+      start.push_back(cc->has_dictionary_page() ? cc->dictionary_page_offset() : cc->data_page_offset());
+      bytes.push_back(cc->total_compressed_size());
+      row0.push_back(nrows);
+      column.push_back(static_cast<int32_t>(j));
+      codec.push_back(cc->compression() == parquet::Compression::SNAPPY ? LDF_PQ_SNAPPY : LDF_PQ_UNCOMPRESSED);
+      if (g == row_groups.at(0).front()) physical.push_back(static_cast<int32_t>(cc->type()));
+    }
+    nrows += rg->num_rows();
+  }
+  std::ifstream in(files.at(0), std::ios::binary);
+  const std::vector<uint8_t> file((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+  const auto nchunks = static_cast<int32_t>(start.size());
+  int32_t npages     = 0;
+  std::vector<int32_t> chunk_physical;
+  for (int32_t k = 0; k < nchunks; ++k) chunk_physical.push_back(physical.at(column[k]));
+  ldf_check(ldf_b200_parquet_pages(file.data(), static_cast<int64_t>(file.size()), start.data(), bytes.data(),
+                                   row0.data(), column.data(), codec.data(), chunk_physical.data(), nchunks,
+                                   nullptr, 0, &npages));
+  std::vector<ldf_parquet_page> pages(static_cast<size_t>(npages));
+  ldf_check(ldf_b200_parquet_pages(file.data(), static_cast<int64_t>(file.size()), start.data(), bytes.data(),
+                                   row0.data(), column.data(), codec.data(), chunk_physical.data(), nchunks,
+                                   pages.data(), npages, &npages));
+  TaskMemoryResource& mr = *ctx.mr();
+  void* dfile            = mr.allocate(file.size() + 16, ctx.stream());
+  cudaMemcpyAsync(dfile, file.data(), file.size(), cudaMemcpyHostToDevice, ctx.stream());
+  std::vector<int32_t> types, nullable;
+  for (auto& c : ocols) {
+    types.push_back(ldf_type_of(c));
+    nullable.push_back(c.nullable() ? 1 : 0);
+  }
+  std::vector<ldf_column> res(ocols.size());
+  ldf_allocator alloc = task_allocator(ctx);
+  ldf_check(ldf_b200_parquet_decode(static_cast<const uint8_t*>(dfile), static_cast<int64_t>(file.size()),
+                                    pages.data(), npages, physical.data(), types.data(), nullable.data(),
+                                    static_cast<int32_t>(ocols.size()), nrows, res.data(), &alloc, ctx.stream()));
+  mr.deallocate(dfile, file.size() + 16, ctx.stream());
+  bind_outputs(ocols, res, ctx);
+}
+
 }  // namespace ldf_integration
