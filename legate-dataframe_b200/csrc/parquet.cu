@@ -140,6 +140,15 @@ __device__ __forceinline__ SnapElem snap_at(const SnapShared& sh, int r)
   return snap_decode(q[0], x);
 }
 
+__device__ __forceinline__ void store_u32(uint8_t* p, uint32_t v)  // p 4-byte aligned
+{
+#ifdef __CUDA_ARCH__
+  *reinterpret_cast<uint32_t*>(p) = v;
+#else
+  memcpy(p, &v, 4);
+#endif
+}
+
 __device__ __forceinline__ uint32_t load_u32(const uint8_t* p)  // p 4-byte aligned
 {
 #ifdef __CUDA_ARCH__
@@ -186,18 +195,18 @@ __device__ void snap_sizes(SnapStage& st, SnapShared& sh)
   __syncwarp();
 }
 
-// Stages the stream from the 16-byte boundary at or below stream index i:
-// in[k] = src[ib + k] for the indices inside [0, n); with `sizes`, size[]
-// too.
-__device__ void snap_stage(SnapStage& st, SnapShared& sh, int64_t i, bool sizes)
+constexpr int kSnapPer = kSnapIn / 16 / kLanes;  // staged 16-byte granules per lane
+struct alignas(16) SnapGranule {
+  uint8_t b[16];
+};
+
+// Loads the stage that starts at the 16-byte boundary at or below stream
+// index i into registers (the bytes inside [0, n)); returns its first index.
+__device__ int64_t snap_load(const SnapStage& st, int64_t i, SnapGranule (&reg)[kSnapPer])
 {
-  const int lane = threadIdx.x % kLanes;
+  const int lane   = threadIdx.x % kLanes;
   const int64_t ib = i - static_cast<int64_t>(reinterpret_cast<uintptr_t>(st.src + i) & 15);
-  constexpr int kPer = kSnapIn / 16 / kLanes;  // granules per lane
-  struct alignas(16) Granule {
-    uint8_t b[16];
-  } reg[kPer];
-  for (int r = 0; r < kPer; ++r) {  // all loads first, then the stores
+  for (int r = 0; r < kSnapPer; ++r) {
     const int64_t b = ib + 16 * (lane + r * kLanes);
     if (b >= 0 && b + 16 <= st.n) {
       copy16(reg[r].b, st.src + b);
@@ -205,11 +214,27 @@ __device__ void snap_stage(SnapStage& st, SnapShared& sh, int64_t i, bool sizes)
       for (int k = 0; k < 16; ++k) reg[r].b[k] = b + k >= 0 && b + k < st.n ? st.src[b + k] : 0;
     }
   }
+  return ib;
+}
+
+// Makes the loaded stage the staged one: in[k] = src[ib + k].
+__device__ void snap_commit(SnapStage& st, SnapShared& sh, int64_t ib, const SnapGranule (&reg)[kSnapPer])
+{
+  const int lane = threadIdx.x % kLanes;
   __syncwarp();  // every lane is done with the previous contents
   st.ib    = ib;
   st.sized = false;
-  for (int r = 0; r < kPer; ++r) copy16(sh.in + 16 * (lane + r * kLanes), reg[r].b);
+  for (int r = 0; r < kSnapPer; ++r) copy16(sh.in + 16 * (lane + r * kLanes), reg[r].b);
   __syncwarp();
+}
+
+// Stages the stream from the 16-byte boundary at or below stream index i;
+// with `sizes`, size[] too.
+__device__ void snap_stage(SnapStage& st, SnapShared& sh, int64_t i, bool sizes)
+{
+  SnapGranule reg[kSnapPer];
+  const int64_t ib = snap_load(st, i, reg);  // all loads first, then the stores
+  snap_commit(st, sh, ib, reg);
   if (sizes) snap_sizes(st, sh);
 }
 
@@ -326,22 +351,40 @@ __device__ bool snappy_warp(const uint8_t* src, int64_t n, uint8_t* dst, int64_t
       const SnapElem e   = snap_at(sh, static_cast<int>(i - st.ib));
       const int64_t body = i + e.hdr;
       if (body > n || body + e.l > n || o + e.l > total) return false;
-      int64_t from_i = body;
-      for (int64_t done = 0; done < e.l;) {
-        if (from_i >= st.ib + kSnapIn) snap_stage(st, sh, from_i, false);
-        const int64_t piece = e.l - done < st.ib + kSnapIn - from_i ? e.l - done : st.ib + kSnapIn - from_i;
-        const uint8_t* from = sh.in + (from_i - st.ib);
-        const int64_t at    = o + done;
+      // Copied a stage at a time with four-byte stores, the next stage's
+      // loads in flight meanwhile; the ring keeps only the literal's last
+      // kSnapWin bytes.
+      const int64_t l         = e.l;
+      const int64_t ring_from = l > kSnapWin ? l - kSnapWin : 0;
+      int64_t from_i          = body;
+      if (from_i >= st.ib + kSnapIn) snap_stage(st, sh, from_i, false);
+      for (int64_t done = 0; done < l;) {
+        const int64_t avail = st.ib + kSnapIn - from_i;
+        const int64_t piece = l - done < avail ? l - done : avail;
+        const bool more     = done + piece < l;
+        SnapGranule reg[kSnapPer];
+        int64_t next_ib = 0;
+        if (more) next_ib = snap_load(st, from_i + piece, reg);
+        const uint8_t* f = sh.in + (from_i - st.ib);
+        uint8_t* to      = dst + o + done;
+        int64_t head     = (4 - static_cast<int64_t>(reinterpret_cast<uintptr_t>(to) & 3)) & 3;
+        if (head > piece) head = piece;
+        for (int64_t k = lane; k < head; k += kLanes) to[k] = f[k];
+        const int64_t words = (piece - head) >> 2;
 #pragma unroll 4
-        for (int64_t k = lane; k < piece; k += kLanes) {
-          const uint8_t b          = from[k];
-          dst[at + k]              = b;
-          sh.win[(at + k) & kMask] = b;
+        for (int64_t w = lane; w < words; w += kLanes) {
+          const uint8_t* q = f + head + 4 * w;
+          store_u32(to + head + 4 * w, static_cast<uint32_t>(q[0]) | static_cast<uint32_t>(q[1]) << 8 |
+                                         static_cast<uint32_t>(q[2]) << 16 | static_cast<uint32_t>(q[3]) << 24);
         }
+        for (int64_t k = head + 4 * words + lane; k < piece; k += kLanes) to[k] = f[k];
+        for (int64_t k = (ring_from > done ? ring_from - done : 0) + lane; k < piece; k += kLanes)
+          sh.win[(o + done + k) & kMask] = f[k];
         done += piece;
         from_i += piece;
+        if (more) snap_commit(st, sh, next_ib, reg);
       }
-      o += e.l;
+      o += l;
       i = from_i;
       __syncwarp();
       continue;
@@ -606,6 +649,366 @@ __global__ void __launch_bounds__(kPqThreads) pq_dict_strings_kernel(const PqPag
   }
 }
 
+// ---- large byte-array Snappy pages: the element chain ranked in parallel ----------
+// A Snappy page of a byte-array column can hold hundreds of thousands of short
+// elements (a 1 MB dictionary page of short strings about 60,000), which one
+// warp parses in turn.  Such pages are decoded by the whole GPU instead:
+//  1. every position of the stream gets the position of the element that would
+//     follow a tag there (nxt), and doubling gives the position kChainStep
+//     elements on;
+//  2. one thread per page lays checkpoints kChainStep elements apart through the
+//     doubled table, one thread per checkpoint walks its kChainStep elements;
+//  3. every element is decoded on its own; a scan of the output lengths gives
+//     its output position;
+//  4. every output byte points at its source: a literal's input byte, or for
+//     byte k of a copy of offset d the output byte o - d + k % d; pointer
+//     jumping (log2 of the page size rounds) takes every byte to a literal
+//     input byte, which is then copied.
+constexpr int64_t kChainMinBytes = 131072;  // Snappy pages from this many output bytes
+constexpr int64_t kDictChainMinBytes = 16384;  // dictionary pages from this many data bytes
+constexpr int kChainLog          = 8;
+constexpr int kChainStep         = 1 << kChainLog;  // elements between checkpoints
+constexpr int64_t kChainMaxInput = int64_t(32) << 20;  // bytes per call and kind (pages beyond: the per-page kernels)
+
+struct ChainPage {
+  int page;           // index in the page table
+  int64_t file_off;   // file offset of the Snappy stream (behind a v2 page's levels)
+  int64_t n;          // compressed stream bytes
+  int64_t lv;         // v2 levels in front of the stream (copied as they are)
+  int64_t u;          // stream output bytes
+  int64_t elem_cap;   // element slots (every element takes 2 input bytes or more)
+  int64_t ck_cap;     // checkpoint slots
+};
+struct ChainState {
+  int64_t start;  // first tag (behind the length preamble); -1 when the preamble is bad
+  int64_t nck;    // checkpoints laid
+  int64_t nelem;  // elements (set by the walk that reaches the stream's end)
+};
+struct ChainBases {  // the flattened index spaces: first index of each page
+  const int64_t* in;    // stream positions
+  const int64_t* out;   // output bytes (the page's scratch offset; levels included)
+  const int64_t* elem;  // element slots
+  const int64_t* ck;    // checkpoint slots
+  int n;                // chain pages
+};
+
+// Last page q with bases[q] <= g.
+__device__ __forceinline__ int chain_page_of(const int64_t* bases, int n, int64_t g)
+{
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (bases[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Input bytes of the element whose tag is at b[x] (x < n), or -1 when its
+// extra length bytes run past n.
+__device__ __forceinline__ int64_t chain_elem_size(const uint8_t* b, int64_t x, int64_t n)
+{
+  const uint32_t t = b[x];
+  if ((t & 3) != 0) return (t & 3) == 1 ? 2 : ((t & 3) == 2 ? 3 : 5);
+  const uint32_t L = t >> 2;
+  if (L < 60) return L + 2;
+  const int nb = static_cast<int>(L) - 59;
+  if (x + 1 + nb > n) return -1;
+  uint64_t len = 0;
+  for (int k = 0; k < nb; ++k) len |= static_cast<uint64_t>(b[x + 1 + k]) << (8 * k);
+  return 1 + nb + static_cast<int64_t>(len) + 1;
+}
+
+__global__ void chain_start_kernel(const uint8_t* file, const ChainPage* cp, ChainState* st, int npages,
+                                   unsigned long long* err)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npages; q += gridDim.x * blockDim.x) {
+    const ChainPage& c = cp[q];
+    const uint8_t* b   = file + c.file_off;
+    int64_t i = 0, start = -1;
+    uint64_t len = 0;
+    for (int sh = 0; sh <= 35; sh += 7) {
+      if (i >= c.n) break;
+      const uint8_t v = b[i++];
+      len |= static_cast<uint64_t>(v & 0x7f) << sh;
+      if (!(v & 0x80)) {
+        start = i;
+        break;
+      }
+    }
+    if (start < 0 || len != static_cast<uint64_t>(c.u)) {
+      start = -1;
+      pq_error(err, c.page, kPqErrSnappy);
+    }
+    st[q] = ChainState{start, 0, 0};
+  }
+}
+
+__global__ void chain_next_kernel(const uint8_t* file, const ChainPage* cp, const ChainState* st, ChainBases B,
+                                  int64_t total, int64_t* nxt)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int q        = chain_page_of(B.in, B.n, g);
+    const ChainPage& c = cp[q];
+    const int64_t x    = g - B.in[q];
+    int64_t v          = -1;
+    if (st[q].start >= 0 && x >= st[q].start && x < c.n) {
+      const int64_t sz = chain_elem_size(file + c.file_off, x, c.n);
+      if (sz > 0 && x + sz < c.n) v = B.in[q] + x + sz;
+    }
+    nxt[g] = v;
+  }
+}
+
+__global__ void chain_double_kernel(const int64_t* in, int64_t* out, int64_t total)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t v = in[g];
+    out[g]          = v < 0 ? -1 : in[v];
+  }
+}
+
+// One thread per page: checkpoints kChainStep elements apart.
+__global__ void chain_checkpoints_kernel(const ChainPage* cp, ChainState* st, ChainBases B, const int64_t* jump,
+                                         int64_t* ck)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < B.n; q += gridDim.x * blockDim.x) {
+    int64_t c = st[q].start >= 0 ? B.in[q] + st[q].start : -1;
+    int64_t j = 0;
+    while (c >= 0 && j < cp[q].ck_cap) {
+      ck[B.ck[q] + j++] = c;
+      c = jump[c];
+    }
+    st[q].nck = j;
+  }
+}
+
+// One thread per checkpoint: the element positions of its kChainStep elements.
+__global__ void chain_walk_kernel(const uint8_t* file, const ChainPage* cp, ChainState* st, ChainBases B,
+                                  int64_t total_ck, const int64_t* ck, int64_t* epos, unsigned long long* err)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total_ck;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int q        = chain_page_of(B.ck, B.n, g);
+    const int64_t j    = g - B.ck[q];
+    if (j >= st[q].nck) continue;
+    const ChainPage& c = cp[q];
+    const uint8_t* b   = file + c.file_off;
+    int64_t x          = ck[g] - B.in[q];
+    for (int t = 0; t < kChainStep; ++t) {
+      const int64_t k = j * kChainStep + t;
+      if (k >= c.elem_cap) {
+        pq_error(err, c.page, kPqErrSnappy);
+        break;
+      }
+      epos[B.elem[q] + k] = x;
+      const int64_t sz    = chain_elem_size(b, x, c.n);
+      if (sz < 0 || x + sz > c.n) {
+        pq_error(err, c.page, kPqErrSnappy);
+        break;
+      }
+      x += sz;
+      if (x == c.n) {
+        st[q].nelem = k + 1;
+        break;
+      }
+    }
+  }
+}
+
+// Every element slot: output length and (copy) offset or (literal) -(body + 1).
+__global__ void chain_decode_kernel(const uint8_t* file, const ChainPage* cp, const ChainState* st, ChainBases B,
+                                    int64_t total_elem, const int64_t* epos, int64_t* elen, int64_t* emeta)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total_elem;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int q     = chain_page_of(B.elem, B.n, g);
+    const int64_t k = g - B.elem[q];
+    if (k >= st[q].nelem) {
+      elen[g]  = 0;
+      emeta[g] = 0;
+      continue;
+    }
+    const ChainPage& c = cp[q];
+    const uint8_t* b   = file + c.file_off;
+    const int64_t x    = epos[g];
+    const uint32_t t   = b[x];
+    int64_t l, meta;
+    if ((t & 3) == 0) {
+      l       = t >> 2;
+      int hdr = 1;
+      if (l >= 60) {
+        const int nb = static_cast<int>(l) - 59;
+        l            = 0;
+        for (int i = 0; i < nb; ++i) l |= static_cast<int64_t>(b[x + 1 + i]) << (8 * i);
+        hdr += nb;
+      }
+      l += 1;
+      meta = -(x + hdr) - 1;
+    } else if ((t & 3) == 1) {
+      l    = 4 + ((t >> 2) & 7);
+      meta = (static_cast<int64_t>(t >> 5) << 8) | b[x + 1];
+    } else {
+      l    = (t >> 2) + 1;
+      meta = (t & 3) == 2 ? (b[x + 1] | b[x + 2] << 8)
+                          : static_cast<int64_t>(static_cast<uint32_t>(b[x + 1]) | static_cast<uint32_t>(b[x + 2]) << 8 |
+                                                 static_cast<uint32_t>(b[x + 3]) << 16 |
+                                                 static_cast<uint32_t>(b[x + 4]) << 24);
+    }
+    elen[g]  = l;
+    emeta[g] = meta;
+  }
+}
+
+// Every output byte: its source, another output byte (>= 0, scratch index) or
+// a file byte (-(offset + 1)).
+__global__ void chain_ptr_kernel(const ChainPage* cp, const ChainState* st, ChainBases B, int64_t total_out,
+                                 const int64_t* eoff, const int64_t* elen, const int64_t* emeta, int64_t* ptr,
+                                 unsigned long long* err)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total_out;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int q        = chain_page_of(B.out, B.n, g);
+    const ChainPage& c = cp[q];
+    const int64_t r    = g - B.out[q];
+    if (r >= c.lv + c.u) {  // alignment padding behind the page
+      ptr[g] = -1;
+      continue;
+    }
+    if (r < c.lv) {  // a v2 page's levels, stored uncompressed
+      ptr[g] = -(c.file_off - c.lv + r) - 1;
+      continue;
+    }
+    const int64_t s  = r - c.lv;
+    const int64_t e0 = B.elem[q], ne = st[q].nelem;
+    if (ne <= 0) {
+      ptr[g] = -1;
+      pq_error(err, c.page, kPqErrSnappy);
+      continue;
+    }
+    const int64_t base = eoff[e0];
+    int64_t lo = 0, hi = ne - 1;  // last element starting at or before s
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (eoff[e0 + mid] - base <= s) lo = mid;
+      else hi = mid - 1;
+    }
+    const int64_t o = eoff[e0 + lo] - base, l = elen[e0 + lo], m = emeta[e0 + lo];
+    if (s >= o + l || (s == o && o + l > c.u) || (m >= 0 && (m == 0 || m > o))) {
+      ptr[g] = -1;
+      pq_error(err, c.page, kPqErrSnappy);
+      continue;
+    }
+    if (m < 0) {
+      ptr[g] = -(c.file_off + (-m - 1) + (s - o)) - 1;
+    } else {
+      const int64_t src = m >= l ? s - m : o - m + (s - o) % m;
+      ptr[g]            = B.out[q] + c.lv + src;
+    }
+  }
+}
+
+__global__ void chain_jump_kernel(const int64_t* in, int64_t* out, int64_t total)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t p = in[g];
+    out[g]          = p >= 0 ? in[p] : p;
+  }
+}
+
+__global__ void chain_final_kernel(const uint8_t* file, const ChainPage* cp, ChainBases B, const int64_t* ptr,
+                                   int64_t total, uint8_t* scratch, unsigned long long* err)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t p = ptr[g];
+    if (p < 0) {
+      scratch[g] = file[-p - 1];
+    } else {
+      scratch[g] = 0;
+      pq_error(err, cp[chain_page_of(B.out, B.n, g)].page, kPqErrSnappy);
+    }
+  }
+}
+
+// Byte-array dictionary pages from kDictChainMinBytes: the chain of length
+// prefixes ranked the same way (next entry at x + 4 + length), each
+// checkpoint's thread writing its entries.
+struct DictChain {
+  int page;
+  const uint8_t* data;  // the page's data (decompressed)
+  int64_t n;            // data bytes
+  int64_t nv;           // entries
+  int64_t entry0;       // first entry in the entry table
+  int64_t ck_cap;
+};
+
+__device__ __forceinline__ int64_t dict_len_at(const uint8_t* d, int64_t x)
+{
+  return static_cast<int64_t>(static_cast<uint32_t>(d[x]) | static_cast<uint32_t>(d[x + 1]) << 8 |
+                              static_cast<uint32_t>(d[x + 2]) << 16 | static_cast<uint32_t>(d[x + 3]) << 24);
+}
+
+__global__ void dict_next_kernel(const DictChain* dc, ChainBases B, int64_t total, int64_t* nxt)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int q        = chain_page_of(B.in, B.n, g);
+    const DictChain& c = dc[q];
+    const int64_t x    = g - B.in[q];
+    int64_t v          = -1;
+    if (x + 4 <= c.n) {
+      const int64_t e = x + 4 + dict_len_at(c.data, x);
+      if (e < c.n) v = B.in[q] + e;
+    }
+    nxt[g] = v;
+  }
+}
+
+__global__ void dict_checkpoints_kernel(const DictChain* dc, ChainBases B, const int64_t* jump, int64_t* ck,
+                                        int64_t* nck)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < B.n; q += gridDim.x * blockDim.x) {
+    const DictChain& c = dc[q];
+    int64_t x          = c.n > 0 ? B.in[q] : -1;
+    int64_t j          = 0;
+    while (x >= 0 && j < c.ck_cap && j * kChainStep < c.nv) {
+      ck[B.ck[q] + j++] = x;
+      x = jump[x];
+    }
+    nck[q] = j;
+  }
+}
+
+__global__ void dict_walk_kernel(const DictChain* dc, ChainBases B, int64_t total_ck, const int64_t* ck,
+                                 const int64_t* nck, int64_t* entry_off, int32_t* entry_len, unsigned long long* err)
+{
+  for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total_ck;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int q     = chain_page_of(B.ck, B.n, g);
+    const int64_t j = g - B.ck[q];
+    const DictChain& c = dc[q];
+    if (j == 0 && nck[q] == 0 && c.nv > 0) pq_error(err, c.page, kPqErrValues);
+    if (j >= nck[q]) continue;
+    int64_t x = ck[g] - B.in[q];
+    for (int t = 0; t < kChainStep; ++t) {
+      const int64_t k = j * kChainStep + t;
+      if (k >= c.nv) break;
+      const int64_t len = x + 4 <= c.n ? dict_len_at(c.data, x) : -1;
+      if (len < 0 || x + 4 + len > c.n) {
+        pq_error(err, c.page, kPqErrValues);
+        break;
+      }
+      entry_off[c.entry0 + k] = x + 4;
+      entry_len[c.entry0 + k] = static_cast<int32_t>(len);
+      x += 4 + len;
+    }
+  }
+}
+
 struct PqColumns {
   int ncols;
   int32_t physical[64];
@@ -852,9 +1255,9 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
   }
   // check the page table, lay out the decompression scratch
   std::vector<int64_t> covered(ncols, 0);
-  std::vector<int> snappy, dict_strings, data_pages;
+  std::vector<int> snappy, chain, dict_strings, dict_chain, data_pages;
   std::vector<int64_t> soff;
-  int64_t scratch_bytes = 0, nentries = 0;
+  int64_t scratch_bytes = 0, nentries = 0, chain_in = 0, dict_in = 0;
   std::vector<PqPage> dev_pages(npages);
   for (int p = 0; p < npages; ++p) {
     const ldf_parquet_page& h = pages[p];
@@ -871,16 +1274,27 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
     dev_pages[p].h          = h;
     dev_pages[p].data_bytes = h.codec == LDF_PQ_SNAPPY ? h.uncompressed : h.compressed;
     if (h.codec == LDF_PQ_SNAPPY) {
-      snappy.push_back(p);
-      soff.push_back(scratch_bytes);
-      scratch_bytes += (h.uncompressed + 15) & ~int64_t(15);
+      const int64_t lv = h.kind == LDF_PQ_DATA_V2 ? h.levels_bytes : 0;
+      if (C.physical[h.column] == LDF_PQ_BYTE_ARRAY && h.uncompressed - lv >= kChainMinBytes &&
+          chain_in + h.compressed <= kChainMaxInput) {
+        chain.push_back(p);  // decoded by the whole GPU (scratch laid out below)
+        chain_in += h.compressed - lv;
+      } else {
+        snappy.push_back(p);
+      }
     }
     if (h.kind == LDF_PQ_DICT_PAGE) {
       LDF_REQUIRE(h.encoding == 0 || h.encoding == 2, "parquet_decode: dictionary pages must be PLAIN");
       if (C.physical[h.column] == LDF_PQ_BYTE_ARRAY) {
         dev_pages[p].dict_entry0 = nentries;
         nentries += h.num_values;
-        dict_strings.push_back(p);
+        const int64_t bytes = dev_pages[p].data_bytes;
+        if (bytes >= kDictChainMinBytes && dict_in + bytes <= kChainMaxInput) {
+          dict_chain.push_back(p);  // ranked by the whole GPU
+          dict_in += bytes;
+        } else {
+          dict_strings.push_back(p);
+        }
       }
     } else {
       LDF_REQUIRE(h.encoding == 0 || h.encoding == 2 || h.encoding == 8 ||
@@ -897,6 +1311,42 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
   }
   for (int j = 0; j < ncols; ++j)
     LDF_REQUIRE(covered[j] == nrows, "parquet_decode: the data pages do not cover every row of a column");
+  // scratch: the chain pages' outputs first (one index space), then the others
+  std::vector<ChainPage> cpages;
+  std::vector<int64_t> cbases;  // in | out | elem | ck, one entry per chain page each
+  int64_t chain_elems = 0, chain_cks = 0, chain_out = 0, chain_maxu = 1;
+  {
+    std::vector<int64_t> in_b, out_b, el_b, ck_b;
+    int64_t in_run = 0;
+    for (int p : chain) {
+      const ldf_parquet_page& h = pages[p];
+      const int64_t lv          = h.kind == LDF_PQ_DATA_V2 ? h.levels_bytes : 0;
+      ChainPage c{};
+      c.page     = p;
+      c.file_off = h.offset + lv;
+      c.n        = h.compressed - lv;
+      c.lv       = lv;
+      c.u        = h.uncompressed - lv;
+      c.elem_cap = c.n / 2 + 1;
+      c.ck_cap   = c.elem_cap / kChainStep + 2;
+      in_b.push_back(in_run);
+      out_b.push_back(scratch_bytes);
+      el_b.push_back(chain_elems);
+      ck_b.push_back(chain_cks);
+      in_run += c.n;
+      chain_elems += c.elem_cap;
+      chain_cks += c.ck_cap;
+      chain_maxu = std::max(chain_maxu, h.uncompressed);
+      scratch_bytes += (h.uncompressed + 15) & ~int64_t(15);
+      cpages.push_back(c);
+    }
+    chain_out = scratch_bytes;
+    for (auto* v : {&in_b, &out_b, &el_b, &ck_b}) cbases.insert(cbases.end(), v->begin(), v->end());
+    for (int p : snappy) {
+      soff.push_back(scratch_bytes);
+      scratch_bytes += (pages[p].uncompressed + 15) & ~int64_t(15);
+    }
+  }
   {  // decompress the largest pages first: a page is one warp's sequential work
     std::vector<int> order(snappy.size());
     for (size_t q = 0; q < order.size(); ++q) order[q] = static_cast<int>(q);
@@ -916,6 +1366,7 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
   cudaStream_t s      = ctx.stream();
   Buffer<uint8_t> scratch(al, std::max<int64_t>(scratch_bytes, 16));
   for (size_t q = 0; q < snappy.size(); ++q) dev_pages[snappy[q]].data = scratch.get() + soff[q];
+  for (size_t q = 0; q < chain.size(); ++q) dev_pages[chain[q]].data = scratch.get() + cbases[chain.size() + q];
   for (int p = 0; p < npages; ++p)
     if (pages[p].codec != LDF_PQ_SNAPPY) dev_pages[p].data = file + pages[p].offset;
   Buffer<PqPage> d_pages(al, std::max(npages, 1));
@@ -948,6 +1399,56 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
   Buffer<int32_t> entry_len(al, std::max<int64_t>(nentries, 1));
   const int nsn = static_cast<int>(snappy.size()), nds = static_cast<int>(dict_strings.size()),
             ndp = static_cast<int>(data_pages.size());
+  if (!chain.empty()) {  // large byte-array pages: the element chains ranked by the whole GPU
+    const int nc          = static_cast<int>(chain.size());
+    const int64_t cin     = chain_in;
+    Buffer<ChainPage> d_cp(al, nc);
+    Buffer<ChainState> d_st(al, nc);
+    Buffer<int64_t> d_cb(al, cbases.size());
+    LDF_CUDA(cudaMemcpyAsync(d_cp.get(), cpages.data(), nc * sizeof(ChainPage), cudaMemcpyHostToDevice, s));
+    LDF_CUDA(cudaMemcpyAsync(d_cb.get(), cbases.data(), cbases.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    const ChainBases B{d_cb.get(), d_cb.get() + nc, d_cb.get() + 2 * nc, d_cb.get() + 3 * nc, nc};
+    Buffer<int64_t> j0(al, cin), j1(al, cin), j2(al, cin);
+    launch("chain_start", chain_start_kernel, pq_blocks(nc, 128), 128, 0, s, file,
+           static_cast<const ChainPage*>(d_cp.get()), d_st.get(), nc, d_err.get());
+    launch("chain_next", chain_next_kernel, pq_blocks(cin, 256), 256, 0, s, file,
+           static_cast<const ChainPage*>(d_cp.get()), static_cast<const ChainState*>(d_st.get()), B, cin, j0.get());
+    const int64_t* jump = j0.get();
+    for (int r = 0; r < kChainLog; ++r) {
+      int64_t* out = (r % 2 == 0) ? j1.get() : j2.get();
+      launch("chain_double", chain_double_kernel, pq_blocks(cin, 256), 256, 0, s, jump, out, cin);
+      jump = out;
+    }
+    Buffer<int64_t> ck(al, chain_cks);
+    launch("chain_checkpoints", chain_checkpoints_kernel, pq_blocks(nc, 128), 128, 0, s,
+           static_cast<const ChainPage*>(d_cp.get()), d_st.get(), B, jump, ck.get());
+    Buffer<int64_t> epos(al, chain_elems), elen(al, chain_elems), emeta(al, chain_elems), eoff(al, chain_elems);
+    launch("chain_walk", chain_walk_kernel, pq_blocks(chain_cks, 128), 128, 0, s, file,
+           static_cast<const ChainPage*>(d_cp.get()), d_st.get(), B, chain_cks, static_cast<const int64_t*>(ck.get()),
+           epos.get(), d_err.get());
+    launch("chain_decode", chain_decode_kernel, pq_blocks(chain_elems, 256), 256, 0, s, file,
+           static_cast<const ChainPage*>(d_cp.get()), static_cast<const ChainState*>(d_st.get()), B, chain_elems,
+           static_cast<const int64_t*>(epos.get()), elen.get(), emeta.get());
+    Buffer<int64_t> etotal(al, 1);
+    exclusive_scan_i64(elen.get(), eoff.get(), chain_elems, etotal.get(), ctx);
+    Buffer<int64_t> p0(al, chain_out), p1(al, chain_out);
+    launch("chain_ptr", chain_ptr_kernel, pq_blocks(chain_out, 256), 256, 0, s,
+           static_cast<const ChainPage*>(d_cp.get()), static_cast<const ChainState*>(d_st.get()), B, chain_out,
+           static_cast<const int64_t*>(eoff.get()), static_cast<const int64_t*>(elen.get()),
+           static_cast<const int64_t*>(emeta.get()), p0.get(), d_err.get());
+    int rounds = 1;  // every pointer moves back one byte or more: log2 of the page size rounds reach a literal
+    while ((int64_t(1) << rounds) <= chain_maxu) ++rounds;
+    int64_t* pin = p0.get();
+    int64_t* pout = p1.get();
+    for (int r = 0; r < rounds; ++r) {
+      launch("chain_jump", chain_jump_kernel, pq_blocks(chain_out, 256), 256, 0, s,
+             static_cast<const int64_t*>(pin), pout, chain_out);
+      std::swap(pin, pout);
+    }
+    launch("chain_final", chain_final_kernel, pq_blocks(chain_out, 256), 256, 0, s, file,
+           static_cast<const ChainPage*>(d_cp.get()), B, static_cast<const int64_t*>(pin), chain_out, scratch.get(),
+           d_err.get());
+  }
   if (nsn > 0)
     launch("pq_snappy", pq_snappy_kernel, static_cast<unsigned>(nsn), kLanes, 0, s,
            file, d_pages.get(), static_cast<const int*>(d_lists.get()), nsn, scratch.get(),
@@ -956,6 +1457,47 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
     launch("pq_dict_strings", pq_dict_strings_kernel, static_cast<unsigned>(nds), kPqThreads, 0, s,
            static_cast<const PqPage*>(d_pages.get()), static_cast<const int*>(d_lists.get()) + nsn, nds,
            entry_off.get(), entry_len.get(), d_err.get());
+  if (!dict_chain.empty()) {  // large dictionary pages: the length-prefix chains ranked by the whole GPU
+    const int nc = static_cast<int>(dict_chain.size());
+    std::vector<DictChain> dc;
+    std::vector<int64_t> in_b, ck_b;
+    int64_t in_run = 0, ck_run = 0;
+    for (int p : dict_chain) {
+      DictChain c{};
+      c.page   = p;
+      c.data   = dev_pages[p].data;
+      c.n      = dev_pages[p].data_bytes;
+      c.nv     = pages[p].num_values;
+      c.entry0 = dev_pages[p].dict_entry0;
+      c.ck_cap = c.nv / kChainStep + 2;
+      in_b.push_back(in_run);
+      ck_b.push_back(ck_run);
+      in_run += c.n;
+      ck_run += c.ck_cap;
+      dc.push_back(c);
+    }
+    std::vector<int64_t> bases(in_b);
+    bases.insert(bases.end(), ck_b.begin(), ck_b.end());
+    Buffer<DictChain> d_dc(al, nc);
+    Buffer<int64_t> d_b(al, bases.size()), d_nck(al, nc), ck(al, ck_run);
+    LDF_CUDA(cudaMemcpyAsync(d_dc.get(), dc.data(), nc * sizeof(DictChain), cudaMemcpyHostToDevice, s));
+    LDF_CUDA(cudaMemcpyAsync(d_b.get(), bases.data(), bases.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    const ChainBases B{d_b.get(), nullptr, nullptr, d_b.get() + nc, nc};
+    Buffer<int64_t> j0(al, in_run), j1(al, in_run), j2(al, in_run);
+    launch("dict_next", dict_next_kernel, pq_blocks(in_run, 256), 256, 0, s,
+           static_cast<const DictChain*>(d_dc.get()), B, in_run, j0.get());
+    const int64_t* jump = j0.get();
+    for (int r = 0; r < kChainLog; ++r) {
+      int64_t* out = (r % 2 == 0) ? j1.get() : j2.get();
+      launch("chain_double", chain_double_kernel, pq_blocks(in_run, 256), 256, 0, s, jump, out, in_run);
+      jump = out;
+    }
+    launch("dict_checkpoints", dict_checkpoints_kernel, pq_blocks(nc, 128), 128, 0, s,
+           static_cast<const DictChain*>(d_dc.get()), B, jump, ck.get(), d_nck.get());
+    launch("dict_walk", dict_walk_kernel, pq_blocks(ck_run, 128), 128, 0, s,
+           static_cast<const DictChain*>(d_dc.get()), B, ck_run, static_cast<const int64_t*>(ck.get()),
+           static_cast<const int64_t*>(d_nck.get()), entry_off.get(), entry_len.get(), d_err.get());
+  }
   if (ndp > 0)
     launch("pq_data", pq_data_kernel, static_cast<unsigned>(ndp), kPqThreads, 0, s,
            static_cast<const PqPage*>(d_pages.get()), static_cast<const int*>(d_lists.get()) + nsn + nds, C,

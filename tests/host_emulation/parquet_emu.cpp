@@ -84,41 +84,123 @@ int main(int argc, char** argv)
       C.str_len[j] = slen[j].data();
     }
   }
-  // page table and lists, as parquet_decode lays them out
+  // page table and lists, as parquet_decode lays them out (chain pages first in scratch)
   std::vector<PqPage> dp(std::max(npages, 1));
-  std::vector<int> snappy, dict_strings, data_pages;
+  std::vector<int> snappy, chain, dict_strings, dict_chain, data_pages;
   std::vector<int64_t> soff;
-  int64_t scratch_bytes = 0, nentries = 0;
+  int64_t scratch_bytes = 0, nentries = 0, chain_in = 0, dict_in = 0;
   for (int p = 0; p < npages; ++p) {
     const ldf_parquet_page& h = pages[p];
     dp[p].h          = h;
     dp[p].data_bytes = h.codec == LDF_PQ_SNAPPY ? h.uncompressed : h.compressed;
     if (h.codec == LDF_PQ_SNAPPY) {
-      snappy.push_back(p);
-      soff.push_back(scratch_bytes);
-      scratch_bytes += (h.uncompressed + 15) & ~int64_t(15);
+      const int64_t lv = h.kind == LDF_PQ_DATA_V2 ? h.levels_bytes : 0;
+      if (C.physical[h.column] == LDF_PQ_BYTE_ARRAY && h.uncompressed - lv >= kChainMinBytes &&
+          chain_in + h.compressed <= kChainMaxInput) {
+        chain.push_back(p);
+        chain_in += h.compressed - lv;
+      } else {
+        snappy.push_back(p);
+      }
     }
     if (h.kind == LDF_PQ_DICT_PAGE) {
       if (C.physical[h.column] == LDF_PQ_BYTE_ARRAY) {
         dp[p].dict_entry0 = nentries;
         nentries += h.num_values;
-        dict_strings.push_back(p);
+        const int64_t bytes = dp[p].data_bytes;
+        if (bytes >= kDictChainMinBytes && dict_in + bytes <= kChainMaxInput) {
+          dict_chain.push_back(p);
+          dict_in += bytes;
+        } else {
+          dict_strings.push_back(p);
+        }
       }
     } else {
       data_pages.push_back(p);
     }
   }
+  std::vector<ChainPage> cpages;
+  std::vector<int64_t> in_b, out_b, el_b, ck_b;
+  int64_t chain_elems = 0, chain_cks = 0, chain_maxu = 1, in_run = 0;
+  for (int p : chain) {
+    const ldf_parquet_page& h = pages[p];
+    const int64_t lv          = h.kind == LDF_PQ_DATA_V2 ? h.levels_bytes : 0;
+    ChainPage c{};
+    c.page     = p;
+    c.file_off = h.offset + lv;
+    c.n        = h.compressed - lv;
+    c.lv       = lv;
+    c.u        = h.uncompressed - lv;
+    c.elem_cap = c.n / 2 + 1;
+    c.ck_cap   = c.elem_cap / kChainStep + 2;
+    in_b.push_back(in_run);
+    out_b.push_back(scratch_bytes);
+    el_b.push_back(chain_elems);
+    ck_b.push_back(chain_cks);
+    in_run += c.n;
+    chain_elems += c.elem_cap;
+    chain_cks += c.ck_cap;
+    chain_maxu = std::max<int64_t>(chain_maxu, h.uncompressed);
+    scratch_bytes += (h.uncompressed + 15) & ~int64_t(15);
+    cpages.push_back(c);
+  }
+  const int64_t chain_out = scratch_bytes;
+  for (int p : snappy) {
+    soff.push_back(scratch_bytes);
+    scratch_bytes += (pages[p].uncompressed + 15) & ~int64_t(15);
+  }
   std::vector<uint8_t> scratch(std::max<int64_t>(scratch_bytes, 16));
   for (size_t q = 0; q < snappy.size(); ++q) dp[snappy[q]].data = scratch.data() + soff[q];
+  for (size_t q = 0; q < chain.size(); ++q) dp[chain[q]].data = scratch.data() + out_b[q];
   for (int p = 0; p < npages; ++p)
     if (pages[p].codec != LDF_PQ_SNAPPY) dp[p].data = file.data() + pages[p].offset;
+  unsigned long long err = ~0ull;
+  if (!chain.empty()) {  // the chain kernels: one thread runs each grid-stride loop
+    blockIdx.x = 0;
+    const int nc = (int)chain.size();
+    const ChainBases B{in_b.data(), out_b.data(), el_b.data(), ck_b.data(), nc};
+    std::vector<ChainState> st(nc);
+    const int64_t cin = in_run;
+    std::vector<int64_t> j0(std::max<int64_t>(cin, 1)), j1(j0.size()), j2(j0.size());
+    chain_start_kernel(file.data(), cpages.data(), st.data(), nc, &err);
+    chain_next_kernel(file.data(), cpages.data(), st.data(), B, cin, j0.data());
+    const int64_t* jump = j0.data();
+    for (int r = 0; r < kChainLog; ++r) {
+      int64_t* out = (r % 2 == 0) ? j1.data() : j2.data();
+      chain_double_kernel(jump, out, cin);
+      jump = out;
+    }
+    std::vector<int64_t> ck(std::max<int64_t>(chain_cks, 1));
+    chain_checkpoints_kernel(cpages.data(), st.data(), B, jump, ck.data());
+    std::vector<int64_t> epos(std::max<int64_t>(chain_elems, 1)), elen(epos.size()), emeta(epos.size()),
+      eoff(epos.size());
+    chain_walk_kernel(file.data(), cpages.data(), st.data(), B, chain_cks, ck.data(), epos.data(), &err);
+    chain_decode_kernel(file.data(), cpages.data(), st.data(), B, chain_elems, epos.data(), elen.data(),
+                        emeta.data());
+    int64_t run = 0;
+    for (int64_t k = 0; k < chain_elems; ++k) {
+      eoff[k] = run;
+      run += elen[k];
+    }
+    std::vector<int64_t> p0(std::max<int64_t>(chain_out, 1)), p1(p0.size());
+    chain_ptr_kernel(cpages.data(), st.data(), B, chain_out, eoff.data(), elen.data(), emeta.data(), p0.data(),
+                     &err);
+    int rounds = 1;
+    while ((int64_t(1) << rounds) <= chain_maxu) ++rounds;
+    int64_t* pin  = p0.data();
+    int64_t* pout = p1.data();
+    for (int r = 0; r < rounds; ++r) {
+      chain_jump_kernel(pin, pout, chain_out);
+      std::swap(pin, pout);
+    }
+    chain_final_kernel(file.data(), cpages.data(), B, pin, chain_out, scratch.data(), &err);
+  }
   std::vector<int> lists;
   lists.insert(lists.end(), snappy.begin(), snappy.end());
   lists.insert(lists.end(), dict_strings.begin(), dict_strings.end());
   lists.insert(lists.end(), data_pages.begin(), data_pages.end());
   std::vector<int64_t> entry_off(std::max<int64_t>(nentries, 1));
   std::vector<int32_t> entry_len(std::max<int64_t>(nentries, 1));
-  unsigned long long err = ~0ull;
   for (unsigned b = 0; b < snappy.size(); ++b) {
     blockIdx.x = b;
     pq_snappy_kernel(file.data(), dp.data(), lists.data(), (int)snappy.size(), scratch.data(), soff.data(), &err);
@@ -127,6 +209,38 @@ int main(int argc, char** argv)
   if (!dict_strings.empty())
     pq_dict_strings_kernel(dp.data(), lists.data() + snappy.size(), (int)dict_strings.size(), entry_off.data(),
                            entry_len.data(), &err);
+  if (!dict_chain.empty()) {  // the dictionary chain kernels, one thread each loop
+    blockIdx.x   = 0;
+    const int nc = (int)dict_chain.size();
+    std::vector<DictChain> dc;
+    std::vector<int64_t> in_b, ck_b;
+    int64_t in_run = 0, ck_run = 0;
+    for (int p : dict_chain) {
+      DictChain c{};
+      c.page   = p;
+      c.data   = dp[p].data;
+      c.n      = dp[p].data_bytes;
+      c.nv     = pages[p].num_values;
+      c.entry0 = dp[p].dict_entry0;
+      c.ck_cap = c.nv / kChainStep + 2;
+      in_b.push_back(in_run);
+      ck_b.push_back(ck_run);
+      in_run += c.n;
+      ck_run += c.ck_cap;
+      dc.push_back(c);
+    }
+    const ChainBases B{in_b.data(), nullptr, nullptr, ck_b.data(), nc};
+    std::vector<int64_t> j0(std::max<int64_t>(in_run, 1)), j1(j0.size()), j2(j0.size()), ck(ck_run), nck(nc);
+    dict_next_kernel(dc.data(), B, in_run, j0.data());
+    const int64_t* jump = j0.data();
+    for (int r = 0; r < kChainLog; ++r) {
+      int64_t* out = (r % 2 == 0) ? j1.data() : j2.data();
+      chain_double_kernel(jump, out, in_run);
+      jump = out;
+    }
+    dict_checkpoints_kernel(dc.data(), B, jump, ck.data(), nck.data());
+    dict_walk_kernel(dc.data(), B, ck_run, ck.data(), nck.data(), entry_off.data(), entry_len.data(), &err);
+  }
   for (unsigned b = 0; b < data_pages.size(); ++b) {
     blockIdx.x = b;
     pq_data_kernel(dp.data(), lists.data() + snappy.size() + dict_strings.size(), C, entry_off.data(),

@@ -43,7 +43,11 @@ def _section() -> str:
                  ("constexpr int kSnapWin   = 32768;", "constexpr int kSnapWin   = 256;"),
                  ("constexpr int kSnapBatchBytes = 1024;", "constexpr int kSnapBatchBytes = 64;"),
                  ("constexpr int kSnapShort      = 64;", "constexpr int kSnapShort      = 16;"),
-                 ("constexpr int kDictStage = 8192;", "constexpr int kDictStage = 32;")):
+                 ("constexpr int kDictStage = 8192;", "constexpr int kDictStage = 32;"),
+                 # most byte-array pages through the chain path, four elements between checkpoints
+                 ("constexpr int64_t kChainMinBytes = 131072;", "constexpr int64_t kChainMinBytes = 200;"),
+                 ("constexpr int64_t kDictChainMinBytes = 16384;", "constexpr int64_t kDictChainMinBytes = 100;"),
+                 ("constexpr int kChainLog          = 8;", "constexpr int kChainLog          = 2;")):
         assert a in sec, a
         sec = sec.replace(a, b)
     return sec
@@ -240,3 +244,55 @@ def test_snappy_overlapping_and_far_copies(emu, tmp_path):
     path = tmp_path / "s.parquet"
     pq.write_table(t, path, use_dictionary=False, compression="snappy", data_page_size=64 * 1024)
     same(decode(emu, path, tmp_path), expected(path))
+
+
+def _emu_run(exe, path, tmp_path, columns=None):
+    import sys
+
+    sys.path.insert(0, str(ROOT / "legate-dataframe_b200"))
+    from legate_dataframe.lib import parquet as P
+
+    pf = pq.ParquetFile(path)
+    names, idx, physical, types, nullable, _ = P._column_specs(pf, columns)
+    spec = [v for triple in zip(physical, types, nullable) for v in triple]
+    data = np.fromfile(path, dtype=np.uint8)
+    pages, npages = P._page_table(data, pf.metadata, idx, spec[0::3])
+    blob = struct.pack("<4q", len(data), npages, len(idx), pf.metadata.num_rows) + data.tobytes()
+    blob += bytes(memoryview(pages))[: npages * 64] + struct.pack(f"<{len(spec)}i", *spec)
+    inp = tmp_path / "emu_bad.bin"
+    inp.write_bytes(blob)
+    r = subprocess.run([str(exe), str(inp)], capture_output=True)
+    assert r.returncode == 0, r.stderr.decode()[-3000:]
+    return r.stdout.decode().splitlines()[0], [(pages[k].offset, pages[k].uncompressed, pages[k].kind)
+                                              for k in range(npages)]
+
+
+@pytest.mark.parametrize("target", ["chain", "warp"])
+def test_malformed_snappy_page_is_reported(emu, tmp_path, target):
+    """A first element that copies from before the stream's start makes the
+    decode fail with that page's number, through the chain kernels (pages
+    from 200 bytes here) and through the per-page kernel."""
+    rng = np.random.default_rng(11)
+    words = np.array([f"m{i:05d}" + "q" * (i % 7) for i in range(4000)], dtype=object)
+    t = pa.table({"s": pa.array(words[rng.integers(0, len(words), 6000)])})
+    path = tmp_path / "m.parquet"
+    pq.write_table(t, path, compression="snappy", data_page_size=4096)
+    first, pages = _emu_run(emu, path, tmp_path)
+    assert first.startswith("rows")
+    big = [k for k, (_, u, kind) in enumerate(pages) if u >= 200]
+    small = [k for k, (_, u, kind) in enumerate(pages) if u < 200]
+    if target == "warp" and not small:  # make one: a tiny file of one short page
+        t = pa.table({"s": pa.array(["ab", "ab", "abab", "x"] * 3)})
+        pq.write_table(t, path, compression="snappy", use_dictionary=False)
+        first, pages = _emu_run(emu, path, tmp_path)
+        small = [k for k, (_, u, kind) in enumerate(pages) if u < 200]
+    k = (big if target == "chain" else small)[0]
+    data = np.fromfile(path, dtype=np.uint8)
+    i = pages[k][0]
+    while data[i] & 0x80:
+        i += 1
+    data[i + 1] = 0x01
+    data[i + 2] = 0x05
+    data.tofile(path)
+    first, _ = _emu_run(emu, path, tmp_path)
+    assert first == f"error 1 {k}", first

@@ -102,3 +102,80 @@ def test_parquet_not_on_device_reads_through_arrow(tmp_path):
     q = tmp_path / "n.parquet"
     pq.write_table(nested, q)
     assert device_read([q], ["a"]).column("a").to_pylist() == [1, 2]
+
+
+def _big_string_pages(tmp_path, compression, dictionary, version="1.0"):
+    """A file whose byte-array pages are large enough for the chain path
+    (dictionary pages of ~1 MB, PLAIN pages of ~1 MB) mixed with small ones."""
+    rng = np.random.default_rng(8)
+    n = 300_000
+    words = np.array([f"k{i:07d}-" + "z" * (i % 11) for i in range(120_000)], dtype=object)
+    t = pa.table({"s": pa.array(words[rng.integers(0, len(words), n)], mask=rng.random(n) < 0.05),
+                  "run": pa.array(np.repeat(np.array(["aaaa" * 20, "b", ""], dtype=object), n // 3)),
+                  "x": pa.array(rng.integers(0, 2**40, n))})
+    p = tmp_path / f"big_{compression}_{dictionary}_{version}.parquet"
+    pq.write_table(t, p, compression=compression, use_dictionary=dictionary, data_page_version=version,
+                   row_group_size=150_000)
+    return p
+
+
+@pytest.mark.parametrize("compression", ["snappy", "none"])
+@pytest.mark.parametrize("dictionary", [True, False])
+@pytest.mark.parametrize("version", ["1.0", "2.0"])
+def test_parquet_large_byte_array_pages(tmp_path, compression, dictionary, version):
+    """Pages decoded by the whole GPU (Snappy element chains and dictionary
+    length-prefix chains ranked in parallel) beside the per-page kernels."""
+    p = _big_string_pages(tmp_path, compression, dictionary, version)
+    assert_tables_equal(device_read([p]), pq.read_table(p), sort_by=None)
+
+
+def _first_pages(path, column):
+    """(payload offset, compressed bytes, kind, uncompressed bytes) of every page of a column."""
+    from legate_dataframe.lib import parquet as P
+
+    pf = pq.ParquetFile(path)
+    _, idx, physical, _, _, _ = P._column_specs(pf, [column])
+    data = np.fromfile(path, dtype=np.uint8)
+    pages, n = P._page_table(data, pf.metadata, idx, physical)
+    return data, [(pages[k].offset, pages[k].compressed, pages[k].kind, pages[k].uncompressed) for k in range(n)]
+
+
+@pytest.mark.parametrize("which", ["chain_dictionary", "warp_data"])
+def test_parquet_malformed_snappy_page_raises(tmp_path, which):
+    """A Snappy stream whose first element copies from before the start is
+    rejected with the page number, on both decoding paths."""
+    p = _big_string_pages(tmp_path, "snappy", True)
+    data, pages = _first_pages(p, "s")
+    if which == "chain_dictionary":  # large enough for the chain path
+        off, size, _, _ = next(pg for pg in pages if pg[2] == 0 and pg[3] >= 131072)
+    else:  # small enough for the per-page kernel
+        off, size, _, _ = next(pg for pg in pages if pg[2] != 0 and pg[3] < 131072)
+    i = off
+    while data[i] & 0x80:  # the length preamble
+        i += 1
+    data[i + 1] = 0x01  # a copy of 4 bytes at offset 0 * 256 + next byte, before any output
+    data[i + 2] = 0x05
+    q = tmp_path / "bad.parquet"
+    data.tofile(q)
+    with pytest.raises(ValueError, match="Parquet page"):
+        device_read([q], ["s"])
+
+
+def test_parquet_truncated_dictionary_raises(tmp_path):
+    """An uncompressed dictionary page whose last length prefix runs past
+    its data (the chain path for large dictionaries) is rejected."""
+    p = _big_string_pages(tmp_path, "none", True)
+    data, pages = _first_pages(p, "s")
+    off, size, _, _ = next(pg for pg in pages if pg[2] == 0)
+    assert size >= 16384
+    x = off
+    while x + 4 <= off + size:  # walk to the last entry
+        ln = int(data[x]) | int(data[x + 1]) << 8 | int(data[x + 2]) << 16 | int(data[x + 3]) << 24
+        if x + 4 + ln >= off + size:
+            break
+        x += 4 + ln
+    data[x + 3] = 0x7F  # its length now runs far past the page
+    q = tmp_path / "trunc.parquet"
+    data.tofile(q)
+    with pytest.raises(ValueError, match="Parquet page"):
+        device_read([q], ["s"])
