@@ -1209,14 +1209,61 @@ __global__ void __launch_bounds__(kPqThreads) pq_data_kernel(const PqPage* pages
 }
 
 // Characters of one string column: row i's bytes at offs[i], local ranges.
-__global__ void pq_copy_strings_kernel(const uint8_t* const* src, const int64_t* len, const int64_t* offs, int64_t rows,
-                                       uint8_t* chars, ldf_range* ranges)
+// A block takes kPqStrRows rows a thread; every thread reads its strings
+// eight bytes at a time with the loads in flight together into a shared
+// stage laid out at the output's 16-byte phase, and the block writes the
+// stage with 16-byte stores (the range's two end chunks, shared with the
+// neighbouring tiles, byte by byte).  A tile whose characters exceed the
+// stage writes them directly.
+constexpr int kPqStrRows  = 2;
+constexpr int kPqStrStage = 16 * 1024;
+struct alignas(16) PqStrStage {
+  uint8_t b[kPqStrStage];
+};
+
+__global__ void __launch_bounds__(256) pq_copy_strings_kernel(const uint8_t* const* src, const int64_t* len,
+                                                              const int64_t* offs, int64_t rows, int64_t nchars,
+                                                              uint8_t* chars, ldf_range* ranges)
 {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t o = offs[i], n = len[i];
-    ranges[i]       = ldf_range{o, o + n - 1};
-    const uint8_t* s = src[i];
-    for (int64_t k = 0; k < n; ++k) chars[o + k] = s[k];
+  __shared__ PqStrStage stage;
+  const int64_t per_tile = static_cast<int64_t>(blockDim.x) * kPqStrRows;
+  for (int64_t tile = blockIdx.x; tile * per_tile < rows; tile += gridDim.x) {
+    const int64_t i0 = tile * per_tile;
+    const int64_t lo = offs[i0];
+    const int64_t hi = i0 + per_tile < rows ? offs[i0 + per_tile] : nchars;
+    // stage.b[k] <-> chars[abase + k], with chars + abase 16-byte aligned
+    const int64_t abase = lo - static_cast<int64_t>(reinterpret_cast<uintptr_t>(chars + lo) & 15);
+    const bool staged   = hi - abase <= kPqStrStage;
+    for (int j = 0; j < kPqStrRows; ++j) {
+      const int64_t i = i0 + j * blockDim.x + threadIdx.x;
+      if (i >= rows) continue;
+      const int64_t o = offs[i], n = len[i];
+      ranges[i]        = ldf_range{o, o + n - 1};
+      const uint8_t* s = src[i];
+      uint8_t* q       = staged ? stage.b + (o - abase) : chars + o;
+      for (int64_t k = 0; k < n; k += 8) {
+        uint8_t b[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) b[u] = k + u < n ? s[k + u] : 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (k + u < n) q[k + u] = b[u];
+      }
+    }
+    if (staged) {
+      __syncthreads();
+      const int64_t nchunks = (hi - abase + 15) >> 4;  // chunk c: chars [abase + 16c, abase + 16c + 16)
+      for (int64_t c = threadIdx.x; c < nchunks; c += blockDim.x) {
+        const int64_t a0 = abase + 16 * c;
+        if (a0 >= lo && a0 + 16 <= hi) {
+          copy16(chars + a0, stage.b + 16 * c);
+        } else {
+          for (int k = 0; k < 16; ++k)
+            if (a0 + k >= lo && a0 + k < hi) chars[a0 + k] = stage.b[16 * c + k];
+        }
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -1524,9 +1571,9 @@ void parquet_decode(const uint8_t* file, int64_t file_bytes, const ldf_parquet_p
     out[j].num_chars     = nchars;
     out[j].chars_base    = 0;
     if (nrows > 0)
-      launch("pq_strings", pq_copy_strings_kernel, pq_blocks(nrows, 256), 256, 0, s,
+      launch("pq_strings", pq_copy_strings_kernel, pq_blocks(ceil_div(nrows, kPqStrRows), 256), 256, 0, s,
              static_cast<const uint8_t* const*>(C.str_src[j]), static_cast<const int64_t*>(C.str_len[j]),
-             static_cast<const int64_t*>(offs.get()), nrows, reinterpret_cast<uint8_t*>(out[j].chars),
+             static_cast<const int64_t*>(offs.get()), nrows, nchars, reinterpret_cast<uint8_t*>(out[j].chars),
              static_cast<ldf_range*>(out[j].data));
   }
   ctx.finish();

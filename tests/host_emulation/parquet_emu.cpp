@@ -264,7 +264,7 @@ int main(int argc, char** argv)
       }
       chars.assign(std::max<int64_t>(o, 1), 0);
       blockIdx.x = 0;
-      pq_copy_strings_kernel(ssrc[j].data(), slen[j].data(), offs.data(), nrows, chars.data(), ranges.data());
+      pq_copy_strings_kernel(ssrc[j].data(), slen[j].data(), offs.data(), nrows, o, chars.data(), ranges.data());
     }
     for (int64_t r = 0; r < nrows; ++r) {
       if (C.nullable[j] && !valid[j][r]) {
