@@ -63,3 +63,25 @@ def test_distinct_special_floats():
     t, _, _ = special_float_tables()
     res = run_distinct(t, ["k"])
     assert res.num_rows == 5  # 0.0, -0.0, NaN, -NaN, 1.0 (bit-pattern keys, as Arrow's grouper)
+
+
+def test_distinct_known_answer():
+    """The reference's hard-coded answer (cpp/tests/test_stream_compaction.cpp:50-74):
+    distinct on ("a", "b"), then sorted by (a asc, b desc, c asc) with nulls
+    first, through this library's own sort."""
+    from legate_dataframe import LogicalTable
+    from legate_dataframe.lib.sort import sort
+    from legate_dataframe.lib.stream_compaction import distinct
+
+    t = pa.table({"a": pa.array([0, 0, 0, 1, 1, 1], pa.int32(), mask=np.array([1, 1, 1, 0, 0, 0], bool)),
+                  "b": pa.array(["this", "this", "string", "string", "col", "col"]),
+                  "c": pa.array([0, 0, 2, 3, 4, 4], pa.float64())})
+    res = distinct(LogicalTable.from_arrow(t), ["a", "b"])
+    got = sort(res, ["a", "b", "c"], sort_ascending=[True, False, True], nulls_at_end=False).to_arrow()
+    exp = pa.table({"a": pa.array([0, 0, 1, 1], pa.int32(), mask=np.array([1, 1, 0, 0], bool)),
+                    "b": pa.array(["this", "string", "string", "col"]),
+                    "c": pa.array([0, 2, 3, 4], pa.float64())})
+    assert got.column_names == exp.column_names
+    for name in exp.column_names:
+        assert got.column(name).to_pylist() == exp.column(name).to_pylist(), name
+    assert got.schema.field("a").type == pa.int32() and got.schema.field("c").type == pa.float64()
