@@ -183,3 +183,13 @@ def test_oracle_float_sums_with_infinities_vs_arrow():
     t = pa.table({"k": k, "v": v})
     aggs = [("v", "sum", "s"), ("v", "mean", "m")]
     assert_tables_equal(R.groupby(t, ["k"], aggs), A.groupby(t, ["k"], aggs), sort_by=["k"])
+
+
+def test_oracle_distinct_known_answer():
+    """The oracle's distinct keys (its groupby with no aggregation) against the
+    reference's hard-coded answer (cpp/tests/test_stream_compaction.cpp:50-74)."""
+    t = pa.table({"a": pa.array([0, 0, 0, 1, 1, 1], pa.int32(), mask=np.array([1, 1, 1, 0, 0, 0], bool)),
+                  "b": pa.array(["this", "this", "string", "string", "col", "col"])})
+    got = R.sort(R.groupby(t, ["a", "b"], []), ["a", "b"], ascending=[True, False], nulls_at_end=False)
+    assert got.column("a").to_pylist() == [None, None, 1, 1]
+    assert got.column("b").to_pylist() == ["this", "string", "string", "col"]
