@@ -412,6 +412,20 @@ __device__ __forceinline__ void zero_fixed(void* dst, int64_t di, int w)
   }
 }
 
+// Prefetch bytes [lo, hi) of a buffer into L2 with one bulk-copy-engine
+// instruction (cp.async.bulk.prefetch.L2, no registers held while it is in
+// flight).  The range is shrunk inward to 16-byte bounds, as the instruction
+// requires, so no byte outside [lo, hi) is touched; a range under 16 bytes is
+// skipped.  A hint only: the data is still loaded by the caller.
+__device__ __forceinline__ void l2_prefetch_bulk(const void* base, int64_t lo, int64_t hi)
+{
+  const uint64_t b0 = reinterpret_cast<uint64_t>(base);
+  const uint64_t a  = (b0 + static_cast<uint64_t>(lo) + 15) & ~15ull;
+  const uint64_t e  = (b0 + static_cast<uint64_t>(hi)) & ~15ull;
+  if (e <= a || e - a > 0xfffffff0ull) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(static_cast<uint32_t>(e - a)) : "memory");
+}
+
 // Bounded spin budget for device-side waits (look-back).  A wait that runs
 // out sets the call's error word and returns; it never traps or hangs.
 constexpr uint32_t kSpinLimit = 1u << 22;

@@ -213,7 +213,22 @@ struct PassArgs {
   RadixPayload pay;  // columns moved by this pass (payload_empty: none)
   FusedKey fused;    // FUSED passes
   int* err;
+  // > 0: each tile stages in L2, by bulk prefetches, the rows of the tile
+  // this many tiles ahead (about one wave of resident CTAs; tiles are taken
+  // in order): the row ids and carried words of a pass on the carried word,
+  // and the key columns of a first pass over rows in input order
+  // (pf_columns).
+  int64_t pf_ahead;
+  int pf_columns;
 };
+
+// L2 prefetch of rows [lo, hi) of a fixed-width column and its validity.
+__device__ __forceinline__ void prefetch_column(const DCol& c, int64_t lo, int64_t hi)
+{
+  if (c.type == LDF_STRING || c.data == nullptr) return;
+  l2_prefetch_bulk(c.data, lo * c.width, hi * c.width);
+  if (c.valid) l2_prefetch_bulk(c.valid, lo, hi);
+}
 
 // Rows of a thread whose payload loads are issued together in a pass that
 // moves columns.
@@ -567,6 +582,27 @@ __device__ __forceinline__ void load_tile_rows(const PassArgs& a, int64_t tile, 
   }
 }
 
+// Tiles ahead that a onesweep tile prefetches into L2 (one wave of resident
+// CTAs); LDF_B200_L2_PREFETCH=0 turns the prefetch off.
+int64_t prefetch_tiles()
+{
+  static const bool off = [] {
+    const char* e = std::getenv("LDF_B200_L2_PREFETCH");
+    return e != nullptr && std::atoi(e) == 0;
+  }();
+  return off ? 0 : static_cast<int64_t>(num_sms()) * kRadixMinBlocks;
+}
+// Whether a first pass over rows in input order prefetches its key columns
+// (LDF_B200_L2_PREFETCH_FIRST=0 turns it off).
+int prefetch_first_pass()
+{
+  static const bool off = [] {
+    const char* e = std::getenv("LDF_B200_L2_PREFETCH_FIRST");
+    return e != nullptr && std::atoi(e) == 0;
+  }();
+  return off ? 0 : 1;
+}
+
 // One tile per CTA.  WRITE_KEYS: later passes of the same word follow, so
 // carry the word along.  MOVE: the pass also moves a.pay's columns (the last
 // pass only, which carries no word).
@@ -586,6 +622,22 @@ __global__ void __launch_bounds__(RT, kRadixMinBlocks) onesweep_kernel(PassArgs 
   uint64_t key[RI];
   int32_t val[RI];
   uint32_t dr[RI];
+  if (a.pf_ahead > 0 && threadIdx.x == 0 && (tile + a.pf_ahead) * RTILE < a.n) {
+    const int64_t lo = (tile + a.pf_ahead) * RTILE;
+    const int64_t hi = min(lo + static_cast<int64_t>(RTILE), a.n);
+    if (!GATHER) {
+      if (a.vals_in) l2_prefetch_bulk(a.vals_in, lo * 4, hi * 4);
+      if (a.p.src != DigitSrc::CLASS) l2_prefetch_bulk(a.keys_in, lo * 8, hi * 8);
+    } else if (a.pf_columns && a.vals_in == nullptr) {  // rows in input order: the key columns are read in order
+      if (FUSEDG) {
+        for (int k = 0; k < a.fused.n; ++k) prefetch_column(a.fused.key[k].col, lo, hi);
+      } else if (a.p.src == DigitSrc::BUCKET) {
+        for (int k = 0; k < a.p.hash_keys.n; ++k) prefetch_column(a.p.hash_keys.c[k], lo, hi);
+      } else {
+        prefetch_column(a.p.key.col, lo, hi);
+      }
+    }
+  }
   load_tile_rows<GATHER, FUSEDG>(a, tile, key, val, dr);
   rank_and_scatter<WRITE_KEYS, MOVE>(a, tile, key, val, dr, sh, s_keys, s_vals, s_dig);
 }
@@ -820,6 +872,8 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
     if (k + 1 == run.size() && payload) a.pay = *payload;
     if (fused) a.fused = *fused;
     a.err        = ctx.err();
+    a.pf_ahead   = prefetch_tiles();
+    a.pf_columns = prefetch_first_pass();
     const unsigned g = static_cast<unsigned>(tiles);
     const bool move = !payload_empty(a.pay);
     if (gather && p.src == DigitSrc::FUSED) {  // the fused word's first pass
