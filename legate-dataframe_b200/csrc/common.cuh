@@ -236,6 +236,22 @@ __device__ __forceinline__ uint64_t dbits(const DCol& c, int64_t r)
   }
 }
 
+// dvalid / dbits with an evict-first hint, for a column read once in row
+// order: its lines leave L2 before the hash tables a pass probes.
+__device__ __forceinline__ bool dvalid_stream(const DCol& c, int64_t r)
+{
+  return c.valid == nullptr || __ldcs(c.valid + r) != 0;
+}
+__device__ __forceinline__ uint64_t dbits_stream(const DCol& c, int64_t r)
+{
+  switch (c.width) {
+    case 1: return __ldcs(static_cast<const uint8_t*>(c.data) + r);
+    case 2: return __ldcs(static_cast<const uint16_t*>(c.data) + r);
+    case 4: return __ldcs(static_cast<const uint32_t*>(c.data) + r);
+    default: return __ldcs(reinterpret_cast<const unsigned long long*>(c.data) + r);
+  }
+}
+
 __device__ __forceinline__ bool is_signed_int_dev(int t)
 {
   return t == LDF_INT8 || t == LDF_INT16 || t == LDF_INT32 || t == LDF_INT64 ||

@@ -325,11 +325,11 @@ __device__ void group_ids(const GbPlan& p, IdPool& pool, const int64_t (&r)[R], 
     pending[j] = false;
     word[j] = h[j] = idx[j] = hi[j] = 0;
     if (r[j] >= p.n) continue;
-    if (M != KeyMode::GEN && !dvalid(p.k.c[0], r[j])) {
+    if (M != KeyMode::GEN && !dvalid_stream(p.k.c[0], r[j])) {
       id[j] = kIdNull;
       continue;
     }
-    const uint64_t kb = key_bits<M>(p.k, r[j]);
+    const uint64_t kb = M == KeyMode::GEN ? key_bits<M>(p.k, r[j]) : dbits_stream(p.k.c[0], r[j]);
     if (M == KeyMode::GEN) {
       h[j]    = kb;
       word[j] = (static_cast<uint64_t>(r[j]) << 32) | static_cast<uint32_t>(kb);
@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(kGbThreads) assign_kernel(GbPlan p, uint32_t* 
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         if (r[j] >= p.n) continue;
-        gid[r[j]] = id[j];
+        __stcs(gid + r[j], id[j]);
         if (id[j] == kUnsetId) continue;
         if (id[j] < static_cast<uint32_t>(H)) atomicAdd(cnt + id[j], 1u);
         else red_add(p.states + static_cast<int64_t>(id[j]) * p.stride, 1);
@@ -545,10 +545,10 @@ struct ColArgs {
 template <int W, bool SGN, bool FLT>
 __device__ __forceinline__ uint64_t load_raw(const void* data, int64_t r)
 {
-  if (W == 1) return __ldg(static_cast<const unsigned char*>(data) + r);
-  if (W == 2) return __ldg(static_cast<const unsigned short*>(data) + r);
-  if (W == 4) return __ldg(static_cast<const unsigned int*>(data) + r);
-  return __ldg(static_cast<const unsigned long long*>(data) + r);
+  if (W == 1) return __ldcs(static_cast<const unsigned char*>(data) + r);
+  if (W == 2) return __ldcs(static_cast<const unsigned short*>(data) + r);
+  if (W == 4) return __ldcs(static_cast<const unsigned int*>(data) + r);
+  return __ldcs(static_cast<const unsigned long long*>(data) + r);
 }
 template <int W, bool SGN, bool FLT>
 __device__ __forceinline__ uint64_t ordered64(uint64_t raw)
@@ -603,10 +603,10 @@ __global__ void __launch_bounds__(kGbThreads) column_kernel(ColArgs a)
     for (int j = 0; j < kRows; ++j) {
       const int64_t r = base + static_cast<int64_t>(j) * blockDim.x + threadIdx.x;
       ok[j]           = r < a.n;
-      g[j] = ok[j] ? __ldg(a.gid + r) : kUnsetId;
+      g[j] = ok[j] ? __ldcs(a.gid + r) : kUnsetId;
       if (g[j] != kUnsetId) g[j] = __ldg(a.newid + g[j]);
       raw[j] = ok[j] ? load_raw<W, SGN, FLT>(a.col.data, r) : 0;
-      if (ok[j] && a.nullable) ok[j] = __ldg(a.col.valid + r) != 0;
+      if (ok[j] && a.nullable) ok[j] = __ldcs(a.col.valid + r) != 0;
       ok[j] = ok[j] && g[j] != kUnsetId;
     }
     if (W <= 4 && a.vrange) {
@@ -795,9 +795,9 @@ __device__ __forceinline__ void red_or32(uint32_t* p, uint32_t v)
 template <int W>
 __device__ __forceinline__ uint32_t load_bits(const void* data, int64_t r)
 {
-  if (W == 1) return __ldg(static_cast<const uint8_t*>(data) + r);
-  if (W == 2) return __ldg(static_cast<const uint16_t*>(data) + r);
-  return __ldg(static_cast<const uint32_t*>(data) + r);
+  if (W == 1) return __ldcs(static_cast<const uint8_t*>(data) + r);
+  if (W == 2) return __ldcs(static_cast<const uint16_t*>(data) + r);
+  return __ldcs(static_cast<const uint32_t*>(data) + r);
 }
 
 template <int W>
@@ -818,9 +818,9 @@ __global__ void __launch_bounds__(kGbThreads, 2) nunique_kernel(NdArgs a)
       g[j]            = kUnsetId;
       x[j]            = 0;
       if (r < a.n) {
-        g[j] = __ldg(a.gid + r);
+        g[j] = __ldcs(a.gid + r);
         x[j] = load_bits<W>(a.col.data, r);
-        if (a.col.valid != nullptr && __ldg(a.col.valid + r) == 0) g[j] = kUnsetId;
+        if (a.col.valid != nullptr && __ldcs(a.col.valid + r) == 0) g[j] = kUnsetId;
       }
     }
     // then the rank of each group (eight dependent loads in flight)
