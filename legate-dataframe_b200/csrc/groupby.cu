@@ -519,6 +519,18 @@ __global__ void __launch_bounds__(kGbThreads) assign_kernel(GbPlan p, uint32_t* 
     if (cnt[g]) red_add(p.states + static_cast<int64_t>(g) * p.stride, cnt[g]);
 }
 
+// Factor from the sampled group estimate to the key-table sizing estimate
+// (LDF_B200_GB_EST_MULT, 1 to 8).
+inline int64_t est_multiplier()
+{
+  static const int64_t m = [] {
+    const char* e = std::getenv("LDF_B200_GB_EST_MULT");
+    const int v   = e ? std::atoi(e) : 4;
+    return static_cast<int64_t>(v >= 1 && v <= 8 ? v : 4);
+  }();
+  return m;
+}
+
 // ---- pass 2: one value column (valid count, sum, min, max) ---------------------
 struct ColArgs {
   const uint32_t* gid;
@@ -1546,7 +1558,7 @@ void run_groupby(const OpContext& ctx, GbPlan p, const ldf_column* table, const 
     const double scale = std::sqrt(static_cast<double>(n) / static_cast<double>(ns));
     est_groups         = static_cast<int64_t>(scale * h[1] + (h[0] - h[1])) + 1;
     est_pairs          = static_cast<int64_t>(static_cast<double>(h[2]) * n / ns) + 1;
-    est_groups         = std::min<int64_t>(4 * est_groups, n);
+    est_groups         = std::min<int64_t>(est_multiplier() * est_groups, n);
     est_pairs          = std::min<int64_t>(est_pairs, n);
   }
   if (std::getenv("LDF_B200_DEBUG"))
