@@ -433,13 +433,22 @@ __device__ __forceinline__ void zero_fixed(void* dst, int64_t di, int w)
 // flight).  The range is shrunk inward to 16-byte bounds, as the instruction
 // requires, so no byte outside [lo, hi) is touched; a range under 16 bytes is
 // skipped.  A hint only: the data is still loaded by the caller.
+// The 16-byte-aligned span inside bytes [lo, hi) of the buffer at address
+// b0: its start in *addr, its size as the result (0: nothing to prefetch).
+__host__ __device__ __forceinline__ uint32_t prefetch_span(uint64_t b0, int64_t lo, int64_t hi, uint64_t* addr)
+{
+  const uint64_t a = (b0 + static_cast<uint64_t>(lo) + 15) & ~15ull;
+  const uint64_t e = (b0 + static_cast<uint64_t>(hi)) & ~15ull;
+  *addr            = a;
+  if (hi <= lo || e <= a || e - a > 0xfffffff0ull) return 0;
+  return static_cast<uint32_t>(e - a);
+}
 __device__ __forceinline__ void l2_prefetch_bulk(const void* base, int64_t lo, int64_t hi)
 {
-  const uint64_t b0 = reinterpret_cast<uint64_t>(base);
-  const uint64_t a  = (b0 + static_cast<uint64_t>(lo) + 15) & ~15ull;
-  const uint64_t e  = (b0 + static_cast<uint64_t>(hi)) & ~15ull;
-  if (e <= a || e - a > 0xfffffff0ull) return;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(static_cast<uint32_t>(e - a)) : "memory");
+  uint64_t a;
+  const uint32_t bytes = prefetch_span(reinterpret_cast<uint64_t>(base), lo, hi, &a);
+  if (bytes == 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
 }
 
 // Bounded spin budget for device-side waits (look-back).  A wait that runs
