@@ -72,6 +72,7 @@ def _compile(src: str, verbose: bool) -> Path:
 def build(force: bool = False, verbose: bool = False) -> Path:
     """Compile (if stale) and return the path of libldf_b200.so."""
     if LIB.exists() and not force and LIB.stat().st_mtime >= _newest_input_mtime():
+        sys.stderr.write(f"[ldf_b200 build] {LIB.name} is newer than every source: not recompiled\n")
         return LIB
     BUILD_DIR.mkdir(parents=True, exist_ok=True)
     subprocess.run([sys.executable, str(CSRC / "pow5_table.py"), str(BUILD_DIR / "pow5_table.inc")], check=True)
@@ -83,6 +84,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
     os.replace(tmp, LIB)
+    sys.stderr.write(f"[ldf_b200 build] compiled {len(objs)} CUDA sources for sm_100a into {LIB.name}\n")
     return LIB
 
 
