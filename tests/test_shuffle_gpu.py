@@ -1,6 +1,6 @@
 """The multi-rank exchange on the GPU path: `repartition_by_hash` with the
-local hash_partition kernel and NCCL all-to-alls, as a one-rank job (each
-gpurun call gets one GPU, so the exchange is the rank's send to itself).  The
+local hash_partition kernel and NCCL all-to-alls, as a one-rank job on one
+GPU (the exchange is then the rank's send to itself).  The
 rank must get back every row, in the oracle's bucket order: rows of bucket 0
 ... of the only rank, input order within each."""
 
