@@ -854,7 +854,7 @@ def main():
     else:
         dom_ms, algo_kernel, achieved = float("nan"), 0, float("nan")
     traffic = None
-    tp = ROOT / "profiles" / f"groupby_config1_{dom}_traffic.json"
+    tp = ROOT / "profiles" / f"groupby_200m_{dom}_traffic.json"
     if tp.exists():
         try:
             tj = json.loads(tp.read_text())

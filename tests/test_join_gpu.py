@@ -91,7 +91,7 @@ def test_join_unique_build_single_pass(how):
     assert_tables_equal(res, exp)
 
 
-def test_join_config0_shape():
+def test_join_1m_x_1m_uniform_int64_keys():
     # the reference benchmark shape: 1M x 1M int64 keys U[0, 2^20), seeds 1 and 2
     l_rng, r_rng = np.random.default_rng(1), np.random.default_rng(2)
     n = 1_000_000
