@@ -79,3 +79,23 @@ def test_partition_many_columns(nparts):
     exp, eoffs, _ = R.hash_partition(t, ["k"], nparts)
     assert offs == eoffs
     assert got.equals(exp)
+
+
+@pytest.mark.parametrize("nparts", [3, 256, 10_000])
+def test_partition_single_nullable_key(nparts):
+    """One key column, with nulls: strings of 0 to 60 bytes (longer than 32
+    bytes take the byte-wise hash), and int64 values; bucket counts above the
+    shared-memory counters (10,000) included."""
+    rng = np.random.default_rng(nparts + 11)
+    n = 50_000
+    words = [("w" * int(rng.integers(0, 61)))[: int(rng.integers(0, 61))] + str(i) for i in range(3000)]
+    t = pa.table({
+        "s": pa.array([None if rng.random() < 0.05 else words[int(v)] for v in rng.integers(0, 3000, n)]),
+        "k": pa.array(rng.integers(-10**12, 10**12, n), mask=rng.random(n) < 0.05),
+        "row": np.arange(n),
+    })
+    for keys in (["s"], ["k"]):
+        res, offs = run_partition(t, keys, nparts)
+        exp, eoffs, _ = R.hash_partition(t, keys, nparts)
+        assert offs == eoffs
+        assert_tables_equal(res, exp, sort_by=None)
