@@ -603,6 +603,39 @@ int prefetch_first_pass()
   return off ? 0 : 1;
 }
 
+// Whether p points into device memory (not pinned host or managed memory, as
+// a zero-copy legate store would be): the first pass prefetches only columns
+// held there.
+bool on_device(const void* p)
+{
+  if (p == nullptr) return true;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice;
+}
+bool column_on_device(const DCol& c) { return on_device(c.data) && on_device(c.valid); }
+
+// The key columns the first pass of `p` reads in row order are all in
+// device memory.
+bool pass_columns_on_device(const RadixPass& p, const FusedKey* fused)
+{
+  if (p.src == DigitSrc::FUSED) {
+    if (fused == nullptr) return false;
+    for (int k = 0; k < fused->n; ++k)
+      if (!column_on_device(fused->key[k].col)) return false;
+    return true;
+  }
+  if (p.src == DigitSrc::BUCKET) {
+    for (int k = 0; k < p.hash_keys.n; ++k)
+      if (!column_on_device(p.hash_keys.c[k])) return false;
+    return true;
+  }
+  return column_on_device(p.key.col);
+}
+
 // One tile per CTA.  WRITE_KEYS: later passes of the same word follow, so
 // carry the word along.  MOVE: the pass also moves a.pay's columns (the last
 // pass only, which carries no word).
@@ -873,7 +906,7 @@ void radix_sort_rows(const OpContext& ctx, const std::vector<RadixPass>& passes,
     if (fused) a.fused = *fused;
     a.err        = ctx.err();
     a.pf_ahead   = prefetch_tiles();
-    a.pf_columns = prefetch_first_pass();
+    a.pf_columns = gather && k == 0 && prefetch_first_pass() && pass_columns_on_device(p, fused) ? 1 : 0;
     const unsigned g = static_cast<unsigned>(tiles);
     const bool move = !payload_empty(a.pay);
     if (gather && p.src == DigitSrc::FUSED) {  // the fused word's first pass
