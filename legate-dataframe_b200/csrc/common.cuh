@@ -428,11 +428,6 @@ __device__ __forceinline__ void zero_fixed(void* dst, int64_t di, int w)
   }
 }
 
-// Prefetch bytes [lo, hi) of a buffer into L2 with one bulk-copy-engine
-// instruction (cp.async.bulk.prefetch.L2, no registers held while it is in
-// flight).  The range is shrunk inward to 16-byte bounds, as the instruction
-// requires, so no byte outside [lo, hi) is touched; a range under 16 bytes is
-// skipped.  A hint only: the data is still loaded by the caller.
 // The 16-byte-aligned span inside bytes [lo, hi) of the buffer at address
 // b0: its start in *addr, its size as the result (0: nothing to prefetch).
 __host__ __device__ __forceinline__ uint32_t prefetch_span(uint64_t b0, int64_t lo, int64_t hi, uint64_t* addr)
@@ -443,6 +438,12 @@ __host__ __device__ __forceinline__ uint32_t prefetch_span(uint64_t b0, int64_t 
   if (hi <= lo || e <= a || e - a > 0xfffffff0ull) return 0;
   return static_cast<uint32_t>(e - a);
 }
+
+// Prefetch bytes [lo, hi) of a buffer into L2 with one bulk-copy-engine
+// instruction (cp.async.bulk.prefetch.L2, no registers held while it is in
+// flight).  The range is shrunk inward to 16-byte bounds, as the instruction
+// requires, so no byte outside [lo, hi) is touched; a range under 16 bytes is
+// skipped.  A hint only: the data is still loaded by the caller.
 __device__ __forceinline__ void l2_prefetch_bulk(const void* base, int64_t lo, int64_t hi)
 {
   uint64_t a;
